@@ -1,0 +1,316 @@
+#!/usr/bin/env python
+"""Benchmark of the engine on the FP32 dispersive-sphere workload.
+
+Workload (one "step" = one FDTD time step over the whole grid): 384^3 inner
+cells + 12-cell CPML on all faces = 408^3 = 67.9 M cells, dl = 1 mm, sphere
+r = 0.1 m of a Drude (wp = 2e10, gamma = 1e9) + Lorentz (d_eps = 2, w0 = 3e10,
+delta = 5e8) ADE medium, x-propagating TFSF Gaussian, NF2FF at 1/3/5 GHz
+accumulated in FP64; fields, CPML psi and ADE state in FP32.  Inputs are
+synthetic (no dataset is involved); the 3.3 GB of resident field state is far
+larger than the 126 MB L2, so every step streams from HBM.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+Prints one JSON line.  `value` is device-timed Mcell-updates/s over K steps
+(CUDA events on the engine's stream, max over ranks); `e2e` is the same metric
+through the public run path (scene compile + upload + K steps + read-back of
+all fields and NF2FF currents, wall clock), the path the reference's own
+benchmark times (test/benchmark.cu:174-216).  With N > 1 every rank runs its
+own copy of the scene (independent scenes, no data-path collective): weak
+scaling.  `--impl reference` times the CPU restatement of the reference's
+algorithm (oracle/, OpenMP over all host cores) on a bounded sample of the
+same scene.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mcell-updates/s and % HBM roofline, FP32/batched/learned vs FP64 plain, 1 B200"
+UNIT = "Mcell-updates/s"
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def esize(precision):
+    return 8 if precision == "fp64" else 4
+
+
+def algorithmic_bytes(gi, kernel, precision):
+    """Compulsory DRAM bytes of one launch of `kernel` on grid `gi`.
+
+    Bulk half-step (H or E): read the 3 updated and the 3 dual components,
+    write the 3 updated ones, read the 1-byte material id: 9 T + 1 per cell.
+    CPML: read + write psi of the 2 tangential components of every slab cell.
+    ADE (E only): per dispersive cell and component, read + write J (per
+    pole), J_prev (per pole) and E_prev (M-Lorentz).
+    """
+    T = esize(precision)
+    nx, ny, nz = gi.nx, gi.ny, gi.nz
+    cells = nx * ny * nz
+    pml = [0] * 6
+    # slab cells per axis
+    b = 0
+    Ls = list(getattr(gi, "_pml", [0] * 6))
+    for a, n_a in enumerate((nx, ny, nz)):
+        L = Ls[2 * a] + Ls[2 * a + 1]
+        b += L * cells // n_a
+    if kernel in (0, 2):  # H or E half-step
+        byt = cells * (9 * T + 1) + b * 2 * 2 * T
+        if kernel == 2 and gi.ade_kind:
+            P = gi.ade_poles
+            per_comp = 2 * T * P + ((2 * T * P + 2 * T) if gi.ade_kind == 3 else 0)
+            byt += gi.n_dispersive_cells * 3 * per_comp
+        return byt
+    return None
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = Path(tempfile.mkstemp(suffix=".csv")[1])
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for r in rows for q in range(4) if r[5 + q].lower() == "active"})
+        loaded = sorted(sm)[len(sm) // 4:] if len(sm) > 4 else sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def build_scene(cells, precision):
+    from xfdtd_cuda_b200 import configs
+    return configs.dispersive_sphere(cells=cells, precision=precision)
+
+
+def cpu_sample(cells: int, steps: int, precision="fp64"):
+    """Time the CPU restatement on a bounded sample of the workload."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import xfdtd_cuda_b200 as X
+    from oracle import OracleSim
+    sim = build_scene(cells, "fp64")
+    sc, keep = sim.lower()
+    h = X.Handle(sc, keep)
+    o = OracleSim(h, steps + 2)
+    o.run(2)  # warm-up (first touch of the arrays)
+    gi = h.info()
+    t0 = time.perf_counter()
+    o.run(steps)
+    dt = time.perf_counter() - t0
+    n = gi.nx * gi.ny * gi.nz
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": n * steps / dt / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"dispersive sphere {gi.nx}x{gi.ny}x{gi.nz} ({cells}^3 + 12-cell CPML), FP64, {steps} steps, "
+                      f"CPU restatement (oracle/, OpenMP {threads} threads), {dt:.1f} s"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    cells = args.ref_cells
+    sample = cpu_sample(cells, max(1, args.warmup))  # warm-up steps
+    res = cpu_sample(cells, max(1, args.steps))
+    out = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "dispersive sphere (Drude+Lorentz ADE, TFSF, 12-cell CPML, NF2FF 1/3/5 GHz), "
+                                  f"bounded CPU sample {cells}^3 inner cells", "cells_per_step": None},
+           "cpu_baseline": res,
+           "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    del sample
+    print(json.dumps(out))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--cells", type=int, default=384)
+    ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
+    ap.add_argument("--profile-steps", type=int, default=6)
+    ap.add_argument("--ref-cells", type=int, default=128)
+    ap.add_argument("--cpu-steps", type=int, default=40)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = (torch, tdist)
+
+    if args.impl == "reference":
+        rc = run_reference(args, rank, world)
+        if dist:
+            dist[1].destroy_process_group()
+        return rc
+
+    import xfdtd_cuda_b200 as X
+    from xfdtd_cuda_b200 import _lib as L
+
+    sim = build_scene(args.cells, args.precision)
+    sc, keep = sim.lower()
+    h = X.Handle(sc, keep)
+    h.set_device(local)
+    total = args.warmup + args.steps + args.profile_steps
+    h.init(total)
+    gi = h.info()
+    gi._pml = [sc.pml.cells[q] for q in range(6)]
+    cells = gi.nx * gi.ny * gi.nz
+
+    h.step(args.warmup)
+    h.sync()
+
+    def barrier():
+        if dist:
+            dist[1].barrier()
+
+    barrier()
+    with ClockSampler(local) as clk:
+        ms = h.timed_step(args.steps)
+    barrier()
+    if dist:
+        t = dist[0].tensor([ms], dtype=dist[0].float64, device="cuda")
+        dist[1].all_reduce(t, op=dist[1].ReduceOp.MAX)
+        ms = float(t.item())
+    value = cells * args.steps * world / (ms / 1e3) / 1e6
+
+    # per-kernel device time (launches bracketed by events, no graph)
+    kms, kcnt = h.profile_kernels(args.profile_steps)
+    tot = sum(kms)
+    kernels = {L.KERNEL_NAMES[q]: {"launches": kcnt[q], "ms_per_launch": kms[q] / kcnt[q], "share": kms[q] / tot}
+               for q in range(L.K_COUNT) if kcnt[q]}
+    dom = max(range(L.K_COUNT), key=lambda q: kms[q])
+    peak, peak_kind = peaks()
+    alg = algorithmic_bytes(gi, dom, args.precision)
+    launch_ms = kms[dom] / kcnt[dom]
+    achieved = alg / (launch_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "kernel": L.KERNEL_NAMES[dom], "peak_source": peak_kind,
+                "algorithmic_bytes_per_launch": alg}
+    traffic_file = ROOT / "profiles" / "traffic.txt"
+    if traffic_file.exists():
+        for line in traffic_file.read_text().splitlines():
+            parts = line.split()
+            if len(parts) == 3 and parts[0] == "traffic_bytes_per_cell" and parts[1] == L.KERNEL_NAMES[dom].split()[0]:
+                roofline["traffic"] = float(parts[2]) * cells
+    step_bytes = cells * (12 * esize(args.precision) + 1)
+    step_roof = {"bytes_per_cell": 12 * esize(args.precision) + 1, "achieved": step_bytes / (ms / args.steps / 1e3) / 1e9,
+                 "peak": peak, "unit": "GB/s"}
+    step_roof["frac"] = step_roof["achieved"] / peak
+    launches = gi.launches_per_step * args.steps + (args.steps + 63) // 64
+
+    e2e = None
+    if not args.no_e2e:
+        barrier()
+        t0 = time.perf_counter()
+        sc2, keep2 = sim.lower()
+        h2 = X.Handle(sc2, keep2)
+        h2.set_device(local)
+        h2.init(args.steps)
+        h2.step(args.steps)
+        h2.sync()
+        d2h = 0
+        for f in range(6):
+            d2h += h2.read_field(f).size * esize(args.precision)
+        for f in range(gi.n_freqs):
+            for face in range(6):
+                for w in range(4):
+                    d2h += h2.read_nf2ff(f, face, w).size * 16
+        wall = time.perf_counter() - t0
+        h2d = cells * 1 + 64 * 1024  # material ids + coefficient/profile tables
+        if dist:
+            t = dist[0].tensor([wall], dtype=dist[0].float64, device="cuda")
+            dist[1].all_reduce(t, op=dist[1].ReduceOp.MAX)
+            wall = float(t.item())
+        e2e = {"value": cells * args.steps * world / wall / 1e6, "unit": UNIT,
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+               "path": "Handle(scene) + init + step + read-back (SimulationHD.run flow), wall clock"}
+        h2.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_sample(args.ref_cells, args.cpu_steps)
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic",
+               "config": {"workload": f"dispersive sphere {gi.nx}x{gi.ny}x{gi.nz} ({args.cells}^3 + 12-cell CPML), "
+                                      "Drude+Lorentz ADE, TFSF Gaussian, NF2FF 1/3/5 GHz (FP64 accumulation)",
+                          "cells_per_step": cells, "parallelism": f"scene-replica x{world}" if world > 1 else "1 GPU",
+                          "l2": "resident state 3.3 GB >> 126 MB L2 (no flush needed)"},
+               "e2e": e2e, "roofline": roofline, "step_roofline": step_roof, "cpu_baseline": cpu,
+               "clocks": clk.summary(), "gpu_launches": launches, "kernels": kernels}
+        print(json.dumps(out))
+    h.close()
+    if dist:
+        dist[1].barrier()
+        dist[1].destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

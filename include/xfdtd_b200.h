@@ -1,0 +1,324 @@
+/*
+ * xfdtd_b200.h -- C-ABI of the B200-native FDTD engine.
+ *
+ * This is the drop-in boundary for the GPU path of XFDTD_CUDA.  The reference
+ * exposes one C++ class, xfdtd::cuda::SimulationHD
+ * (include/xfdtd_cuda/simulation/simulation_hd.cuh:37-88), built from an
+ * XFDTD_CORE xfdtd::Simulation.  XFDTD_CORE (the host scene library) is not
+ * part of the reference, so the scene enters here as a plain description
+ * (xfb_scene) and the engine compiles it on the host (voxelisation, update
+ * coefficients, CPML profiles, TFSF geometry, NF2FF surfaces) exactly where
+ * XFDTD_CORE's Simulation::init would have done it.
+ *
+ * Conventions
+ *  - Every call returns an int status (XFB_OK == 0).  No C++ exception crosses
+ *    this boundary.  xfb_last_error() gives the message of the last failure on
+ *    a handle (thread-local message for calls without a handle).
+ *  - A handle owns one CUDA stream on the device that was current when it was
+ *    created.  A handle is not thread-safe.
+ *  - Grid indices follow the reference layout: row-major (i, j, k), k fastest
+ *    (include/xfdtd_cuda/tensor.cuh:203-212); the box has nx*ny*nz cells and the
+ *    Yee component shapes are Ex (nx, ny+1, nz+1), Ey (nx+1, ny, nz+1),
+ *    Ez (nx+1, ny+1, nz), Hx (nx+1, ny, nz), Hy (nx, ny+1, nz),
+ *    Hz (nx, ny, nz+1).  In 2-D (TMz) nz == 1.
+ *  - All host-side read-back buffers are double precision, whatever precision
+ *    the device computes in.
+ */
+#ifndef XFDTD_B200_H_
+#define XFDTD_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define XFB_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------- */
+#define XFB_OK 0
+#define XFB_ERR_INVALID 1   /* bad argument or scene                        */
+#define XFB_ERR_CUDA 2      /* CUDA runtime error                            */
+#define XFB_ERR_OOM 3       /* device or host allocation failed              */
+#define XFB_ERR_STATE 4     /* call not allowed in the current state         */
+#define XFB_ERR_RANGE 5     /* index / id out of range                       */
+#define XFB_ERR_NUMERIC 6   /* non-finite value detected by the watchdog      */
+#define XFB_ERR_TIMEOUT 7   /* a bounded device wait gave up                 */
+#define XFB_ERR_NO_DEVICE 8 /* no CUDA device available                      */
+
+/* ---- enumerations ------------------------------------------------------- */
+enum xfb_precision { XFB_FP32 = 0, XFB_FP64 = 1 };
+enum xfb_field { XFB_EX = 0, XFB_EY = 1, XFB_EZ = 2, XFB_HX = 3, XFB_HY = 4, XFB_HZ = 5 };
+enum xfb_face { XFB_XN = 0, XFB_XP = 1, XFB_YN = 2, XFB_YP = 3, XFB_ZN = 4, XFB_ZP = 5 };
+enum xfb_shape { XFB_SHAPE_CUBE = 0, XFB_SHAPE_SPHERE = 1, XFB_SHAPE_CYLINDER = 2 };
+enum xfb_pole_kind {
+  XFB_POLE_DEBYE = 0,    /* p = {delta_eps, tau}                         */
+  XFB_POLE_DRUDE = 1,    /* p = {omega_p, gamma}                         */
+  XFB_POLE_LORENTZ = 2,  /* p = {delta_eps, omega_0, delta}              */
+  XFB_POLE_MLORENTZ = 3  /* p = {a0, a1, b0, b1, b2}:
+                            chi(w) = (a0 + a1 jw) / (b0 + b1 jw + b2 (jw)^2) */
+};
+enum xfb_waveform { XFB_WAVE_GAUSSIAN = 0, XFB_WAVE_COS_GAUSSIAN = 1 };
+/* surface-current selector of one NF2FF face (reference: ja, jb, ma, mb,
+ * src/include/nf2ff/frequency_domain/nf2ff_frequency_domain_data.cuh:336) */
+enum xfb_current { XFB_JA = 0, XFB_JB = 1, XFB_MA = 2, XFB_MB = 3 };
+/* which E update the scene needs (the reference picks one updator for the
+ * whole grid: src/simulation/simulation_hd.cu:407-503) */
+enum xfb_ade_kind { XFB_ADE_NONE = 0, XFB_ADE_DEBYE = 1, XFB_ADE_DRUDE = 2, XFB_ADE_MLORENTZ = 3 };
+
+#define XFB_MAX_POLES 4
+#define XFB_MAX_MATERIALS 255
+
+/* ---- scene description -------------------------------------------------- */
+typedef struct xfb_pole {
+  int kind; /* enum xfb_pole_kind */
+  double p[5];
+} xfb_pole;
+
+typedef struct xfb_material {
+  double eps_r;   /* relative permittivity (eps_inf of a dispersive medium) */
+  double mu_r;    /* relative permeability                                  */
+  double sigma_e; /* electric conductivity, S/m                              */
+  double sigma_m; /* magnetic conductivity, Ohm/m                            */
+  int is_pec;     /* perfect electric conductor: E held at zero              */
+  int n_poles;    /* 0 .. XFB_MAX_POLES dispersive poles                     */
+  xfb_pole poles[XFB_MAX_POLES];
+} xfb_material;
+
+/* Shapes.  CUBE: p[0..2] min corner, p[3..5] size (may be +inf).
+ * SPHERE: p[0..2] centre, p[3] radius.
+ * CYLINDER: p[0..2] centre of the circular section, p[3] radius, p[4] axis
+ * (0=x, 1=y, 2=z), p[5] length along the axis centred on the centre (+inf:
+ * infinite).  The last object containing a cell centre decides its material. */
+typedef struct xfb_object {
+  int shape;
+  int material;
+  double p[8];
+} xfb_object;
+
+typedef struct xfb_pml {
+  int cells[6];        /* CPML thickness per face (enum xfb_face); 0 = PEC wall */
+  double order_m;      /* polynomial grading order (default 3)              */
+  double sigma_ratio;  /* sigma_max / sigma_opt (default 1)                  */
+  double alpha_max;    /* CFS alpha at the interface (default 0.05)         */
+} xfb_pml;
+
+typedef struct xfb_tfsf {
+  int enabled;
+  int inset[3];        /* cells between the inner domain edge and the TF box */
+  double theta, phi, psi; /* incidence direction and polarisation, rad     */
+  int waveform;        /* enum xfb_waveform                                  */
+  double tau, t0, freq;   /* waveform parameters (s, s, Hz)                  */
+} xfb_tfsf;
+
+typedef struct xfb_nf2ff {
+  int enabled;
+  int inset[3];        /* cells between the inner domain edge and the box    */
+  int n_freqs;
+  const double* freqs; /* Hz */
+} xfb_nf2ff;
+
+typedef struct xfb_probe {
+  int field;           /* enum xfb_field */
+  int index[3];        /* component index (i, j, k) */
+} xfb_probe;
+
+typedef struct xfb_movie {
+  int field;           /* enum xfb_field */
+  int lo[3], hi[3];    /* half-open component-index box */
+  int interval;        /* a frame every `interval` steps, starting at step 0 */
+} xfb_movie;
+
+typedef struct xfb_scene {
+  int dim;             /* 3 or 2 (TMz: Ez, Hx, Hy) */
+  int precision;       /* enum xfb_precision */
+  double dx, dy, dz;
+  double courant;      /* dt = courant / (c * sqrt(sum 1/d^2)) */
+  double domain_min[3];   /* physical corner of the inner domain (no PML) */
+  int domain_cells[3];    /* inner cells per axis (nz = 1 in 2-D) */
+  int n_materials;        /* materials[0] is the background */
+  const xfb_material* materials;
+  int n_objects;
+  const xfb_object* objects;
+  xfb_pml pml;
+  xfb_tfsf tfsf;
+  xfb_nf2ff nf2ff;
+  int n_probes;
+  const xfb_probe* probes;
+  int n_movies;
+  const xfb_movie* movies;
+} xfb_scene;
+
+/* ---- grid information --------------------------------------------------- */
+typedef struct xfb_grid_info {
+  int dim, precision;
+  int nx, ny, nz;            /* total cells including CPML */
+  double dx, dy, dz, dt;
+  double origin[3];          /* physical position of node (0,0,0) */
+  int n_materials;
+  int ade_kind;              /* enum xfb_ade_kind */
+  int ade_poles;
+  int tfsf_box[6];           /* is, ie, js, je, ks, ke (nodes) or zeros */
+  int nf2ff_box[6];          /* is, ie, js, je, ks, ke (nodes) or zeros */
+  int n_freqs;
+  long long current_step;    /* steps taken since the last init */
+  long long total_steps;     /* steps the last init sized its buffers for */
+  size_t device_bytes;       /* device memory held by the handle */
+  long long n_dispersive_cells; /* cells whose material has ADE poles */
+  int launches_per_step;     /* engine kernels one time step launches */
+} xfb_grid_info;
+
+typedef struct xfb_handle xfb_handle;
+
+/* ---- lifecycle ---------------------------------------------------------- */
+
+/* Compile a scene on the host (no device work).  Replaces the reference
+ * constructor SimulationHD(xfdtd::Simulation*)
+ * (include/xfdtd_cuda/simulation/simulation_hd.cuh:39) together with the
+ * XFDTD_CORE Simulation::init it triggers (src/simulation/simulation_hd.cu:259-267). */
+int xfb_create(const xfb_scene* scene, xfb_handle** out);
+
+/* Release every device and host resource.  Replaces ~SimulationHD and
+ * SimulationHD::releaseDevice (simulation_hd.cuh:41,47). */
+int xfb_destroy(xfb_handle* h);
+
+/* Device ordinal the handle will use (default: the device current at the
+ * first xfb_init).  Must be called before the first xfb_init. */
+int xfb_set_device(xfb_handle* h, int ordinal);
+
+/* Launch-shape hint.  Replaces SimulationHD::setGridDim / setBlockDim
+ * (simulation_hd.cuh:53,55).  The engine sizes its own grid; the thread count
+ * of the block hint (bx*by*bz, a multiple of 32, at most 1024) selects the
+ * bulk-update tile: 32 lanes along k times (threads/32) rows along j. */
+int xfb_set_launch_hint(xfb_handle* h, const unsigned grid[3], const unsigned block[3]);
+
+/* Allocate and zero device state for a run of `total_steps` steps (sizes the
+ * movie, probe and NF2FF-transform buffers).  Replaces SimulationHD::init
+ * (simulation_hd.cuh:51) plus copyHostToDevice (simulation_hd.cuh:43). */
+int xfb_init(xfb_handle* h, long long total_steps);
+
+/* Reference run(n) (simulation_hd.cuh:49; src/simulation/simulation_hd.cu:106-257):
+ * re-initialise for n steps, advance n steps, wait for the device.  Results
+ * stay on the device until read. */
+int xfb_run(xfb_handle* h, long long n_steps);
+
+/* Advance n more steps from the current state (no re-initialisation; n must
+ * not take the run beyond the steps xfb_init sized for).  Asynchronous. */
+int xfb_step(xfb_handle* h, long long n_steps);
+
+/* Block until the handle's stream is idle; reports device-side errors. */
+int xfb_sync(xfb_handle* h);
+
+/* Advance n steps bracketed by CUDA events on the handle's stream (after a
+ * synchronize); *ms = elapsed device time of the n steps. */
+int xfb_timed_step(xfb_handle* h, long long n, double* ms);
+
+/* Kernel classes of one time step, for xfb_profile_kernels. */
+enum xfb_kernel_class {
+  XFB_K_UPDATE_H = 0, XFB_K_AUX = 1, XFB_K_UPDATE_E = 2, XFB_K_NF2FF = 3, XFB_K_PROBE = 4,
+  XFB_K_MOVIE = 5, XFB_K_COUNT = 6
+};
+/* Advance n steps launching every kernel individually with CUDA events around
+ * it; ms[c] = summed device time and launches[c] = launch count of class c
+ * (arrays of XFB_K_COUNT). */
+int xfb_profile_kernels(xfb_handle* h, long long n, double* ms, long long* launches);
+
+/* Use CUDA-graph replay of the step loop (default 1) and the steps per
+ * captured graph (default 64). */
+int xfb_set_graph(xfb_handle* h, int enabled, int steps_per_graph);
+
+int xfb_get_grid_info(const xfb_handle* h, xfb_grid_info* out);
+
+/* ---- read-back (reference copyDeviceToHost, simulation_hd.cuh:45) -------- */
+
+/* One field component in its reference shape, converted to double. */
+int xfb_read_field(xfb_handle* h, int field, double* dst, size_t dst_len);
+/* Overwrite one field component (reference shape, double) - initial values. */
+int xfb_write_field(xfb_handle* h, int field, const double* src, size_t src_len);
+/* Time series of probe `id` (one value per step taken, double). */
+int xfb_read_probe(xfb_handle* h, int id, double* dst, size_t dst_len, long long* n_written);
+/* Movie frames of monitor `id`: [frames, lo..hi box] in double; the reference
+ * MovieMonitor<F>::update frame rule (src/monitor/movie_monitor.cu:17-46). */
+int xfb_movie_shape(const xfb_handle* h, int id, int shape_out[4]);
+int xfb_read_movie(xfb_handle* h, int id, double* dst, size_t dst_len);
+/* NF2FF surface current `which` (enum xfb_current) of `face` at frequency
+ * `freq`: complex, interleaved (re, im), face extent shape.  The reference
+ * NF2FFFrequencyDomainData<D>::calculateJ/M accumulators
+ * (src/nf2ff/frequency_domain/nf2ff_frequency_domain.data.cu:80-194). */
+int xfb_nf2ff_face_shape(const xfb_handle* h, int face, int shape_out[3]);
+int xfb_read_nf2ff(xfb_handle* h, int freq, int face, int which, double* dst, size_t dst_len);
+/* Far field from the accumulated surface currents, computed on the device.
+ * For each (theta[i], phi[i]) writes 4 doubles: Re/Im E_theta, Re/Im E_phi of
+ * r*E (the e^{-jkr} factor removed), in the e^{+jwt} phasor convention of the
+ * DFT.  Replaces XFDTD_CORE NFFFTFrequencyDomain::processFarField, which the
+ * reference calls on the host (test/dielectric_sphere_scatter.cu:85-91). */
+int xfb_far_field(xfb_handle* h, int freq, int n_angles, const double* theta,
+                  const double* phi, double* out);
+
+/* ---- checkpoint / resume ------------------------------------------------ */
+/* Byte size of the full solver state (fields, CPML psi, ADE state, TFSF
+ * auxiliary grid, NF2FF accumulators, monitors, step counter). */
+int xfb_state_size(const xfb_handle* h, size_t* bytes);
+int xfb_get_state(xfb_handle* h, void* dst, size_t dst_len);
+int xfb_set_state(xfb_handle* h, const void* src, size_t src_len);
+
+/* ---- status -------------------------------------------------------------- */
+/* Scan the fields for non-finite values; *bad = number of non-finite entries.
+ * Returns XFB_ERR_NUMERIC when any is found. */
+int xfb_check_finite(xfb_handle* h, long long* bad);
+const char* xfb_last_error(const xfb_handle* h);
+const char* xfb_status_string(int status);
+int xfb_abi_version(void);
+
+/* ---- compiled-scene export (host only; used by the CPU restatement) ------ */
+/* The arrays the host scene compiler produced, i.e. what XFDTD_CORE would hand
+ * to the reference's *HD wrappers.  Pointers stay valid until xfb_destroy. */
+typedef struct xfb_compiled_view {
+  int dim, nx, ny, nz;
+  double dx, dy, dz, dt;
+  const uint8_t* material_id;   /* [nx][ny][nz] cell material index          */
+  int n_materials;
+  const double* coeff;          /* [n_materials][18] cexe cexhy cexhz ceye ceyhz
+                                   ceyhx ceze cezhx cezhy chxh chxey chxez chyh
+                                   chyez chyex chzh chzex chzey               */
+  int ade_kind, ade_poles;
+  const double* ade_mat;        /* [n_materials][3] is_dispersive ceep cejsum */
+  const double* ade_pole;       /* [n_materials][poles][7] cjj cjjp cjen cje
+                                   cjep cjsj cjsjp                            */
+  int pml_cells[6];
+  const double* pml_ae[3];      /* per axis, length n_axis+1 (E nodes)        */
+  const double* pml_be[3];
+  const double* pml_ah[3];      /* per axis, length n_axis (H half nodes)     */
+  const double* pml_bh[3];
+  int tfsf_enabled;
+  int tfsf_box[6];
+  const double* tfsf_proj_int[3];  /* length box_n+1 */
+  const double* tfsf_proj_half[3]; /* length box_n+2 */
+  double tfsf_transform_e[3], tfsf_transform_h[3];
+  double tfsf_ca[3], tfsf_cb[3];
+  int aux_nl;                   /* aux E nodes 0..nl, H nodes 0..nl-1        */
+  double aux_ceih, aux_chie, aux_abc;
+  const double* aux_source;     /* E source at aux node 0, index t = time t*dt;
+                                   length total_steps+1 (valid after init)    */
+  long long total_steps;
+  int nf2ff_enabled;
+  int nf2ff_box[6];
+  int n_freqs;
+  const double* freqs;
+  const double* nf2ff_te;       /* [n_freqs][total_steps] complex (re,im)    */
+  const double* nf2ff_th;
+} xfb_compiled_view;
+
+int xfb_compiled_view_get(const xfb_handle* h, xfb_compiled_view* out);
+
+/* Host only: size the step-count dependent tables (TFSF source samples,
+ * NF2FF DFT kernels) for a run of total_steps steps without touching a
+ * device, so xfb_compiled_view_get exposes them.  xfb_init calls it. */
+int xfb_prepare_tables(xfb_handle* h, long long total_steps);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* XFDTD_B200_H_ */
