@@ -64,20 +64,22 @@ def algorithmic_bytes(gi, kernel, precision):
     T = esize(precision)
     nx, ny, nz = gi.nx, gi.ny, gi.nz
     cells = nx * ny * nz
-    pml = [0] * 6
     # slab cells per axis
     b = 0
     Ls = list(getattr(gi, "_pml", [0] * 6))
     for a, n_a in enumerate((nx, ny, nz)):
         L = Ls[2 * a] + Ls[2 * a + 1]
         b += L * cells // n_a
+    ade = 0
+    if gi.ade_kind:
+        P = gi.ade_poles
+        per_comp = 2 * T * P + ((2 * T * P + 2 * T) if gi.ade_kind == 3 else 0)
+        ade = gi.n_dispersive_cells * 3 * per_comp
     if kernel in (0, 2):  # H or E half-step
         byt = cells * (9 * T + 1) + b * 2 * 2 * T
-        if kernel == 2 and gi.ade_kind:
-            P = gi.ade_poles
-            per_comp = 2 * T * P + ((2 * T * P + 2 * T) if gi.ade_kind == 3 else 0)
-            byt += gi.n_dispersive_cells * 3 * per_comp
-        return byt
+        return byt + (ade if kernel == 2 else 0)
+    if kernel == 6:  # one-sweep step: read E^n, H^{n-1/2}; write H^{n+1/2}, E^{n+1}
+        return cells * (12 * T + 1) + b * 4 * 2 * T + ade
     return None
 
 
@@ -130,9 +132,20 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def build_scene(cells, precision):
+def build_scene(cells, precision, scene="dispersive"):
+    """The benchmark workload, or a reduced variant for kernel diagnostics
+    (vacuum: PEC box only; pml: + CPML; tfsf: + CPML + TFSF; nf2ff: + NF2FF)."""
     from xfdtd_cuda_b200 import configs
-    return configs.dispersive_sphere(cells=cells, precision=precision)
+    if scene == "dispersive":
+        return configs.dispersive_sphere(cells=cells, precision=precision)
+    s = configs.dispersive_sphere(cells=cells, precision=precision, freqs=(1e9, 3e9, 5e9) if scene == "nf2ff" else ())
+    s.objects = s.objects[:1]
+    if scene == "vacuum":
+        s.boundaries = []
+        s.sources = []
+    elif scene == "pml":
+        s.sources = []
+    return s
 
 
 def cpu_sample(cells: int, steps: int, precision="fp64"):
@@ -187,6 +200,9 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--path", choices=["auto", "split", "fused"], default="auto")
+    ap.add_argument("--scene", choices=["dispersive", "vacuum", "pml", "tfsf", "nf2ff"], default="dispersive")
+    ap.add_argument("--tile-rows", type=int, default=8)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -210,10 +226,13 @@ def main():
     import xfdtd_cuda_b200 as X
     from xfdtd_cuda_b200 import _lib as L
 
-    sim = build_scene(args.cells, args.precision)
+    sim = build_scene(args.cells, args.precision, args.scene)
     sc, keep = sim.lower()
     h = X.Handle(sc, keep)
     h.set_device(local)
+    path = {"auto": L.PATH_AUTO, "split": L.PATH_SPLIT, "fused": L.PATH_FUSED}[args.path]
+    h.set_kernel_path(path)
+    h.set_launch_hint((1, 1, 1), (32, args.tile_rows, 1))
     total = args.warmup + args.steps + args.profile_steps
     h.init(total)
     gi = h.info()
@@ -269,6 +288,8 @@ def main():
         sc2, keep2 = sim.lower()
         h2 = X.Handle(sc2, keep2)
         h2.set_device(local)
+        h2.set_kernel_path(path)
+        h2.set_launch_hint((1, 1, 1), (32, args.tile_rows, 1))
         h2.init(args.steps)
         h2.step(args.steps)
         h2.sync()

@@ -66,6 +66,11 @@ enum xfb_current { XFB_JA = 0, XFB_JB = 1, XFB_MA = 2, XFB_MB = 3 };
 /* which E update the scene needs (the reference picks one updator for the
  * whole grid: src/simulation/simulation_hd.cu:407-503) */
 enum xfb_ade_kind { XFB_ADE_NONE = 0, XFB_ADE_DEBYE = 1, XFB_ADE_DRUDE = 2, XFB_ADE_MLORENTZ = 3 };
+/* How a 3-D time step is executed.  SPLIT: an H half-step kernel and an E
+ * half-step kernel (the reference's updateH/updateE split, correctors fused).
+ * FUSED: one kernel per step that sweeps the grid once (H and E together,
+ * ping-pong field buffers).  AUTO: FUSED in 3-D, SPLIT in 2-D. */
+enum xfb_kernel_path { XFB_PATH_AUTO = 0, XFB_PATH_SPLIT = 1, XFB_PATH_FUSED = 2 };
 
 #define XFB_MAX_POLES 4
 #define XFB_MAX_MATERIALS 255
@@ -167,6 +172,7 @@ typedef struct xfb_grid_info {
   size_t device_bytes;       /* device memory held by the handle */
   long long n_dispersive_cells; /* cells whose material has ADE poles */
   int launches_per_step;     /* engine kernels one time step launches */
+  int kernel_path;           /* enum xfb_kernel_path in use (after init) */
 } xfb_grid_info;
 
 typedef struct xfb_handle xfb_handle;
@@ -217,12 +223,15 @@ int xfb_timed_step(xfb_handle* h, long long n, double* ms);
 /* Kernel classes of one time step, for xfb_profile_kernels. */
 enum xfb_kernel_class {
   XFB_K_UPDATE_H = 0, XFB_K_AUX = 1, XFB_K_UPDATE_E = 2, XFB_K_NF2FF = 3, XFB_K_PROBE = 4,
-  XFB_K_MOVIE = 5, XFB_K_COUNT = 6
+  XFB_K_MOVIE = 5, XFB_K_STEP = 6, XFB_K_COUNT = 7
 };
 /* Advance n steps launching every kernel individually with CUDA events around
  * it; ms[c] = summed device time and launches[c] = launch count of class c
  * (arrays of XFB_K_COUNT). */
 int xfb_profile_kernels(xfb_handle* h, long long n, double* ms, long long* launches);
+
+/* Select the 3-D kernel path (enum xfb_kernel_path); before xfb_init. */
+int xfb_set_kernel_path(xfb_handle* h, int path);
 
 /* Use CUDA-graph replay of the step loop (default 1) and the steps per
  * captured graph (default 64). */

@@ -10,9 +10,10 @@ FIELDS_3D = (0, 1, 2, 3, 4, 5)
 FIELDS_2D = (2, 3, 4)
 
 
-def engine(sim: X.Simulation, n_steps: int, graph=True, block=(32, 8, 1)) -> X.Handle:
+def engine(sim: X.Simulation, n_steps: int, graph=True, block=(32, 8, 1), path=0) -> X.Handle:
     sc, keep = sim.lower()
     h = X.Handle(sc, keep)
+    h.set_kernel_path(path)
     h.set_launch_hint((1, 1, 1), block)
     h.set_graph(graph, 16)
     h.init(n_steps)

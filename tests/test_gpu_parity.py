@@ -37,8 +37,11 @@ def add_movie(sim, field=0, interval=7):
     return sim
 
 
-def run_pair(sim, n):
-    h = engine(sim, n)
+PATHS = [1, 2]  # XFB_PATH_SPLIT (H and E half-step kernels), XFB_PATH_FUSED (one-sweep step)
+
+
+def run_pair(sim, n, path=0):
+    h = engine(sim, n, path=path)
     h.step(n)
     h.sync()
     o = oracle_of(sim, n)
@@ -65,14 +68,16 @@ def check_all(h, o, dim, n_probes, n_movies, nf, tol=FP64_TOL, expect_exact=True
         assert bit_equal(gf, of), "FP64 fields agree within tolerance but not bit for bit"
 
 
-def test_fp64_dielectric_sphere_bitexact():
+@pytest.mark.parametrize("path", PATHS)
+def test_fp64_dielectric_sphere_bitexact(path):
     sim = add_movie(small_sphere())
-    h, o = run_pair(sim, 90)
+    h, o = run_pair(sim, 90, path)
     check_all(h, o, 3, 3, 1, nf=True)
 
 
+@pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("kind", ["drude", "debye", "drude_lorentz", "mlorentz"])
-def test_fp64_ade_bitexact(kind):
+def test_fp64_ade_bitexact(kind, path):
     mats = {
         "drude": X.DrudeMedium("d", 1.0, [2e10], [1e9]),
         "debye": X.DebyeMedium("b", 2.0, [6.0], [2e-11]),
@@ -83,7 +88,7 @@ def test_fp64_ade_bitexact(kind):
     sim = configs.dispersive_sphere(cells=26, dl=4e-3, pml=6, precision="fp64", freqs=(1e9, 3e9), tfsf_inset=4,
                                     nf2ff_inset=2, radius=0.03, material=mats[kind],
                                     probes=[((0.0, 0.0, 0.0), 2), ((0.01, 0.0, 0.0), 1)])
-    h, o = run_pair(sim, 80)
+    h, o = run_pair(sim, 80, path)
     check_all(h, o, 3, 2, 0, nf=True)
 
 
@@ -95,14 +100,15 @@ def test_fp64_cylinder_2d_bitexact():
     check_all(h, o, 2, 5, 1, nf=False)
 
 
-def test_fp64_no_tfsf_no_pml_initial_field():
-    # PEC box with an initial Ez blob: pure Yee update, no correctors
+@pytest.mark.parametrize("path", PATHS)
+def test_fp64_no_tfsf_no_pml_initial_field(path):
+    # PEC box with random initial fields: pure Yee update, no correctors
     sim = X.Simulation(3e-3, 3e-3, 3e-3, 0.9)
     sim.addObject(X.Object("domain", X.Cube(X.Vector(0, 0, 0), X.Vector(0.051, 0.042, 0.039)), X.Material.createAir()))
     sim.addObject(X.Object("blk", X.Cube(X.Vector(0.01, 0.01, 0.01), X.Vector(0.01, 0.02, 0.01)),
                            X.Material("lossy", X.ElectroMagneticProperty(4.0, 1.5, 0.02, 0.0))))
     n = 60
-    h = engine(sim, n)
+    h = engine(sim, n, path=path)
     o = oracle_of(sim, n)
     rng = np.random.default_rng(7)
     for f in range(6):
@@ -117,11 +123,12 @@ def test_fp64_no_tfsf_no_pml_initial_field():
     assert bit_equal(gf, of)
 
 
-def test_fp32_against_fp64_oracle():
+@pytest.mark.parametrize("path", PATHS)
+def test_fp32_against_fp64_oracle(path):
     sim32 = small_sphere("fp32")
     sim64 = small_sphere("fp64")
     n = 240
-    h = engine(sim32, n)
+    h = engine(sim32, n, path=path)
     h.step(n)
     h.sync()
     o = oracle_of(sim64, n)
@@ -156,21 +163,32 @@ def test_far_field_kernel_matches_numpy():
 
 
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])
-def test_graph_and_tile_invariance(precision):
+def test_graph_tile_and_path_invariance(precision):
+    # Tile shape and graph replay never change a bit.  Across kernel paths the
+    # FP64 build (no FMA contraction) is bit-identical; the FP32 build contracts
+    # the two paths' expressions differently, so there they agree to round-off.
     sim = configs.dispersive_sphere(cells=30, dl=4e-3, pml=5, precision=precision, freqs=(2e9,), tfsf_inset=4,
                                     nf2ff_inset=2, radius=0.035)
     n = 50
-    ref = engine(sim, n, graph=False, block=(32, 8, 1))
-    ref.step(n)
-    ref.sync()
-    want = fields_of(ref, 3)
-    for graph, block in [(True, (32, 8, 1)), (True, (32, 4, 1)), (True, (64, 16, 1))]:
-        h = engine(sim, n, graph=graph, block=block)
+    refs = {}
+    for path in (1, 2):
+        r = engine(sim, n, graph=False, block=(32, 8, 1), path=path)
+        r.step(n)
+        r.sync()
+        refs[path] = r
+    for graph, block, path in [(True, (32, 8, 1), 1), (True, (32, 4, 1), 1), (True, (64, 16, 1), 1),
+                               (True, (32, 8, 1), 2), (True, (32, 4, 1), 2), (True, (64, 16, 1), 2)]:
+        h = engine(sim, n, graph=graph, block=block, path=path)
         h.step(17)
         h.step(n - 17)
         h.sync()
-        assert bit_equal(fields_of(h, 3), want)
-        assert np.array_equal(h.read_nf2ff(0, 1, 2), ref.read_nf2ff(0, 1, 2))
+        assert bit_equal(fields_of(h, 3), fields_of(refs[path], 3))
+        assert np.array_equal(h.read_nf2ff(0, 1, 2), refs[path].read_nf2ff(0, 1, 2))
+    a, b = fields_of(refs[1], 3), fields_of(refs[2], 3)
+    if precision == "fp64":
+        assert bit_equal(a, b)
+    else:
+        assert compare_fields(a, b) < 1e-4
 
 
 def test_checkpoint_resume_equivalence():

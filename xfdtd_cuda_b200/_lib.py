@@ -24,9 +24,10 @@ WAVE_GAUSSIAN, WAVE_COS_GAUSSIAN = 0, 1
 JA, JB, MA, MB = 0, 1, 2, 3
 ADE_NONE, ADE_DEBYE, ADE_DRUDE, ADE_MLORENTZ = 0, 1, 2, 3
 MAX_POLES = 4
-K_UPDATE_H, K_AUX, K_UPDATE_E, K_NF2FF, K_PROBE, K_MOVIE, K_COUNT = range(7)
+K_UPDATE_H, K_AUX, K_UPDATE_E, K_NF2FF, K_PROBE, K_MOVIE, K_STEP, K_COUNT = range(8)
 KERNEL_NAMES = ("k_h3/k_h2 (H half-step)", "k_aux (TFSF aux grid)", "k_e3/k_e2 (E half-step)", "k_nf2ff",
-                "k_probe", "k_movie")
+                "k_probe", "k_movie", "k_step3 (one-sweep H+E step)")
+PATH_AUTO, PATH_SPLIT, PATH_FUSED = 0, 1, 2
 
 
 class Pole(C.Structure):
@@ -87,7 +88,7 @@ class GridInfo(C.Structure):
         ("origin", C.c_double * 3), ("n_materials", C.c_int), ("ade_kind", C.c_int), ("ade_poles", C.c_int),
         ("tfsf_box", C.c_int * 6), ("nf2ff_box", C.c_int * 6), ("n_freqs", C.c_int),
         ("current_step", C.c_longlong), ("total_steps", C.c_longlong), ("device_bytes", C.c_size_t),
-        ("n_dispersive_cells", C.c_longlong), ("launches_per_step", C.c_int),
+        ("n_dispersive_cells", C.c_longlong), ("launches_per_step", C.c_int), ("kernel_path", C.c_int),
     ]
 
 
@@ -130,6 +131,7 @@ SIGNATURES = [
     ("xfb_timed_step", C.c_int, [_H, C.c_longlong, C.POINTER(C.c_double)]),
     ("xfb_profile_kernels", C.c_int, [_H, C.c_longlong, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
     ("xfb_set_graph", C.c_int, [_H, C.c_int, C.c_int]),
+    ("xfb_set_kernel_path", C.c_int, [_H, C.c_int]),
     ("xfb_get_grid_info", C.c_int, [_H, C.POINTER(GridInfo)]),
     ("xfb_read_field", C.c_int, [_H, C.c_int, _dp, C.c_size_t]),
     ("xfb_write_field", C.c_int, [_H, C.c_int, _dp, C.c_size_t]),

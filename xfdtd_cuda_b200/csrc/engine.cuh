@@ -1,0 +1,496 @@
+// Per-precision engine: device buffers, launch sequencing, CUDA-graph replay,
+// read-back.  Included by engine_f32.cu (compiled with FMA contraction) and
+// engine_f64.cu (compiled with --fmad=false, so FP64 reproduces the CPU
+// restatement bit for bit).
+#pragma once
+
+#include <algorithm>
+#include <cstring>
+
+#include "fused3d.cuh"
+#include "handle.h"
+#include "kernels.cuh"
+
+namespace xfb {
+
+template <typename T>
+int init_device(xfb_handle* h) {
+  Compiled& c = h->c;
+  const int nx = c.nx, ny = c.ny, nz = c.nz;
+  if (c.dim == 3) {
+    h->nzp = roundup(nz + 1, 32);
+    h->sy = h->nzp;
+    h->sx = (ny + 1) * h->nzp;
+  } else {
+    h->nzp = 1;
+    h->sy = 1;
+    h->sx = roundup(ny + 1, 32);
+  }
+  h->elems = (nx + 1) * h->sx;
+  h->guard = roundup(h->sx + 40 * h->sy + 256, 64);
+  const size_t fbytes = (h->elems + 2 * h->guard) * sizeof(T);
+  int rc;
+  for (int q = 0; q < 6; ++q) {
+    if (c.dim == 2 && !(q == XFB_EZ || q == XFB_HX || q == XFB_HY)) continue;
+    void* p;
+    if ((rc = alloc(h, &p, fbytes, true))) return rc;
+    h->f[q] = as<T>(p) + h->guard;
+    if (fused(h)) {
+      if ((rc = alloc(h, &p, fbytes, true))) return rc;
+      h->f1[q] = as<T>(p) + h->guard;
+    }
+  }
+  // material ids in the padded layout
+  {
+    std::vector<uint8_t> m(static_cast<size_t>(h->elems), 0);
+    for (int i = 0; i < nx; ++i)
+      for (int j = 0; j < ny; ++j)
+        for (int k = 0; k < nz; ++k) m[off3(h, i, j, k)] = c.mat_id[(static_cast<size_t>(i) * ny + j) * nz + k];
+    void* p;  // same guard as the fields (the one-sweep kernel stages halo windows)
+    if ((rc = alloc(h, &p, m.size() + 2 * h->guard, false))) return rc;
+    XFB_CUDA(h, cudaMemcpy(static_cast<uint8_t*>(p) + h->guard, m.data(), m.size(), cudaMemcpyHostToDevice));
+    h->mid = static_cast<uint8_t*>(p) + h->guard;
+  }
+  if ((rc = upload<T>(h, &h->lut, c.coeff))) return rc;
+  if ((rc = upload<T>(h, &h->lut8, c.coeff8))) return rc;
+  {
+    void* p;
+    if ((rc = alloc(h, &p, c.mat_disp.size(), false))) return rc;
+    XFB_CUDA(h, cudaMemcpy(p, c.mat_disp.data(), c.mat_disp.size(), cudaMemcpyHostToDevice));
+    h->mat_disp = static_cast<uint8_t*>(p);
+  }
+  // CPML
+  const int L[6] = {c.pml[0], c.pml[1], c.pml[2], c.pml[3], c.pml[4], c.pml[5]};
+  for (int a = 0; a < 3; ++a) {
+    if ((rc = upload<T>(h, &h->prof[a], c.pml_ae[a]))) return rc;
+    if ((rc = upload<T>(h, &h->prof[3 + a], c.pml_be[a]))) return rc;
+    if ((rc = upload<T>(h, &h->prof[6 + a], c.pml_ah[a]))) return rc;
+    if ((rc = upload<T>(h, &h->prof[9 + a], c.pml_bh[a]))) return rc;
+  }
+  const long long Lx = L[0] + L[1], Ly = L[2] + L[3], Lz = L[4] + L[5];
+  if (c.dim == 3) {
+    h->ysx = Ly * h->nzp;
+    h->zsy = Lz;
+    h->zsx = (ny + 1) * Lz;
+    const size_t bx = Lx * h->sx * sizeof(T), by = (nx + 1) * h->ysx * sizeof(T), bz = (nx + 1) * h->zsx * sizeof(T);
+    const size_t sz[12] = {bx, bx, by, by, bz, bz, bx, bx, by, by, bz, bz};
+    for (int q = 0; q < 12; ++q)
+      if ((rc = alloc(h, &h->psi[q], sz[q], true))) return rc;
+    if (fused(h))
+      for (int q = 0; q < 6; ++q)
+        if ((rc = alloc(h, &h->psi_h1[q], sz[6 + q], true))) return rc;
+  } else {
+    h->ysx = Ly;
+    const size_t bx = Lx * h->sx * sizeof(T), by = (nx + 1) * Ly * sizeof(T);
+    if ((rc = alloc(h, &h->psi[1], bx, true))) return rc;   // ez_x
+    if ((rc = alloc(h, &h->psi[2], by, true))) return rc;   // ez_y
+    if ((rc = alloc(h, &h->psi[6], bx, true))) return rc;   // hy_x
+    if ((rc = alloc(h, &h->psi[9], by, true))) return rc;   // hx_y
+  }
+  // TFSF
+  if (c.tfsf_on) {
+    for (int a = 0; a < 3; ++a) {
+      void* p;
+      if ((rc = upload<double>(h, &p, c.proj_int[a]))) return rc;
+      h->proj[a] = static_cast<double*>(p);
+      if ((rc = upload<double>(h, &p, c.proj_half[a]))) return rc;
+      h->proj[3 + a] = static_cast<double*>(p);
+    }
+    void* p;
+    if ((rc = alloc(h, &p, 2 * (c.aux_nl + 1) * sizeof(double), true))) return rc;
+    h->e_aux = static_cast<double*>(p);
+    if ((rc = alloc(h, &p, c.aux_nl * sizeof(double), true))) return rc;
+    h->h_aux = static_cast<double*>(p);
+    if ((rc = upload<double>(h, &p, c.aux_source))) return rc;
+    h->src = static_cast<double*>(p);
+  }
+  // ADE
+  if (c.ade_kind != XFB_ADE_NONE) {
+    if ((rc = upload<T>(h, &h->ade_mat, c.ade_mat))) return rc;
+    if ((rc = upload<T>(h, &h->ade_pole, c.ade_pole))) return rc;
+    const int* b = c.ade_box;
+    const long long bk = roundup(std::max(1, b[5] - b[4]), 32);
+    h->bsy = bk;
+    h->bsx = std::max(1, b[3] - b[2]) * bk;
+    h->bn = std::max(1, b[1] - b[0]) * h->bsx;
+    const int P = std::max(1, c.ade_poles);
+    if ((rc = alloc(h, &h->J, 3 * P * h->bn * sizeof(T), true))) return rc;
+    if (c.ade_kind == XFB_ADE_MLORENTZ) {
+      if ((rc = alloc(h, &h->Jp, 3 * P * h->bn * sizeof(T), true))) return rc;
+      if ((rc = alloc(h, &h->Ep, 3 * h->bn * sizeof(T), true))) return rc;
+    }
+  }
+  // NF2FF
+  if (c.nf_on) {
+    h->nf_off[0] = 0;
+    for (int f = 0; f < 6; ++f) h->nf_off[f + 1] = h->nf_off[f] + nf_face_points(c, f);
+    h->nf_npts = h->nf_off[6];
+    const size_t nfq = c.freqs.size();
+    void* p;
+    if ((rc = alloc(h, &p, nfq * 4 * h->nf_npts * sizeof(double2), true))) return rc;
+    h->nf_acc = static_cast<double2*>(p);
+    if ((rc = upload<double>(h, &p, c.te))) return rc;
+    h->te = static_cast<double2*>(p);
+    if ((rc = upload<double>(h, &p, c.th))) return rc;
+    h->th = static_cast<double2*>(p);
+  }
+  // probes
+  if (!c.probes.empty()) {
+    const size_t n = c.probes.size();
+    std::vector<long long> idx(n);
+    std::vector<int> fld(n);
+    for (size_t p = 0; p < n; ++p) {
+      idx[p] = off3(h, c.probes[p].index[0], c.probes[p].index[1], c.dim == 3 ? c.probes[p].index[2] : 0);
+      fld[p] = c.probes[p].field;
+    }
+    void* p;
+    if ((rc = alloc(h, &p, n * sizeof(long long), false))) return rc;
+    h->probe_idx = static_cast<long long*>(p);
+    XFB_CUDA(h, cudaMemcpy(p, idx.data(), n * sizeof(long long), cudaMemcpyHostToDevice));
+    if ((rc = alloc(h, &p, n * sizeof(int), false))) return rc;
+    h->probe_field = static_cast<int*>(p);
+    XFB_CUDA(h, cudaMemcpy(p, fld.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    if ((rc = alloc(h, &p, n * std::max(1LL, c.total_steps) * sizeof(double), true))) return rc;
+    h->probe_out = static_cast<double*>(p);
+  }
+  // movies
+  for (const xfb_movie& mv : c.movies) {
+    const long long frames = (c.total_steps + mv.interval - 1) / mv.interval;
+    const long long per = static_cast<long long>(mv.hi[0] - mv.lo[0]) * (mv.hi[1] - mv.lo[1]) * (mv.hi[2] - mv.lo[2]);
+    void* p;
+    if ((rc = alloc(h, &p, std::max(1LL, frames) * per * sizeof(double), true))) return rc;
+    h->movie_out.push_back(static_cast<double*>(p));
+    h->movie_frames.push_back(frames);
+  }
+  void* p;
+  if ((rc = alloc(h, &p, sizeof(long long), true))) return rc;
+  h->t_dev = static_cast<long long*>(p);
+  if ((rc = alloc(h, &p, sizeof(unsigned long long), false))) return rc;
+  h->scratch_u64 = static_cast<unsigned long long*>(p);
+  XFB_CUDA(h, cudaStreamSynchronize(h->stream));
+  return XFB_OK;
+}
+
+// ---------------------------------------------------------------------------
+template <typename T>
+GridP<T> grid_params(xfb_handle* h, int set = 0) {
+  GridP<T> g;
+  g.nx = h->c.nx; g.ny = h->c.ny; g.nz = h->c.nz;
+  g.sx = h->sx; g.sy = h->sy;
+  void* const* f = set ? h->f1 : h->f;
+  g.ex = as<T>(f[0]); g.ey = as<T>(f[1]); g.ez = as<T>(f[2]);
+  g.hx = as<T>(f[3]); g.hy = as<T>(f[4]); g.hz = as<T>(f[5]);
+  g.mid = h->mid;
+  g.lut = as<const T>(h->lut);
+  return g;
+}
+
+template <typename T>
+PmlP<T> pml_params(xfb_handle* h) {
+  PmlP<T> p;
+  for (int q = 0; q < 6; ++q) p.L[q] = h->c.pml[q];
+  for (int a = 0; a < 3; ++a) {
+    p.ae[a] = as<const T>(h->prof[a]); p.be[a] = as<const T>(h->prof[3 + a]);
+    p.ah[a] = as<const T>(h->prof[6 + a]); p.bh[a] = as<const T>(h->prof[9 + a]);
+  }
+  T** ps[12] = {&p.ey_x, &p.ez_x, &p.ez_y, &p.ex_y, &p.ex_z, &p.ey_z, &p.hy_x, &p.hz_x, &p.hz_y, &p.hx_y, &p.hx_z, &p.hy_z};
+  for (int q = 0; q < 12; ++q) *ps[q] = as<T>(h->psi[q]);
+  p.ysx = h->ysx; p.zsx = h->zsx; p.zsy = h->zsy;
+  return p;
+}
+
+inline TfsfP tfsf_params(xfb_handle* h) {
+  TfsfP t{};
+  const Compiled& c = h->c;
+  t.on = c.tfsf_on;
+  if (!t.on) return t;
+  t.is = c.tf[0]; t.ie = c.tf[1]; t.js = c.tf[2]; t.je = c.tf[3]; t.ks = c.tf[4]; t.ke = c.tf[5];
+  t.pi0 = h->proj[0]; t.pi1 = h->proj[1]; t.pi2 = h->proj[2];
+  t.ph0 = h->proj[3]; t.ph1 = h->proj[4]; t.ph2 = h->proj[5];
+  for (int a = 0; a < 3; ++a) { t.tre[a] = c.tr_e[a]; t.trh[a] = c.tr_h[a]; t.ca[a] = c.ca[a]; t.cb[a] = c.cb[a]; }
+  t.e_aux0 = h->e_aux; t.e_aux1 = h->e_aux + (c.aux_nl + 1); t.h_aux = h->h_aux; t.e_aux = nullptr;
+  return t;
+}
+
+template <typename T>
+AdeP<T> ade_params(xfb_handle* h) {
+  AdeP<T> a{};
+  const Compiled& c = h->c;
+  a.kind = c.ade_kind;
+  if (a.kind == XFB_ADE_NONE) return a;
+  a.P = c.ade_poles;
+  a.b0 = c.ade_box[0]; a.b1 = c.ade_box[1]; a.b2 = c.ade_box[2]; a.b3 = c.ade_box[3]; a.b4 = c.ade_box[4]; a.b5 = c.ade_box[5];
+  a.bsx = h->bsx; a.bsy = h->bsy; a.bn = h->bn;
+  a.mat = as<const T>(h->ade_mat); a.pole = as<const T>(h->ade_pole);
+  a.J = as<T>(h->J); a.Jp = as<T>(h->Jp); a.Ep = as<T>(h->Ep);
+  return a;
+}
+
+inline int chunks_for(int tiles, int n_march, int threads) {
+  const int resident = 148 * std::max(1, 2048 / threads);
+  int ch = (4 * resident + tiles - 1) / std::max(1, tiles);
+  ch = std::min(ch, std::max(1, n_march / 8));
+  return std::max(1, ch);
+}
+
+// Optional per-launch CUDA-event bracketing (profile mode only).
+struct Prof {
+  cudaEvent_t ev[2 * 16];
+  int cls[16];
+  int n = 0;
+};
+
+inline void prof_begin(xfb_handle* h, Prof* p, int cls) {
+  if (!p) return;
+  p->cls[p->n] = cls;
+  cudaEventRecord(p->ev[2 * p->n], h->stream);
+}
+inline void prof_end(xfb_handle* h, Prof* p) {
+  if (!p) return;
+  cudaEventRecord(p->ev[2 * p->n + 1], h->stream);
+  ++p->n;
+}
+
+// Largest j-row count of a (32 x tj) tile that every bulk kernel of type T
+// can launch with (register budget of the compiled kernels).
+template <typename T>
+int tile_rows(xfb_handle* h) {
+  int lim = 1024;
+  cudaFuncAttributes a;
+  if (h->c.dim == 3) {
+    if (cudaFuncGetAttributes(&a, k_h3<T>) == cudaSuccess) lim = std::min(lim, a.maxThreadsPerBlock);
+    if (cudaFuncGetAttributes(&a, k_e3<T>) == cudaSuccess) lim = std::min(lim, a.maxThreadsPerBlock);
+  }
+  int tj = std::max(1, std::min(h->tj, lim / h->tk));
+  int p = 1;
+  while (p * 2 <= tj) p *= 2;
+  return p;
+}
+
+template <typename T>
+PsiH<T> psi_h_set(xfb_handle* h, int set) {
+  void* const* q = set ? h->psi_h1 : h->psi + 6;
+  return PsiH<T>{as<T>(q[0]), as<T>(q[1]), as<T>(q[2]), as<T>(q[3]), as<T>(q[4]), as<T>(q[5])};
+}
+
+template <typename T, int TJ>
+void launch_fused(xfb_handle* h, int parity, TimeP tp, cudaStream_t st) {
+  using S = StepSmem<T, 32, TJ>;
+  const Compiled& c = h->c;
+  const int gx = (c.nz + 31) / 32, gy = (c.ny + TJ - 1) / TJ;
+  const int nch = chunks_for(gx * gy, c.nx, S::threads);
+  const int ich = (c.nx + nch - 1) / nch;
+  dim3 grd(gx, gy, (c.nx + ich - 1) / ich);
+  static bool attr_set = false;  // per instantiation; the attribute is per-function, per-device
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_step3<T, 32, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::bytes));
+    attr_set = true;
+  }
+  k_step3<T, 32, TJ><<<grd, S::threads, S::bytes, st>>>(grid_params<T>(h, parity), grid_params<T>(h, 1 - parity), pml_params<T>(h),
+                                             psi_h_set<T>(h, parity), psi_h_set<T>(h, 1 - parity), tfsf_params(h),
+                                             ade_params<T>(h), tp, ich, as<const T>(h->lut8), h->mat_disp, c.n_mat);
+}
+
+template <typename T>
+void enqueue_step(xfb_handle* h, int off, Prof* pf = nullptr) {
+  const Compiled& c = h->c;
+  TimeP tp{h->t_dev, off};
+  const int parity = static_cast<int>((h->step + off) & 1);
+  // fields after this step: the written set (one-sweep) or the only set (split)
+  GridP<T> g = grid_params<T>(h, fused(h) ? 1 - parity : 0);
+  PmlP<T> pm = pml_params<T>(h);
+  TfsfP tf = tfsf_params(h);
+  cudaStream_t s = h->stream;
+  if (fused(h)) {
+    if (c.tfsf_on) {
+      prof_begin(h, pf, XFB_K_AUX);
+      k_aux<<<1, 1024, 0, s>>>(h->e_aux, h->e_aux + (c.aux_nl + 1), h->h_aux, c.aux_nl, c.aux_ceih, c.aux_chie,
+                               c.aux_abc, h->src, tp);
+      prof_end(h, pf);
+    }
+    prof_begin(h, pf, XFB_K_STEP);
+    const int tj = h->tj;
+    if (tj <= 4) launch_fused<T, 4>(h, parity, tp, s);
+    else if (tj <= 8) launch_fused<T, 8>(h, parity, tp, s);
+    else launch_fused<T, 16>(h, parity, tp, s);
+    prof_end(h, pf);
+  } else if (c.dim == 3) {
+    const int tj = tile_rows<T>(h);
+    dim3 blk(h->tk, tj);
+    const int gx = (c.nz + h->tk - 1) / h->tk, gy = (c.ny + tj - 1) / tj;
+    const int nch = chunks_for(gx * gy, c.nx, h->tk * tj);
+    const int ich = (c.nx + nch - 1) / nch;
+    dim3 grd(gx, gy, (c.nx + ich - 1) / ich);
+    prof_begin(h, pf, XFB_K_UPDATE_H);
+    k_h3<T><<<grd, blk, 0, s>>>(g, pm, tf, tp, ich);
+    prof_end(h, pf);
+    if (c.tfsf_on) {
+      prof_begin(h, pf, XFB_K_AUX);
+      k_aux<<<1, 1024, 0, s>>>(h->e_aux, h->e_aux + (c.aux_nl + 1), h->h_aux, c.aux_nl, c.aux_ceih, c.aux_chie, c.aux_abc, h->src, tp);
+      prof_end(h, pf);
+    }
+    prof_begin(h, pf, XFB_K_UPDATE_E);
+    k_e3<T><<<grd, blk, 0, s>>>(g, pm, tf, ade_params<T>(h), tp, ich);
+    prof_end(h, pf);
+  } else {
+    const int bx = 128;
+    const int gx = (c.ny + bx - 1) / bx;
+    const int nch = chunks_for(gx, c.nx, bx);
+    const int ich = (c.nx + nch - 1) / nch;
+    dim3 grd(gx, (c.nx + ich - 1) / ich);
+    prof_begin(h, pf, XFB_K_UPDATE_H);
+    k_h2<T><<<grd, bx, 0, s>>>(g, pm, tf, tp, ich);
+    prof_end(h, pf);
+    if (c.tfsf_on) {
+      prof_begin(h, pf, XFB_K_AUX);
+      k_aux<<<1, 1024, 0, s>>>(h->e_aux, h->e_aux + (c.aux_nl + 1), h->h_aux, c.aux_nl, c.aux_ceih, c.aux_chie, c.aux_abc, h->src, tp);
+      prof_end(h, pf);
+    }
+    prof_begin(h, pf, XFB_K_UPDATE_E);
+    k_e2<T><<<grd, bx, 0, s>>>(g, pm, tf, tp, ich);
+    prof_end(h, pf);
+  }
+  if (c.nf_on) {
+    NfP nf{};
+    nf.nfreq = static_cast<int>(c.freqs.size());
+    for (int q = 0; q < 6; ++q) nf.box[q] = c.nf[q];
+    for (int q = 0; q < 7; ++q) nf.off[q] = h->nf_off[q];
+    nf.npts = h->nf_npts;
+    nf.acc = h->nf_acc; nf.te = h->te; nf.th = h->th;
+    nf.total_steps = c.total_steps;
+    prof_begin(h, pf, XFB_K_NF2FF);
+    k_nf2ff<T><<<static_cast<unsigned>((h->nf_npts + 255) / 256), 256, 0, s>>>(g, nf, tp);
+    prof_end(h, pf);
+  }
+  if (!c.probes.empty()) {
+    ProbeP pr{static_cast<int>(c.probes.size()), h->probe_idx, h->probe_field, h->probe_out, c.total_steps};
+    prof_begin(h, pf, XFB_K_PROBE);
+    k_probe<T><<<(pr.n + 127) / 128, 128, 0, s>>>(g, pr, tp);
+    prof_end(h, pf);
+  }
+  for (size_t m = 0; m < c.movies.size(); ++m) {
+    const xfb_movie& mv = c.movies[m];
+    const int n0 = mv.hi[0] - mv.lo[0], n1 = mv.hi[1] - mv.lo[1], n2 = mv.hi[2] - mv.lo[2];
+    const long long per = static_cast<long long>(n0) * n1 * n2;
+    const int blocks = static_cast<int>(std::min<long long>((per + 255) / 256, 1024));
+    prof_begin(h, pf, XFB_K_MOVIE);
+    k_movie<T><<<blocks, 256, 0, s>>>(as<const T>(field_ptr(h, fused(h) ? 1 - parity : 0, mv.field)), h->sx, h->sy, mv.lo[0], mv.lo[1], mv.lo[2], n0, n1, n2,
+                                      mv.interval, h->movie_out[m], h->movie_frames[m], tp);
+    prof_end(h, pf);
+  }
+}
+
+template <typename T>
+void enqueue_chunk(xfb_handle* h, int n) {
+  for (int s = 0; s < n; ++s) enqueue_step<T>(h, s);
+  k_bump<<<1, 1, 0, h->stream>>>(h->t_dev, n);
+}
+
+template <typename T>
+int run_steps(xfb_handle* h, long long n) {
+  long long left = n;
+  while (left > 0) {
+    const int chunk = static_cast<int>(std::min<long long>(left, h->graph_steps));
+    if (h->graph_on) {
+      const int key = chunk * 2 + static_cast<int>(h->step & 1);
+      auto it = h->graphs.find(key);
+      if (it == h->graphs.end()) {
+        cudaGraph_t graph;
+        XFB_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        enqueue_chunk<T>(h, chunk);
+        XFB_CUDA(h, cudaStreamEndCapture(h->stream, &graph));
+        cudaGraphExec_t ex;
+        cudaError_t e = cudaGraphInstantiate(&ex, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return cuda_err(h, e, "cudaGraphInstantiate");
+        it = h->graphs.emplace(key, ex).first;
+      }
+      XFB_CUDA(h, cudaGraphLaunch(it->second, h->stream));
+    } else {
+      enqueue_chunk<T>(h, chunk);
+      XFB_CUDA(h, cudaGetLastError());
+    }
+    left -= chunk;
+    h->step += chunk;
+  }
+  return XFB_OK;
+}
+
+template <typename T>
+int profile_steps(xfb_handle* h, long long n, double* ms, long long* launches) {
+  for (int q = 0; q < XFB_K_COUNT; ++q) { ms[q] = 0; launches[q] = 0; }
+  Prof pf;
+  for (int e = 0; e < 32; ++e) XFB_CUDA(h, cudaEventCreate(&pf.ev[e]));
+  int rc = XFB_OK;
+  for (long long q = 0; q < n && rc == XFB_OK; ++q) {
+    pf.n = 0;
+    enqueue_step<T>(h, 0, &pf);
+    k_bump<<<1, 1, 0, h->stream>>>(h->t_dev, 1);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) { rc = cuda_err(h, e, "profile step"); break; }
+    for (int k = 0; k < pf.n; ++k) {
+      float t = 0;
+      cudaEventElapsedTime(&t, pf.ev[2 * k], pf.ev[2 * k + 1]);
+      ms[pf.cls[k]] += t;
+      launches[pf.cls[k]] += 1;
+    }
+    h->step += 1;
+  }
+  for (int e = 0; e < 32; ++e) cudaEventDestroy(pf.ev[e]);
+  return rc;
+}
+
+
+
+template <typename T>
+int read_field_t(xfb_handle* h, int f, double* dst) {
+  std::vector<T> tmp(static_cast<size_t>(h->elems));
+  XFB_CUDA(h, cudaStreamSynchronize(h->stream));
+  XFB_CUDA(h, cudaMemcpy(tmp.data(), field_ptr(h, cur_set(h), f), tmp.size() * sizeof(T), cudaMemcpyDeviceToHost));
+  int s[3];
+  comp_shape(h->c, f, s);
+  size_t o = 0;
+  for (int i = 0; i < s[0]; ++i)
+    for (int j = 0; j < s[1]; ++j)
+      for (int k = 0; k < s[2]; ++k) dst[o++] = static_cast<double>(tmp[off3(h, i, j, k)]);
+  return XFB_OK;
+}
+
+template <typename T>
+int write_field_t(xfb_handle* h, int f, const double* src) {
+  std::vector<T> tmp(static_cast<size_t>(h->elems));
+  XFB_CUDA(h, cudaStreamSynchronize(h->stream));
+  XFB_CUDA(h, cudaMemcpy(tmp.data(), field_ptr(h, cur_set(h), f), tmp.size() * sizeof(T), cudaMemcpyDeviceToHost));
+  int s[3];
+  comp_shape(h->c, f, s);
+  size_t o = 0;
+  for (int i = 0; i < s[0]; ++i)
+    for (int j = 0; j < s[1]; ++j)
+      for (int k = 0; k < s[2]; ++k) tmp[off3(h, i, j, k)] = static_cast<T>(src[o++]);
+  // both sets: entries the update never writes (PEC walls, unused slots) must
+  // agree in the two ping-pong buffers
+  XFB_CUDA(h, cudaMemcpy(h->f[f], tmp.data(), tmp.size() * sizeof(T), cudaMemcpyHostToDevice));
+  if (fused(h)) XFB_CUDA(h, cudaMemcpy(h->f1[f], tmp.data(), tmp.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return XFB_OK;
+}
+
+template <typename T>
+void launch_nonfinite(xfb_handle* h) {
+  for (int q = 0; q < 6; ++q) {
+    if (!h->f[q]) continue;
+    const T* fp = static_cast<const T*>(field_ptr(h, cur_set(h), q));
+    k_nonfinite<T><<<592, 256, 0, h->stream>>>(fp, h->elems, h->scratch_u64);
+  }
+}
+
+}  // namespace xfb
+
+#define XFB_INSTANTIATE_ENGINE(T)                                                          \
+  namespace xfb {                                                                          \
+  template int init_device<T>(xfb_handle*);                                                \
+  template int run_steps<T>(xfb_handle*, long long);                                       \
+  template int profile_steps<T>(xfb_handle*, long long, double*, long long*);              \
+  template int read_field_t<T>(xfb_handle*, int, double*);                                 \
+  template int write_field_t<T>(xfb_handle*, int, const double*);                          \
+  template void launch_nonfinite<T>(xfb_handle*);                                          \
+  }

@@ -1,0 +1,124 @@
+// Engine handle shared by the C-ABI (api.cu) and the per-precision engine
+// translation units (engine_f32.cu, engine_f64.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "xfb_internal.h"
+
+namespace xfb {
+struct Buf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  bool state = false;  // part of the checkpoint state
+};
+
+}  // namespace xfb
+
+struct xfb_handle {
+  using Buf = xfb::Buf;
+  xfb::Compiled c;
+  std::string err;
+  int device = -1;
+  cudaStream_t stream = nullptr;
+  bool inited = false;
+  long long step = 0;
+  unsigned hint_grid[3] = {1, 1, 1}, hint_block[3] = {1, 1, 1};
+  int tk = 32, tj = 8;
+  int path = XFB_PATH_AUTO;  // resolved at init: XFB_PATH_SPLIT or XFB_PATH_FUSED
+  int graph_on = 1, graph_steps = 64;
+  std::map<int, cudaGraphExec_t> graphs;
+  std::vector<Buf> bufs;
+  size_t bytes = 0;
+  int esize = 4;
+  // field layout
+  long long sx = 0, sy = 0, nzp = 0, elems = 0, guard = 0;
+  void* f[6] = {};    // field set 0
+  void* f1[6] = {};   // field set 1 (one-sweep path: step t reads set t&1, writes the other)
+  uint8_t* mid = nullptr;
+  void* lut8 = nullptr;       // [n_mat][8] compact coefficients (one-sweep path)
+  uint8_t* mat_disp = nullptr;
+  void* lut = nullptr;
+  // CPML
+  void* prof[12] = {};  // ae0 ae1 ae2 be0 be1 be2 ah0 ah1 ah2 bh0 bh1 bh2
+  void* psi[12] = {};   // ey_x ez_x ez_y ex_y ex_z ey_z hy_x hz_x hz_y hx_y hx_z hy_z
+  void* psi_h1[6] = {}; // H-side psi of field set 1 (one-sweep path)
+  long long ysx = 0, zsx = 0, zsy = 0;
+  // TFSF
+  double* proj[6] = {};
+  double* e_aux = nullptr;   // [2][nl+1] by step parity
+  double* h_aux = nullptr;
+  double* src = nullptr;
+  // ADE
+  void* ade_mat = nullptr;
+  void* ade_pole = nullptr;
+  void* J = nullptr;
+  void* Jp = nullptr;
+  void* Ep = nullptr;
+  long long bsx = 0, bsy = 0, bn = 0;
+  // NF2FF
+  double2* nf_acc = nullptr;
+  double2* te = nullptr;
+  double2* th = nullptr;
+  int nf_off[7] = {};
+  long long nf_npts = 0;
+  // monitors
+  long long* probe_idx = nullptr;
+  int* probe_field = nullptr;
+  double* probe_out = nullptr;
+  std::vector<double*> movie_out;
+  std::vector<long long> movie_frames;
+  long long* t_dev = nullptr;
+  unsigned long long* scratch_u64 = nullptr;
+};
+
+namespace xfb {
+
+// ---- helpers (api.cu) ----------------------------------------------------
+int set_err(xfb_handle* h, int code, const std::string& m);
+int cuda_err(xfb_handle* h, cudaError_t e, const char* what);
+
+#define XFB_CUDA(h, call)                                   \
+  do {                                                      \
+    cudaError_t e_ = (call);                                \
+    if (e_ != cudaSuccess) return cuda_err((h), e_, #call); \
+  } while (0)
+
+template <typename T>
+T* as(void* p) { return static_cast<T*>(p); }
+
+void free_device(xfb_handle* h);
+int alloc(xfb_handle* h, void** out, size_t bytes, bool state);
+
+template <typename T>
+int upload(xfb_handle* h, void** out, const std::vector<double>& v, bool state = false) {
+  std::vector<T> tmp(v.begin(), v.end());
+  int rc = alloc(h, out, tmp.size() * sizeof(T), state);
+  if (rc) return rc;
+  if (!tmp.empty()) XFB_CUDA(h, cudaMemcpy(*out, tmp.data(), tmp.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return XFB_OK;
+}
+
+long long roundup(long long v, long long m);
+bool fused(const xfb_handle* h);
+int cur_set(const xfb_handle* h);
+void* field_ptr(const xfb_handle* h, int set, int q);
+long long off3(const xfb_handle* h, int i, int j, int k);
+void comp_shape(const Compiled& c, int f, int s[3]);
+int nf_face_points(const Compiled& c, int face);
+int launches_per_step(const xfb_handle* h);
+int check_handle(xfb_handle* h, bool need_init);
+
+// ---- engine (engine.cuh, instantiated for float and double) -------------
+template <typename T> int init_device(xfb_handle* h);
+template <typename T> int run_steps(xfb_handle* h, long long n);
+template <typename T> int profile_steps(xfb_handle* h, long long n, double* ms, long long* launches);
+template <typename T> int read_field_t(xfb_handle* h, int f, double* dst);
+template <typename T> int write_field_t(xfb_handle* h, int f, const double* src);
+template <typename T> void launch_nonfinite(xfb_handle* h);
+
+}  // namespace xfb

@@ -55,9 +55,17 @@ struct TfsfP {
   const double* pi0; const double* pi1; const double* pi2;  // projections at nodes
   const double* ph0; const double* ph1; const double* ph2;  // projections at half nodes
   double tre[3], trh[3], ca[3], cb[3];
-  double* e_aux;  // [nl+1]  E incident at time t*dt
-  double* h_aux;  // [nl]    H incident at (t+1/2)*dt
+  double* e_aux0;  // [nl+1] E incident at t*dt for even t (double buffer by step parity)
+  double* e_aux1;  // [nl+1] ... for odd t
+  double* h_aux;   // [nl]   H incident at (t+1/2)*dt (valid after k_aux of step t)
+  const double* e_aux;  // resolved by tfsf_at_step: E buffer of the current step
 };
+
+// Resolve the auxiliary E buffer that holds E_inc at time t*dt.
+__device__ __forceinline__ TfsfP tfsf_at_step(TfsfP s, long long t) {
+  s.e_aux = (t & 1) ? s.e_aux1 : s.e_aux0;
+  return s;
+}
 
 template <typename T>
 struct AdeP {
@@ -130,7 +138,8 @@ __device__ __forceinline__ int slab(int q, int n, int Ln, int Lp) {
 // registers to the next plane, so every E element is fetched from memory once
 // per plane; k and j neighbours come from lines the block already holds in L1.
 template <typename T>
-__global__ void k_h3(GridP<T> g, PmlP<T> pm, TfsfP tf, TimeP tp, int i_chunk) {
+__global__ void k_h3(GridP<T> g, PmlP<T> pm, TfsfP tf_in, TimeP tp, int i_chunk) {
+  const TfsfP tf = tfsf_at_step(tf_in, cur_step(tp));
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (k >= g.nz || j >= g.ny) return;
@@ -274,6 +283,71 @@ __device__ __forceinline__ T ade_e(const AdeP<T>& a, int comp, long long bi, int
   return e_new;
 }
 
+// ADE state of one cell held in registers (up to kAdeRegPoles poles), so its
+// loads can be issued well before the E update that consumes them.
+constexpr int kAdeRegPoles = 2;
+template <typename T>
+struct AdeRegs {
+  T J[3][kAdeRegPoles], Jp[3][kAdeRegPoles], Ep[3];
+};
+
+template <typename T>
+__device__ __forceinline__ void ade_load(const AdeP<T>& a, long long bi, bool upd_x, bool upd_y, bool upd_z, AdeRegs<T>& r) {
+  const bool upd[3] = {upd_x, upd_y, upd_z};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    if (!upd[c]) continue;
+#pragma unroll
+    for (int p = 0; p < kAdeRegPoles; ++p)
+      if (p < a.P) {
+        r.J[c][p] = a.J[(static_cast<long long>(c) * a.P + p) * a.bn + bi];
+        if (a.kind == kAdeMLorentz) r.Jp[c][p] = a.Jp[(static_cast<long long>(c) * a.P + p) * a.bn + bi];
+      }
+    if (a.kind == kAdeMLorentz) r.Ep[c] = a.Ep[static_cast<long long>(c) * a.bn + bi];
+  }
+}
+
+// ade_e on register-held state (same arithmetic and order); stores the new state.
+template <typename T>
+__device__ __forceinline__ T ade_e_reg(const AdeP<T>& a, int comp, long long bi, int m, T e_cur, T plain,
+                                       const AdeRegs<T>& r) {
+  const T* am = a.mat + 3 * m;
+  const T* ap = a.pole + static_cast<long long>(m) * a.P * 7;
+  T* J = a.J + static_cast<long long>(comp) * a.P * a.bn + bi;
+  if (a.kind == kAdeMLorentz) {
+    T* Jp = a.Jp + static_cast<long long>(comp) * a.P * a.bn + bi;
+    T jsum = 0;
+#pragma unroll
+    for (int p = 0; p < kAdeRegPoles; ++p)
+      if (p < a.P) jsum = jsum + (ap[7 * p + 5] * r.J[comp][p] + ap[7 * p + 6] * r.Jp[comp][p]);
+    const T e_prev = r.Ep[comp];
+    const T e_new = am[1] * e_prev + plain + am[2] * jsum;
+#pragma unroll
+    for (int p = 0; p < kAdeRegPoles; ++p)
+      if (p < a.P) {
+        const T* q = ap + 7 * p;
+        const T jn = q[2] * e_new + q[3] * e_cur + q[4] * e_prev + q[0] * r.J[comp][p] + q[1] * r.Jp[comp][p];
+        Jp[p * a.bn] = r.J[comp][p];
+        J[p * a.bn] = jn;
+      }
+    a.Ep[static_cast<long long>(comp) * a.bn + bi] = e_cur;
+    return e_new;
+  }
+  T jsum = 0;
+#pragma unroll
+  for (int p = 0; p < kAdeRegPoles; ++p)
+    if (p < a.P) jsum = jsum + ap[7 * p + 5] * r.J[comp][p];
+  const T e_new = plain + am[2] * jsum;
+#pragma unroll
+  for (int p = 0; p < kAdeRegPoles; ++p)
+    if (p < a.P) {
+      const T* q = ap + 7 * p;
+      J[p * a.bn] = (a.kind == kAdeDrude) ? q[0] * r.J[comp][p] + q[3] * (e_new + e_cur)
+                                          : q[0] * r.J[comp][p] + q[3] * (e_new - e_cur);
+    }
+  return e_new;
+}
+
 // E half-step, 3-D.  Same tiling as k_h3; H values of plane i are carried to
 // plane i+1 as its i-1 neighbours.
 template <typename T>
@@ -407,7 +481,8 @@ __global__ void k_e3(GridP<T> g, PmlP<T> pm, TfsfP tf, AdeP<T> ad, TimeP tp, int
 // basic_updator_te.cu:9-20 with the 2-D TFSF agency, tfsf_corrector.cu:155-189).
 // Fields: Ez (nx+1, ny+1), Hx (nx+1, ny), Hy (nx, ny+1); idx = i*sx + j.
 template <typename T>
-__global__ void k_h2(GridP<T> g, PmlP<T> pm, TfsfP tf, TimeP tp, int i_chunk) {
+__global__ void k_h2(GridP<T> g, PmlP<T> pm, TfsfP tf_in, TimeP tp, int i_chunk) {
+  const TfsfP tf = tfsf_at_step(tf_in, cur_step(tp));
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= g.ny) return;
   const int i0 = blockIdx.y * i_chunk;
@@ -508,19 +583,22 @@ __global__ void k_e2(GridP<T> g, PmlP<T> pm, TfsfP tf, TimeP tp, int i_chunk) {
 // TFSF 1-D auxiliary grid, one time step (single block).  Before: e = E^t,
 // h = H^{t-1/2}; after: h = H^{t+1/2}, e = E^{t+1} with the source at node 0
 // and a first-order Mur boundary at node nl.
-__global__ void k_aux(double* e, double* h, int nl, double ceih, double chie, double abc, const double* src, TimeP tp) {
+// E^t lives in e_buf[t & 1]; E^{t+1} is written to the other buffer so the
+// bulk kernels of step t can still read E^t after this kernel ran.
+static __global__ void k_aux(double* e0, double* e1, double* h, int nl, double ceih, double chie, double abc,
+                      const double* src, TimeP tp) {
   const long long t = cur_step(tp);
-  __shared__ double e_end[2];
-  if (threadIdx.x == 0) { e_end[0] = e[nl - 1]; e_end[1] = e[nl]; }
+  const double* e = (t & 1) ? e1 : e0;
+  double* en = (t & 1) ? e0 : e1;
   for (int l = threadIdx.x; l < nl; l += blockDim.x) h[l] = h[l] + chie * (e[l + 1] - e[l]);
   __syncthreads();
-  for (int l = threadIdx.x + 1; l < nl; l += blockDim.x) e[l] = e[l] + ceih * (h[l] - h[l - 1]);
-  if (threadIdx.x == 0) e[0] = src[t + 1];
+  for (int l = threadIdx.x + 1; l < nl; l += blockDim.x) en[l] = e[l] + ceih * (h[l] - h[l - 1]);
+  if (threadIdx.x == 0) en[0] = src[t + 1];
   __syncthreads();
-  if (threadIdx.x == 0) e[nl] = e_end[0] + abc * (e[nl - 1] - e_end[1]);
+  if (threadIdx.x == 0) en[nl] = e[nl - 1] + abc * (en[nl - 1] - e[nl]);
 }
 
-__global__ void k_bump(long long* t, int n) { *t += n; }
+static __global__ void k_bump(long long* t, int n) { *t += n; }
 
 // ---------------------------------------------------------------------------
 // NF2FF frequency-domain accumulation: one thread per face point, all faces and
@@ -643,7 +721,7 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-__global__ void k_far(FarP fp) {
+static __global__ void k_far(FarP fp) {
   const int a = blockIdx.x;
   const double th = fp.theta[a], ph = fp.phi[a];
   const double st = sin(th), ct = cos(th), sp = sin(ph), cp = cos(ph);

@@ -165,6 +165,8 @@ int compile_scene(const xfb_scene& s, Compiled& c, std::string* err) {
   // ---- materials: Yee coefficients + ADE ---------------------------------
   c.n_mat = s.n_materials;
   c.coeff.assign(static_cast<size_t>(c.n_mat) * kCoeffs, 0.0);
+  c.coeff8.assign(static_cast<size_t>(c.n_mat) * 8, 0.0);
+  c.mat_disp.assign(c.n_mat, 0);
   c.mat_is_pec.assign(c.n_mat, 0);
   // ADE kind of the whole scene (the reference selects one updator for the
   // whole grid by the storage type: src/simulation/simulation_hd.cu:464-503).
@@ -268,6 +270,10 @@ int compile_scene(const xfb_scene& s, Compiled& c, std::string* err) {
     k[CHXH] = ch; k[CHXEY] = db / s.dz; k[CHXEZ] = -db / s.dy;
     k[CHYH] = ch; k[CHYEZ] = db / s.dx; k[CHYEX] = -db / s.dz;
     k[CHZH] = ch; k[CHZEX] = db / s.dy; k[CHZEY] = -db / s.dx;
+    double* k8 = &c.coeff8[static_cast<size_t>(m) * 8];
+    k8[0] = ce; k8[1] = cbv / s.dx; k8[2] = cbv / s.dy; k8[3] = cbv / s.dz;
+    k8[4] = ch; k8[5] = db / s.dx; k8[6] = db / s.dy; k8[7] = db / s.dz;
+    c.mat_disp[m] = c.ade_mat[static_cast<size_t>(m) * kAdeMat] != 0 ? 1 : 0;
   }
 
   // ---- voxelisation: material of the last object holding the cell centre --

@@ -37,6 +37,12 @@ struct Compiled {
   std::vector<uint8_t> mat_id;   // [nx][ny][nz]
   int n_mat = 0;
   std::vector<double> coeff;     // [n_mat][18]
+  // Compact form of the same coefficients: [n_mat][8] = ce, cb/dx, cb/dy, cb/dz,
+  // ch, db/dx, db/dy, db/dz.  Every entry of `coeff` is +- one of these values
+  // exactly (e.g. cexhy = -cb/dz), so kernels reading this form with the sign
+  // applied reproduce the 18-coefficient update bit for bit.
+  std::vector<double> coeff8;
+  std::vector<uint8_t> mat_disp; // [n_mat] 1 if the material has ADE poles
   std::vector<int> mat_is_pec;
   // ADE (dispersive media)
   int ade_kind = XFB_ADE_NONE, ade_poles = 0;

@@ -566,6 +566,9 @@ class Handle:
     def set_device(self, ordinal: int):
         self._c(self.lib.xfb_set_device(self.h, int(ordinal)))
 
+    def set_kernel_path(self, path: int):
+        self._c(self.lib.xfb_set_kernel_path(self.h, int(path)))
+
     def set_graph(self, enabled: bool, steps: int = 64):
         self._c(self.lib.xfb_set_graph(self.h, int(enabled), int(steps)))
 
