@@ -72,6 +72,13 @@ int alloc(xfb_handle* h, void** out, size_t bytes, bool state) {
 }
 
 
+int copy(xfb_handle* h, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind) {
+  if (bytes == 0) return XFB_OK;
+  XFB_CUDA(h, cudaMemcpyAsync(dst, src, bytes, kind, h->stream));
+  XFB_CUDA(h, cudaStreamSynchronize(h->stream));
+  return XFB_OK;
+}
+
 long long roundup(long long v, long long m) { return (v + m - 1) / m * m; }
 
 bool fused(const xfb_handle* h) { return h->path == XFB_PATH_FUSED; }
@@ -361,7 +368,7 @@ int xfb_read_probe(xfb_handle* h, int id, double* dst, size_t len, long long* n_
   const long long n = h->step;
   if (len < static_cast<size_t>(n)) return set_err(h, XFB_ERR_RANGE, "destination too small");
   XFB_CUDA(h, cudaStreamSynchronize(h->stream));
-  if (n > 0) XFB_CUDA(h, cudaMemcpy(dst, h->probe_out + id * h->c.total_steps, n * sizeof(double), cudaMemcpyDeviceToHost));
+  if (n > 0 && (rc = copy(h, dst, h->probe_out + id * h->c.total_steps, n * sizeof(double), cudaMemcpyDeviceToHost))) return rc;
   if (n_written) *n_written = n;
   return XFB_OK;
 }
@@ -383,7 +390,7 @@ int xfb_read_movie(xfb_handle* h, int id, double* dst, size_t len) {
   const size_t n = static_cast<size_t>(s[0]) * s[1] * s[2] * s[3];
   if (len < n) return set_err(h, XFB_ERR_RANGE, "destination too small");
   XFB_CUDA(h, cudaStreamSynchronize(h->stream));
-  if (n) XFB_CUDA(h, cudaMemcpy(dst, h->movie_out[id], n * sizeof(double), cudaMemcpyDeviceToHost));
+  if (n && (rc = copy(h, dst, h->movie_out[id], n * sizeof(double), cudaMemcpyDeviceToHost))) return rc;
   return XFB_OK;
 }
 
@@ -407,7 +414,7 @@ int xfb_read_nf2ff(xfb_handle* h, int freq, int face, int which, double* dst, si
   if (len < 2 * n) return set_err(h, XFB_ERR_RANGE, "destination too small (complex interleaved)");
   XFB_CUDA(h, cudaStreamSynchronize(h->stream));
   const double2* src = h->nf_acc + (static_cast<long long>(freq) * 4 + which) * h->nf_npts + h->nf_off[face];
-  XFB_CUDA(h, cudaMemcpy(dst, src, n * sizeof(double2), cudaMemcpyDeviceToHost));
+  if ((rc = copy(h, dst, src, n * sizeof(double2), cudaMemcpyDeviceToHost))) return rc;
   return XFB_OK;
 }
 
@@ -465,7 +472,7 @@ int xfb_get_state(xfb_handle* h, void* dst, size_t len) {
   o += sizeof(long long);
   for (const Buf& b : h->bufs)
     if (b.state) {
-      XFB_CUDA(h, cudaMemcpy(o, b.p, b.bytes, cudaMemcpyDeviceToHost));
+      if ((rc = copy(h, o, b.p, b.bytes, cudaMemcpyDeviceToHost))) return rc;
       o += b.bytes;
     }
   return XFB_OK;
@@ -485,7 +492,7 @@ int xfb_set_state(xfb_handle* h, const void* src, size_t len) {
   o += sizeof(long long);
   for (const Buf& b : h->bufs)
     if (b.state) {
-      XFB_CUDA(h, cudaMemcpy(b.p, o, b.bytes, cudaMemcpyHostToDevice));
+      if ((rc = copy(h, b.p, o, b.bytes, cudaMemcpyHostToDevice))) return rc;
       o += b.bytes;
     }
   h->step = step;

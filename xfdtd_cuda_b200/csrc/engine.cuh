@@ -48,7 +48,7 @@ int init_device(xfb_handle* h) {
         for (int k = 0; k < nz; ++k) m[off3(h, i, j, k)] = c.mat_id[(static_cast<size_t>(i) * ny + j) * nz + k];
     void* p;  // same guard as the fields (the one-sweep kernel stages halo windows)
     if ((rc = alloc(h, &p, m.size() + 2 * h->guard, false))) return rc;
-    XFB_CUDA(h, cudaMemcpy(static_cast<uint8_t*>(p) + h->guard, m.data(), m.size(), cudaMemcpyHostToDevice));
+    if ((rc = copy(h, static_cast<uint8_t*>(p) + h->guard, m.data(), m.size(), cudaMemcpyHostToDevice))) return rc;
     h->mid = static_cast<uint8_t*>(p) + h->guard;
   }
   if ((rc = upload<T>(h, &h->lut, c.coeff))) return rc;
@@ -56,7 +56,7 @@ int init_device(xfb_handle* h) {
   {
     void* p;
     if ((rc = alloc(h, &p, c.mat_disp.size(), false))) return rc;
-    XFB_CUDA(h, cudaMemcpy(p, c.mat_disp.data(), c.mat_disp.size(), cudaMemcpyHostToDevice));
+    if ((rc = copy(h, p, c.mat_disp.data(), c.mat_disp.size(), cudaMemcpyHostToDevice))) return rc;
     h->mat_disp = static_cast<uint8_t*>(p);
   }
   // CPML
@@ -146,10 +146,10 @@ int init_device(xfb_handle* h) {
     void* p;
     if ((rc = alloc(h, &p, n * sizeof(long long), false))) return rc;
     h->probe_idx = static_cast<long long*>(p);
-    XFB_CUDA(h, cudaMemcpy(p, idx.data(), n * sizeof(long long), cudaMemcpyHostToDevice));
+    if ((rc = copy(h, p, idx.data(), n * sizeof(long long), cudaMemcpyHostToDevice))) return rc;
     if ((rc = alloc(h, &p, n * sizeof(int), false))) return rc;
     h->probe_field = static_cast<int*>(p);
-    XFB_CUDA(h, cudaMemcpy(p, fld.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    if ((rc = copy(h, p, fld.data(), n * sizeof(int), cudaMemcpyHostToDevice))) return rc;
     if ((rc = alloc(h, &p, n * std::max(1LL, c.total_steps) * sizeof(double), true))) return rc;
     h->probe_out = static_cast<double*>(p);
   }
@@ -445,8 +445,8 @@ int profile_steps(xfb_handle* h, long long n, double* ms, long long* launches) {
 template <typename T>
 int read_field_t(xfb_handle* h, int f, double* dst) {
   std::vector<T> tmp(static_cast<size_t>(h->elems));
-  XFB_CUDA(h, cudaStreamSynchronize(h->stream));
-  XFB_CUDA(h, cudaMemcpy(tmp.data(), field_ptr(h, cur_set(h), f), tmp.size() * sizeof(T), cudaMemcpyDeviceToHost));
+  int rc;
+  if ((rc = copy(h, tmp.data(), field_ptr(h, cur_set(h), f), tmp.size() * sizeof(T), cudaMemcpyDeviceToHost))) return rc;
   int s[3];
   comp_shape(h->c, f, s);
   size_t o = 0;
@@ -459,8 +459,8 @@ int read_field_t(xfb_handle* h, int f, double* dst) {
 template <typename T>
 int write_field_t(xfb_handle* h, int f, const double* src) {
   std::vector<T> tmp(static_cast<size_t>(h->elems));
-  XFB_CUDA(h, cudaStreamSynchronize(h->stream));
-  XFB_CUDA(h, cudaMemcpy(tmp.data(), field_ptr(h, cur_set(h), f), tmp.size() * sizeof(T), cudaMemcpyDeviceToHost));
+  int rc;
+  if ((rc = copy(h, tmp.data(), field_ptr(h, cur_set(h), f), tmp.size() * sizeof(T), cudaMemcpyDeviceToHost))) return rc;
   int s[3];
   comp_shape(h->c, f, s);
   size_t o = 0;
@@ -469,8 +469,8 @@ int write_field_t(xfb_handle* h, int f, const double* src) {
       for (int k = 0; k < s[2]; ++k) tmp[off3(h, i, j, k)] = static_cast<T>(src[o++]);
   // both sets: entries the update never writes (PEC walls, unused slots) must
   // agree in the two ping-pong buffers
-  XFB_CUDA(h, cudaMemcpy(h->f[f], tmp.data(), tmp.size() * sizeof(T), cudaMemcpyHostToDevice));
-  if (fused(h)) XFB_CUDA(h, cudaMemcpy(h->f1[f], tmp.data(), tmp.size() * sizeof(T), cudaMemcpyHostToDevice));
+  if ((rc = copy(h, h->f[f], tmp.data(), tmp.size() * sizeof(T), cudaMemcpyHostToDevice))) return rc;
+  if (fused(h) && (rc = copy(h, h->f1[f], tmp.data(), tmp.size() * sizeof(T), cudaMemcpyHostToDevice))) return rc;
   return XFB_OK;
 }
 

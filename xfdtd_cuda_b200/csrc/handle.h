@@ -93,13 +93,19 @@ T* as(void* p) { return static_cast<T*>(p); }
 
 void free_device(xfb_handle* h);
 int alloc(xfb_handle* h, void** out, size_t bytes, bool state);
+// Every host<->device copy of the library goes through this: it is issued on
+// the handle's stream (a non-blocking stream, which the legacy default stream
+// does not order against) and waited for, so it lands after the zero-fill of
+// alloc() and after every kernel already queued, and the host buffer may be
+// released on return.
+int copy(xfb_handle* h, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind);
 
 template <typename T>
 int upload(xfb_handle* h, void** out, const std::vector<double>& v, bool state = false) {
   std::vector<T> tmp(v.begin(), v.end());
   int rc = alloc(h, out, tmp.size() * sizeof(T), state);
   if (rc) return rc;
-  if (!tmp.empty()) XFB_CUDA(h, cudaMemcpy(*out, tmp.data(), tmp.size() * sizeof(T), cudaMemcpyHostToDevice));
+  if (!tmp.empty()) return copy(h, *out, tmp.data(), tmp.size() * sizeof(T), cudaMemcpyHostToDevice);
   return XFB_OK;
 }
 
