@@ -265,6 +265,26 @@ int xfb_read_nf2ff(xfb_handle* h, int freq, int face, int which, double* dst, si
 int xfb_far_field(xfb_handle* h, int freq, int n_angles, const double* theta,
                   const double* phi, double* out);
 
+/* Same far field as xfb_far_field, computed without allocating device memory.
+ * No counterpart in the reference.  For hosts that cannot allocate on the
+ * device once they are running: frameworks that hand the solver a fixed
+ * device-memory budget at start-up and treat any later cudaMalloc as a fault,
+ * and latency-bound loops where cudaMalloc/cudaFree would stall the device.
+ * xfb_far_field allocates its angle and output buffers per call; this entry
+ * point uses one fixed device array of the library instead (192 KiB on every
+ * device that loads the library, kept until process exit), so it accepts at
+ * most XFB_FAR_FIELD_STATIC_MAX_ANGLES angles per call and returns
+ * XFB_ERR_RANGE beyond that.  The caller still passes the host angle and
+ * output arrays.  The first call on a device looks the array's device address
+ * up (cudaGetSymbolAddress) and caches it; make that first call before any
+ * stream capture.  All calls on a device share the one array: calls that
+ * overlap on the GPU (e.g. two handles on different streams) race, so keep
+ * them apart.  Nothing needs clearing between calls: every output entry of the
+ * n angles is rewritten by each call. */
+#define XFB_FAR_FIELD_STATIC_MAX_ANGLES 4096
+int xfb_far_field_static(xfb_handle* h, int freq, int n_angles, const double* theta,
+                         const double* phi, double* out);
+
 /* ---- checkpoint / resume ------------------------------------------------ */
 /* Byte size of the full solver state (fields, CPML psi, ADE state, TFSF
  * auxiliary grid, NF2FF accumulators, monitors, step counter). */

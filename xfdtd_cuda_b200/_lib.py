@@ -24,6 +24,7 @@ WAVE_GAUSSIAN, WAVE_COS_GAUSSIAN = 0, 1
 JA, JB, MA, MB = 0, 1, 2, 3
 ADE_NONE, ADE_DEBYE, ADE_DRUDE, ADE_MLORENTZ = 0, 1, 2, 3
 MAX_POLES = 4
+FAR_FIELD_STATIC_MAX_ANGLES = 4096  # XFB_FAR_FIELD_STATIC_MAX_ANGLES
 K_UPDATE_H, K_AUX, K_UPDATE_E, K_NF2FF, K_PROBE, K_MOVIE, K_STEP, K_COUNT = range(8)
 KERNEL_NAMES = ("k_h3/k_h2 (H half-step)", "k_aux (TFSF aux grid)", "k_e3/k_e2 (E half-step)", "k_nf2ff",
                 "k_probe", "k_movie", "k_step3 (one-sweep H+E step)")
@@ -141,6 +142,7 @@ SIGNATURES = [
     ("xfb_nf2ff_face_shape", C.c_int, [_H, C.c_int, C.c_int * 3]),
     ("xfb_read_nf2ff", C.c_int, [_H, C.c_int, C.c_int, C.c_int, _dp, C.c_size_t]),
     ("xfb_far_field", C.c_int, [_H, C.c_int, C.c_int, _dp, _dp, _dp]),
+    ("xfb_far_field_static", C.c_int, [_H, C.c_int, C.c_int, _dp, _dp, _dp]),
     ("xfb_state_size", C.c_int, [_H, C.POINTER(C.c_size_t)]),
     ("xfb_get_state", C.c_int, [_H, C.c_void_p, C.c_size_t]),
     ("xfb_set_state", C.c_int, [_H, C.c_void_p, C.c_size_t]),

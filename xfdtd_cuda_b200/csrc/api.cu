@@ -15,6 +15,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -119,6 +120,35 @@ int check_handle(xfb_handle* h, bool need_init) {
 }
 
 }  // namespace xfb
+
+// ---------------------------------------------------------------------------
+// Scratch of xfb_far_field_static: a fixed device array instead of per-call
+// allocations, for callers that must not allocate device memory after start-up.
+// Layout: theta[kFarStaticMaxAngles], phi[kFarStaticMaxAngles],
+// out[4 * kFarStaticMaxAngles] (192 KiB per device that loads the library, held
+// until the process exits).  Device code could name the array directly; host
+// code only holds a host-side stand-in for it, so the device address is fetched
+// with cudaGetSymbolAddress once per device, with that device current.
+namespace {
+constexpr int kFarStaticMaxAngles = XFB_FAR_FIELD_STATIC_MAX_ANGLES;
+static __device__ __align__(256) double g_far_scratch[6 * kFarStaticMaxAngles];
+
+std::mutex g_far_scratch_mu;
+double* g_far_scratch_dev[256] = {};  // per device ordinal
+
+int far_scratch_for(xfb_handle* h, double** out) {
+  if (h->device < 0 || h->device >= 256) return set_err(h, XFB_ERR_RANGE, "device ordinal outside the scratch table");
+  std::lock_guard<std::mutex> lock(g_far_scratch_mu);
+  if (!g_far_scratch_dev[h->device]) {
+    double* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void**>(&p), g_far_scratch);
+    if (e != cudaSuccess) return cuda_err(h, e, "cudaGetSymbolAddress(far-field scratch)");
+    g_far_scratch_dev[h->device] = p;
+  }
+  *out = g_far_scratch_dev[h->device];
+  return XFB_OK;
+}
+}  // namespace
 
 extern "C" {
 
@@ -447,6 +477,42 @@ int xfb_far_field(xfb_handle* h, int freq, int n, const double* theta, const dou
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   cudaFree(d_th); cudaFree(d_ph); cudaFree(d_out);
   if (e != cudaSuccess) return cuda_err(h, e, "far-field kernel");
+  return XFB_OK;
+}
+
+int xfb_far_field_static(xfb_handle* h, int freq, int n, const double* theta, const double* phi, double* out) {
+  int rc = check_handle(h, true);  // makes the handle's device current
+  if (rc) return rc;
+  if (!h->c.nf_on) return set_err(h, XFB_ERR_STATE, "scene has no NF2FF box");
+  if (freq < 0 || freq >= static_cast<int>(h->c.freqs.size())) return set_err(h, XFB_ERR_RANGE, "frequency index out of range");
+  if (n < 0 || (n > 0 && (!theta || !phi || !out))) return set_err(h, XFB_ERR_INVALID, "bad angle arrays");
+  if (n > kFarStaticMaxAngles)
+    return set_err(h, XFB_ERR_RANGE,
+                   "xfb_far_field_static takes at most " + std::to_string(kFarStaticMaxAngles) +
+                       " angles per call (its scratch is a fixed device array); got " + std::to_string(n));
+  if (n == 0) return XFB_OK;
+  double* scratch = nullptr;
+  if ((rc = far_scratch_for(h, &scratch))) return rc;
+  double* d_th = scratch;
+  double* d_ph = scratch + kFarStaticMaxAngles;
+  double* d_out = scratch + 2 * kFarStaticMaxAngles;
+  XFB_CUDA(h, cudaMemcpyAsync(d_th, theta, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  XFB_CUDA(h, cudaMemcpyAsync(d_ph, phi, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  FarP fp{};
+  const Compiled& c = h->c;
+  for (int q = 0; q < 6; ++q) fp.box[q] = c.nf[q];
+  for (int q = 0; q < 7; ++q) fp.off[q] = h->nf_off[q];
+  fp.npts = h->nf_npts;
+  fp.acc = h->nf_acc + static_cast<long long>(freq) * 4 * h->nf_npts;
+  for (int a = 0; a < 3; ++a) fp.origin[a] = c.origin[a];
+  fp.d[0] = c.dx; fp.d[1] = c.dy; fp.d[2] = c.dz;
+  fp.k = 2 * kPi * c.freqs[freq] / c0();
+  fp.eta = std::sqrt(kMu0 / kEps0);
+  fp.theta = d_th; fp.phi = d_ph; fp.out = d_out;  // k_far writes all 4 outputs of every angle
+  k_far<<<n, 256, 0, h->stream>>>(fp);
+  XFB_CUDA(h, cudaGetLastError());
+  XFB_CUDA(h, cudaMemcpyAsync(out, d_out, 4 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  XFB_CUDA(h, cudaStreamSynchronize(h->stream));
   return XFB_OK;
 }
 

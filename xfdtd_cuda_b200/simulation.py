@@ -636,6 +636,16 @@ class Handle:
                                        out.ctypes.data_as(L._dp)))
         return out[:, 0] + 1j * out[:, 1], out[:, 2] + 1j * out[:, 3]
 
+    def far_field_static(self, freq, theta, phi):
+        """xfb_far_field without device allocation (fixed device scratch of the
+        library, at most FAR_FIELD_STATIC_MAX_ANGLES angles per call)."""
+        th = np.ascontiguousarray(theta, dtype=np.float64)
+        ph = np.ascontiguousarray(phi, dtype=np.float64)
+        out = np.empty((len(th), 4), dtype=np.float64)
+        self._c(self.lib.xfb_far_field_static(self.h, freq, len(th), th.ctypes.data_as(L._dp),
+                                              ph.ctypes.data_as(L._dp), out.ctypes.data_as(L._dp)))
+        return out[:, 0] + 1j * out[:, 1], out[:, 2] + 1j * out[:, 3]
+
     def get_state(self) -> bytes:
         n = C.c_size_t()
         self._c(self.lib.xfb_state_size(self.h, C.byref(n)))
