@@ -187,6 +187,34 @@ def run_reference(args, rank, world):
     return 0
 
 
+def plain_compare(local: int, steps: int, warmup: int):
+    """Mcell-updates/s of the C1 workload (dielectric sphere 140^3 + 8-cell CPML
+    = 156^3, TFSF, NF2FF at 1 GHz) in the FP64 plain form (the reference's
+    kernel structure: per-cell coefficient arrays, one launch per component,
+    separate CPML/TFSF corrector launches) next to the FP32 and FP64 fused
+    one-sweep kernel, device-timed the same way as the headline number."""
+    import xfdtd_cuda_b200 as X
+    from xfdtd_cuda_b200 import _lib as L
+    from xfdtd_cuda_b200 import configs
+    res = {}
+    for key, prec, path in (("fp64_plain", "fp64", L.PATH_PLAIN), ("fp64_fused", "fp64", L.PATH_FUSED),
+                            ("fp32_fused", "fp32", L.PATH_FUSED)):
+        sim = configs.dielectric_sphere(precision=prec)
+        sc, keep = sim.lower()
+        h = X.Handle(sc, keep)
+        h.set_device(local)
+        h.set_kernel_path(path)
+        h.init(warmup + steps)
+        gi = h.info()
+        h.step(warmup)
+        h.sync()
+        ms = h.timed_step(steps)
+        res[key] = gi.nx * gi.ny * gi.nz * steps / (ms / 1e3) / 1e6
+        h.close()
+    return {"workload": "dielectric sphere 156x156x156 (140^3 + 8-cell CPML), eps_r=3 mu_r=2, TFSF, NF2FF 1 GHz",
+            "unit": UNIT, "steps": steps, **res, "fp32_fused_over_fp64_plain": res["fp32_fused"] / res["fp64_plain"]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -200,9 +228,10 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--path", choices=["auto", "split", "fused"], default="auto")
+    ap.add_argument("--path", choices=["auto", "split", "fused", "plain"], default="auto")
     ap.add_argument("--scene", choices=["dispersive", "vacuum", "pml", "tfsf", "nf2ff"], default="dispersive")
     ap.add_argument("--tile-rows", type=int, default=8)
+    ap.add_argument("--no-plain", action="store_true", help="skip the FP64 plain-form comparison")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -230,7 +259,7 @@ def main():
     sc, keep = sim.lower()
     h = X.Handle(sc, keep)
     h.set_device(local)
-    path = {"auto": L.PATH_AUTO, "split": L.PATH_SPLIT, "fused": L.PATH_FUSED}[args.path]
+    path = {"auto": L.PATH_AUTO, "split": L.PATH_SPLIT, "fused": L.PATH_FUSED, "plain": L.PATH_PLAIN}[args.path]
     h.set_kernel_path(path)
     h.set_launch_hint((1, 1, 1), (32, args.tile_rows, 1))
     total = args.warmup + args.steps + args.profile_steps
@@ -311,6 +340,10 @@ def main():
                "path": "Handle(scene) + init + step + read-back (SimulationHD.run flow), wall clock"}
         h2.close()
 
+    plain = None
+    if not args.no_plain and world == 1:
+        plain = plain_compare(local, 50, 3)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_sample(args.ref_cells, args.cpu_steps)
@@ -324,7 +357,7 @@ def main():
                           "cells_per_step": cells, "parallelism": f"scene-replica x{world}" if world > 1 else "1 GPU",
                           "l2": "resident state 3.3 GB >> 126 MB L2 (no flush needed)"},
                "e2e": e2e, "roofline": roofline, "step_roofline": step_roof, "cpu_baseline": cpu,
-               "clocks": clk.summary(), "gpu_launches": launches, "kernels": kernels}
+               "clocks": clk.summary(), "gpu_launches": launches, "kernels": kernels, "vs_fp64_plain": plain}
         print(json.dumps(out))
     h.close()
     if dist:

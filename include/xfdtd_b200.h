@@ -69,8 +69,14 @@ enum xfb_ade_kind { XFB_ADE_NONE = 0, XFB_ADE_DEBYE = 1, XFB_ADE_DRUDE = 2, XFB_
 /* How a 3-D time step is executed.  SPLIT: an H half-step kernel and an E
  * half-step kernel (the reference's updateH/updateE split, correctors fused).
  * FUSED: one kernel per step that sweeps the grid once (H and E together,
- * ping-pong field buffers).  AUTO: FUSED in 3-D, SPLIT in 2-D. */
-enum xfb_kernel_path { XFB_PATH_AUTO = 0, XFB_PATH_SPLIT = 1, XFB_PATH_FUSED = 2 };
+ * ping-pong field buffers).  PLAIN: the reference's own GPU structure kept as
+ * a baseline -- 18 per-cell coefficient arrays, one launch per field
+ * component with flat (i, j, k) indexing, CPML and TFSF corrections as
+ * separate launches per face (src/include/updator/update_scheme.cuh:132-197,
+ * src/boundary/pml_corrector.cu:9-291,
+ * src/waveform_source/tfsf/tfsf_corrector.cu:155-271); 3-D scenes without
+ * dispersive media only.  AUTO: FUSED in 3-D, SPLIT in 2-D. */
+enum xfb_kernel_path { XFB_PATH_AUTO = 0, XFB_PATH_SPLIT = 1, XFB_PATH_FUSED = 2, XFB_PATH_PLAIN = 3 };
 
 #define XFB_MAX_POLES 4
 #define XFB_MAX_MATERIALS 255
@@ -223,7 +229,7 @@ int xfb_timed_step(xfb_handle* h, long long n, double* ms);
 /* Kernel classes of one time step, for xfb_profile_kernels. */
 enum xfb_kernel_class {
   XFB_K_UPDATE_H = 0, XFB_K_AUX = 1, XFB_K_UPDATE_E = 2, XFB_K_NF2FF = 3, XFB_K_PROBE = 4,
-  XFB_K_MOVIE = 5, XFB_K_STEP = 6, XFB_K_COUNT = 7
+  XFB_K_MOVIE = 5, XFB_K_STEP = 6, XFB_K_CORRECT = 7, XFB_K_COUNT = 8
 };
 /* Advance n steps launching every kernel individually with CUDA events around
  * it; ms[c] = summed device time and launches[c] = launch count of class c

@@ -38,6 +38,7 @@ def add_movie(sim, field=0, interval=7):
 
 
 PATHS = [1, 2]  # XFB_PATH_SPLIT (H and E half-step kernels), XFB_PATH_FUSED (one-sweep step)
+PLAIN = 3        # XFB_PATH_PLAIN (reference kernel structure; no ADE, 3-D only)
 
 
 def run_pair(sim, n, path=0):
@@ -68,7 +69,7 @@ def check_all(h, o, dim, n_probes, n_movies, nf, tol=FP64_TOL, expect_exact=True
         assert bit_equal(gf, of), "FP64 fields agree within tolerance but not bit for bit"
 
 
-@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("path", PATHS + [PLAIN])
 def test_fp64_dielectric_sphere_bitexact(path):
     sim = add_movie(small_sphere())
     h, o = run_pair(sim, 90, path)
@@ -100,7 +101,7 @@ def test_fp64_cylinder_2d_bitexact():
     check_all(h, o, 2, 5, 1, nf=False)
 
 
-@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("path", PATHS + [PLAIN])
 def test_fp64_no_tfsf_no_pml_initial_field(path):
     # PEC box with random initial fields: pure Yee update, no correctors
     sim = X.Simulation(3e-3, 3e-3, 3e-3, 0.9)
@@ -123,7 +124,7 @@ def test_fp64_no_tfsf_no_pml_initial_field(path):
     assert bit_equal(gf, of)
 
 
-@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("path", PATHS + [PLAIN])
 def test_fp32_against_fp64_oracle(path):
     sim32 = small_sphere("fp32")
     sim64 = small_sphere("fp64")
@@ -236,3 +237,14 @@ def test_simulation_hd_dropin_flow(tmp_path):
     nf = sim.nf2ffs()[0]
     et, ep = nf.processFarField(np.linspace(-math.pi, math.pi, 36), 0.0, "xz")
     assert et.shape == (2, 36) and np.isfinite(et).all()
+
+
+def test_plain_path_rejects_dispersive_and_2d():
+    for sim in (configs.dispersive_sphere(cells=20, dl=4e-3, pml=4, precision="fp64", freqs=(), tfsf_inset=3,
+                                          radius=0.02),
+                configs.cylinder_2d(cells=40, dl=1e-3, pml=6, precision="fp64", radius=0.005, tfsf_inset=4)):
+        sc, keep = sim.lower()
+        h = X.Handle(sc, keep)
+        h.set_kernel_path(PLAIN)
+        with pytest.raises(X.XfbError, match="plain path"):
+            h.init(10)

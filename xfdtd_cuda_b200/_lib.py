@@ -25,10 +25,10 @@ JA, JB, MA, MB = 0, 1, 2, 3
 ADE_NONE, ADE_DEBYE, ADE_DRUDE, ADE_MLORENTZ = 0, 1, 2, 3
 MAX_POLES = 4
 FAR_FIELD_STATIC_MAX_ANGLES = 4096  # XFB_FAR_FIELD_STATIC_MAX_ANGLES
-K_UPDATE_H, K_AUX, K_UPDATE_E, K_NF2FF, K_PROBE, K_MOVIE, K_STEP, K_COUNT = range(8)
+K_UPDATE_H, K_AUX, K_UPDATE_E, K_NF2FF, K_PROBE, K_MOVIE, K_STEP, K_CORRECT, K_COUNT = range(9)
 KERNEL_NAMES = ("k_h3/k_h2 (H half-step)", "k_aux (TFSF aux grid)", "k_e3/k_e2 (E half-step)", "k_nf2ff",
-                "k_probe", "k_movie", "k_step3 (one-sweep H+E step)")
-PATH_AUTO, PATH_SPLIT, PATH_FUSED = 0, 1, 2
+                "k_probe", "k_movie", "k_step3 (one-sweep H+E step)", "plain CPML/TFSF corrector launches")
+PATH_AUTO, PATH_SPLIT, PATH_FUSED, PATH_PLAIN = 0, 1, 2, 3
 
 
 class Pole(C.Structure):

@@ -83,6 +83,7 @@ int copy(xfb_handle* h, void* dst, const void* src, size_t bytes, cudaMemcpyKind
 long long roundup(long long v, long long m) { return (v + m - 1) / m * m; }
 
 bool fused(const xfb_handle* h) { return h->path == XFB_PATH_FUSED; }
+bool plain(const xfb_handle* h) { return h->path == XFB_PATH_PLAIN; }
 // field set holding the state after h->step steps
 int cur_set(const xfb_handle* h) { return fused(h) ? static_cast<int>(h->step & 1) : 0; }
 void* field_ptr(const xfb_handle* h, int set, int q) { return set ? h->f1[q] : h->f[q]; }
@@ -105,6 +106,12 @@ int nf_face_points(const Compiled& c, int face) {
 // ---------------------------------------------------------------------------
 int launches_per_step(const xfb_handle* h) {
   const Compiled& c = h->c;
+  if (plain(h)) {
+    int faces = 0;
+    for (int f = 0; f < 6; ++f) faces += c.pml[f] > 0;
+    return 6 + 2 * faces + (c.tfsf_on ? 1 + 24 : 0) + (c.nf_on ? 1 : 0) + (c.probes.empty() ? 0 : 1) +
+           static_cast<int>(c.movies.size());
+  }
   return (fused(h) ? 1 : 2) + (c.tfsf_on ? 1 : 0) + (c.nf_on ? 1 : 0) + (c.probes.empty() ? 0 : 1) +
          static_cast<int>(c.movies.size());
 }
@@ -235,7 +242,7 @@ int xfb_set_device(xfb_handle* h, int ordinal) {
 
 int xfb_set_kernel_path(xfb_handle* h, int path) {
   if (!h) return set_err(nullptr, XFB_ERR_INVALID, "null handle");
-  if (path < XFB_PATH_AUTO || path > XFB_PATH_FUSED) return set_err(h, XFB_ERR_INVALID, "unknown kernel path");
+  if (path < XFB_PATH_AUTO || path > XFB_PATH_PLAIN) return set_err(h, XFB_ERR_INVALID, "unknown kernel path");
   if (h->inited) return set_err(h, XFB_ERR_STATE, "set the kernel path before xfb_init");
   h->path = path;
   return XFB_OK;
@@ -273,7 +280,10 @@ int xfb_init(xfb_handle* h, long long total_steps) {
   XFB_CUDA(h, cudaStreamSynchronize(h->stream));
   free_device(h);
   size_tables(h->c, total_steps);
-  if (h->path == XFB_PATH_AUTO || h->c.dim == 2) h->path = h->c.dim == 3 ? XFB_PATH_FUSED : XFB_PATH_SPLIT;
+  if (h->path == XFB_PATH_PLAIN && (h->c.dim != 3 || h->c.ade_kind != XFB_ADE_NONE))
+    return set_err(h, XFB_ERR_INVALID, "the plain path handles 3-D scenes without dispersive media only");
+  if (h->path == XFB_PATH_AUTO || (h->c.dim == 2 && h->path != XFB_PATH_PLAIN))
+    h->path = h->c.dim == 3 ? XFB_PATH_FUSED : XFB_PATH_SPLIT;
   int rc;
   try {
     rc = h->c.prec == XFB_FP64 ? init_device<double>(h) : init_device<float>(h);

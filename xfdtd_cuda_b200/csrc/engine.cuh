@@ -10,6 +10,7 @@
 #include "fused3d.cuh"
 #include "handle.h"
 #include "kernels.cuh"
+#include "plain.cuh"
 
 namespace xfb {
 
@@ -53,6 +54,15 @@ int init_device(xfb_handle* h) {
   }
   if ((rc = upload<T>(h, &h->lut, c.coeff))) return rc;
   if ((rc = upload<T>(h, &h->lut8, c.coeff8))) return rc;
+  if (plain(h)) {  // per-cell coefficient arrays, expanded from the LUT on the device
+    PlainCoef<T> pc;
+    for (int q = 0; q < 18; ++q) {
+      if ((rc = alloc(h, &h->plain_c[q], h->elems * sizeof(T), false))) return rc;
+      pc.c[q] = as<T>(h->plain_c[q]);
+    }
+    k_plain_expand<T><<<4 * 148, 256, 0, h->stream>>>(pc, h->mid, as<const T>(h->lut), h->elems);
+    XFB_CUDA(h, cudaGetLastError());
+  }
   {
     void* p;
     if ((rc = alloc(h, &p, c.mat_disp.size(), false))) return rc;
@@ -291,6 +301,87 @@ void launch_fused(xfb_handle* h, int parity, TimeP tp, cudaStream_t st) {
                                              ade_params<T>(h), tp, ich, as<const T>(h->lut8), h->mat_disp, c.n_mat);
 }
 
+// ---- plain path (reference kernel structure) ------------------------------
+constexpr int kPlainBlocks = 148 * 8, kPlainThreads = 256;
+
+template <typename T, bool IS_E>
+void plain_update(xfb_handle* h, const GridP<T>& g) {
+  cudaStream_t s = h->stream;
+  auto cf = [&](int q) { return as<const T>(h->plain_c[q]); };
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  if (IS_E) {
+    k_plain_comp<T, true, 0><<<kPlainBlocks, kPlainThreads, 0, s>>>(g.ex, g.hy, g.hz, cf(CEXE), cf(CEXHY), cf(CEXHZ), nx, ny, nz, g.sx, g.sy);
+    k_plain_comp<T, true, 1><<<kPlainBlocks, kPlainThreads, 0, s>>>(g.ey, g.hz, g.hx, cf(CEYE), cf(CEYHZ), cf(CEYHX), nx, ny, nz, g.sx, g.sy);
+    k_plain_comp<T, true, 2><<<kPlainBlocks, kPlainThreads, 0, s>>>(g.ez, g.hx, g.hy, cf(CEZE), cf(CEZHX), cf(CEZHY), nx, ny, nz, g.sx, g.sy);
+  } else {
+    k_plain_comp<T, false, 0><<<kPlainBlocks, kPlainThreads, 0, s>>>(g.hx, g.ey, g.ez, cf(CHXH), cf(CHXEY), cf(CHXEZ), nx, ny, nz, g.sx, g.sy);
+    k_plain_comp<T, false, 1><<<kPlainBlocks, kPlainThreads, 0, s>>>(g.hy, g.ez, g.ex, cf(CHYH), cf(CHYEZ), cf(CHYEX), nx, ny, nz, g.sx, g.sy);
+    k_plain_comp<T, false, 2><<<kPlainBlocks, kPlainThreads, 0, s>>>(g.hz, g.ex, g.ey, cf(CHZH), cf(CHZEX), cf(CHZEY), nx, ny, nz, g.sx, g.sy);
+  }
+}
+
+// TFSF agencies of one half step in the reference order (3-D agency,
+// src/waveform_source/tfsf/tfsf_corrector.cu:201-271): face, field component.
+template <typename T>
+void plain_tfsf(xfb_handle* h, const GridP<T>& g, TimeP tp, int attr_h) {
+  const Compiled& c = h->c;
+  static const int order[12][2] = {{0, 2}, {1, 2}, {2, 2}, {3, 2}, {4, 0}, {5, 0},
+                                   {2, 0}, {3, 0}, {4, 1}, {5, 1}, {0, 1}, {1, 1}};
+  const TfsfP tf = tfsf_params(h);
+  const int lo[3] = {c.tf[0], c.tf[2], c.tf[4]}, hi[3] = {c.tf[1], c.tf[3], c.tf[5]};
+  for (int q = 0; q < 12; ++q) {
+    const int face = order[q][0], fxyz = order[q][1];
+    const int ax = face / 2, neg = (face % 2) == 0, a = (ax + 1) % 3, b = (ax + 2) % 3;
+    PlainTfsfFace fc{};
+    fc.neg = neg; fc.attr_h = attr_h; fc.fxyz = fxyz;
+    fc.as = lo[a]; fc.ae = hi[a]; fc.bs = lo[b]; fc.be = hi[b];
+    fc.cs = neg ? lo[ax] : hi[ax];
+    const bool offset_a = (!attr_h && fxyz == b) || (attr_h && fxyz == a);
+    if (offset_a) fc.ae += 1; else fc.be += 1;
+    fc.dual = fxyz == a ? b : a;
+    const int flag = (attr_h ? -1 : 1) * (fxyz == a ? -1 : 1) * (neg ? -1 : 1);
+    fc.coef = (attr_h ? c.cb[ax] : c.ca[ax]) * flag;
+    const long long n = static_cast<long long>(fc.ae - fc.as) * (fc.be - fc.bs);
+    const int blocks = static_cast<int>(std::min<long long>((n + 255) / 256, kPlainBlocks));
+    if (ax == 0) k_plain_tfsf<T, 0><<<blocks, 256, 0, h->stream>>>(g, tf, tp, fc);
+    else if (ax == 1) k_plain_tfsf<T, 1><<<blocks, 256, 0, h->stream>>>(g, tf, tp, fc);
+    else k_plain_tfsf<T, 2><<<blocks, 256, 0, h->stream>>>(g, tf, tp, fc);
+  }
+}
+
+// CPML faces XN..ZP of one half step (pml_corrector.cu:273-291 task ranges).
+template <typename T, bool IS_E>
+void plain_pml(xfb_handle* h, const GridP<T>& g) {
+  const Compiled& c = h->c;
+  const PmlP<T> pm = pml_params<T>(h);
+  const int n[3] = {c.nx, c.ny, c.nz};
+  for (int face = 0; face < 6; ++face) {
+    const int L = c.pml[face];
+    if (!L) continue;
+    const int ax = face / 2, side = face % 2, a = (ax + 1) % 3, b = (ax + 2) % 3;
+    PlainPmlFace fc{};
+    // E of a low face: planes 1 .. L-1 (plane L adds a zero correction); else the L slab planes
+    const int planes = (IS_E && side == 0) ? L - 1 : L;
+    fc.c0 = side ? n[ax] - L : (IS_E ? 1 : 0);
+    if (planes <= 0) continue;
+    // w = 0: component along a; w = 1: along b.  The +1 tangential extension
+    // follows the reference ranges (pml_corrector.cu:121-133, 160-172).
+    fc.a_end[0] = n[a] + (IS_E ? 0 : 1); fc.b_end[0] = n[b] + (IS_E ? 1 : 0);
+    fc.a_end[1] = n[a] + (IS_E ? 1 : 0); fc.b_end[1] = n[b] + (IS_E ? 0 : 1);
+    for (int w = 0; w < 2; ++w) fc.span[w] = static_cast<long long>(planes) * fc.a_end[w] * fc.b_end[w];
+    // c_psi: coefficient of component a w.r.t. dual b (b = a+1: slot 3a+1),
+    // of component b w.r.t. dual a (a = b+2: slot 3b+2)
+    const int base = IS_E ? 0 : 9;
+    const T* cps0 = as<const T>(h->plain_c[base + 3 * a + 1]);
+    const T* cps1 = as<const T>(h->plain_c[base + 3 * b + 2]);
+    const long long tot = fc.span[0] + fc.span[1];
+    const int blocks = static_cast<int>(std::min<long long>((tot + 255) / 256, kPlainBlocks));
+    if (ax == 0) k_plain_pml<T, IS_E, 0><<<blocks, 256, 0, h->stream>>>(g, pm, cps0, cps1, fc);
+    else if (ax == 1) k_plain_pml<T, IS_E, 1><<<blocks, 256, 0, h->stream>>>(g, pm, cps0, cps1, fc);
+    else k_plain_pml<T, IS_E, 2><<<blocks, 256, 0, h->stream>>>(g, pm, cps0, cps1, fc);
+  }
+}
+
 template <typename T>
 void enqueue_step(xfb_handle* h, int off, Prof* pf = nullptr) {
   const Compiled& c = h->c;
@@ -301,7 +392,27 @@ void enqueue_step(xfb_handle* h, int off, Prof* pf = nullptr) {
   PmlP<T> pm = pml_params<T>(h);
   TfsfP tf = tfsf_params(h);
   cudaStream_t s = h->stream;
-  if (fused(h)) {
+  if (plain(h)) {
+    prof_begin(h, pf, XFB_K_UPDATE_H);
+    plain_update<T, false>(h, g);
+    prof_end(h, pf);
+    prof_begin(h, pf, XFB_K_CORRECT);
+    if (c.tfsf_on) plain_tfsf<T>(h, g, tp, 1);
+    plain_pml<T, false>(h, g);
+    prof_end(h, pf);
+    if (c.tfsf_on) {
+      prof_begin(h, pf, XFB_K_AUX);
+      k_aux<<<1, 1024, 0, s>>>(h->e_aux, h->e_aux + (c.aux_nl + 1), h->h_aux, c.aux_nl, c.aux_ceih, c.aux_chie, c.aux_abc, h->src, tp);
+      prof_end(h, pf);
+    }
+    prof_begin(h, pf, XFB_K_UPDATE_E);
+    plain_update<T, true>(h, g);
+    prof_end(h, pf);
+    prof_begin(h, pf, XFB_K_CORRECT);
+    if (c.tfsf_on) plain_tfsf<T>(h, g, tp, 0);
+    plain_pml<T, true>(h, g);
+    prof_end(h, pf);
+  } else if (fused(h)) {
     if (c.tfsf_on) {
       prof_begin(h, pf, XFB_K_AUX);
       k_aux<<<1, 1024, 0, s>>>(h->e_aux, h->e_aux + (c.aux_nl + 1), h->h_aux, c.aux_nl, c.aux_ceih, c.aux_chie,

@@ -74,6 +74,7 @@ struct xfb_handle {
   std::vector<long long> movie_frames;
   long long* t_dev = nullptr;
   unsigned long long* scratch_u64 = nullptr;
+  void* plain_c[18] = {};  // per-cell coefficient arrays of the plain path
 };
 
 namespace xfb {
@@ -111,6 +112,7 @@ int upload(xfb_handle* h, void** out, const std::vector<double>& v, bool state =
 
 long long roundup(long long v, long long m);
 bool fused(const xfb_handle* h);
+bool plain(const xfb_handle* h);
 int cur_set(const xfb_handle* h);
 void* field_ptr(const xfb_handle* h, int set, int q);
 long long off3(const xfb_handle* h, int i, int j, int k);
