@@ -78,7 +78,10 @@ def test_fp64_dielectric_sphere_bitexact(path):
 
 @pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("kind", ["drude", "debye", "drude_lorentz", "mlorentz"])
-def test_fp64_ade_bitexact(kind, path):
+@pytest.mark.parametrize("radius", [0.03, 0.018])
+def test_fp64_ade_bitexact(kind, path, radius):
+    # radius 0.03 puts TFSF face planes next to the dispersive box (ADE inside
+    # the step kernel); 0.018 keeps them apart (ADE as a separate box pass)
     mats = {
         "drude": X.DrudeMedium("d", 1.0, [2e10], [1e9]),
         "debye": X.DebyeMedium("b", 2.0, [6.0], [2e-11]),
@@ -87,7 +90,7 @@ def test_fp64_ade_bitexact(kind, path):
                                                    (2 * math.pi * 2e9) ** 2, 2 * math.pi * 2e9, 1.0),
     }
     sim = configs.dispersive_sphere(cells=26, dl=4e-3, pml=6, precision="fp64", freqs=(1e9, 3e9), tfsf_inset=4,
-                                    nf2ff_inset=2, radius=0.03, material=mats[kind],
+                                    nf2ff_inset=2, radius=radius, material=mats[kind],
                                     probes=[((0.0, 0.0, 0.0), 2), ((0.01, 0.0, 0.0), 1)])
     h, o = run_pair(sim, 80, path)
     check_all(h, o, 3, 2, 0, nf=True)

@@ -14,6 +14,8 @@
 
 namespace xfb {
 
+inline int upload_step_items(xfb_handle* h);
+
 template <typename T>
 int init_device(xfb_handle* h) {
   Compiled& c = h->c;
@@ -54,6 +56,7 @@ int init_device(xfb_handle* h) {
   }
   if ((rc = upload<T>(h, &h->lut, c.coeff))) return rc;
   if ((rc = upload<T>(h, &h->lut8, c.coeff8))) return rc;
+  if (fused(h) && (rc = upload_step_items(h))) return rc;
   if (plain(h)) {  // per-cell coefficient arrays, expanded from the LUT on the device
     PlainCoef<T> pc;
     for (int q = 0; q < 18; ++q) {
@@ -283,22 +286,125 @@ PsiH<T> psi_h_set(xfb_handle* h, int set) {
   return PsiH<T>{as<T>(q[0]), as<T>(q[1]), as<T>(q[2]), as<T>(q[3]), as<T>(q[4]), as<T>(q[5])};
 }
 
-template <typename T, int TJ>
-void launch_fused(xfb_handle* h, int parity, TimeP tp, cudaStream_t st) {
-  using S = StepSmem<T, 32, TJ>;
-  const Compiled& c = h->c;
-  const int gx = (c.nz + 31) / 32, gy = (c.ny + TJ - 1) / TJ;
-  const int nch = chunks_for(gx * gy, c.nx, S::threads);
-  const int ich = (c.nx + nch - 1) / nch;
-  dim3 grd(gx, gy, (c.nx + ich - 1) / ich);
-  static bool attr_set = false;  // per instantiation; the attribute is per-function, per-device
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_step3<T, 32, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::bytes));
-    attr_set = true;
+// Tile configurations of the one-sweep kernel: rows per thread R, row warps
+// NWM (tile rows TJ = R * NWM), picked by the launch hint's row count.
+struct StepTile { int r, nwm; };
+constexpr StepTile kStepTiles[3] = {{2, 4}, {2, 8}, {4, 4}};
+constexpr int kStepKinds[4] = {0, 1, 4, 7};  // lean, x-slab planes, ADE box, y/z-slab columns (all)
+
+// Work items of the one-sweep kernel for tiles of TJ x 32 cells: every tile
+// column is cut along i into plane ranges whose cells (with the H halo plane
+// below the range and the halo row and column of the tile) need no more than
+// the range's kind handles.  Ranges are at most `ich` planes long.
+inline void build_step_items(const Compiled& c, int TJ, int NT, bool ade_deferred, std::vector<int4> (&out)[4]) {
+  const int nx = c.nx, ny = c.ny, nz = c.nz;
+  const int* L = c.pml;
+  const int gx = (nz + 31) / 32, gy = (ny + TJ - 1) / TJ;
+  const int nch = chunks_for(gx * gy, nx, NT);
+  const int ich = std::max(8, (nx + nch - 1) / nch);
+  auto xs = [&](int p) { return p < L[0] || p >= nx - L[1]; };
+  const int* b = c.ade_box;
+  const bool ade = !ade_deferred && c.ade_kind != XFB_ADE_NONE && b[1] > b[0];
+  auto kind_of = [](int bits) { return bits == 0 ? 0 : bits == 1 ? 1 : bits == 4 ? 2 : 3; };
+  for (int by = 0; by < gy; ++by)
+    for (int bx = 0; bx < gx; ++bx) {
+      const int j0 = by * TJ, k0 = bx * 32;
+      const int rlo = std::max(j0 - 1, 0), rhi = std::min(j0 + TJ - 1, ny - 1);
+      const int clo = std::max(k0 - 1, 0), chi = std::min(k0 + 31, nz - 1);
+      const bool yz = rlo < L[2] || rhi >= ny - L[3] || clo < L[4] || chi >= nz - L[5];
+      const bool adecol = ade && j0 < b[3] && j0 + TJ > b[2] && k0 < b[5] && k0 + 32 > b[4];
+      auto need = [&](int p) { return (xs(p) ? 1 : 0) | (adecol && p >= b[0] && p < b[1] ? 4 : 0); };
+      int p = 0;
+      while (p < nx) {
+        int q = p + 1, bits;
+        if (yz) {
+          bits = 7;
+          q = std::min(nx, p + ich);
+        } else {
+          const int nd = need(p), halo = p > 0 && xs(p - 1) ? 1 : 0;
+          bits = nd | halo;
+          if (!(halo & ~nd))  // the halo plane adds nothing: extend over equal needs
+            while (q < nx && need(q) == nd && q - p < ich) ++q;
+        }
+        out[kind_of(bits)].push_back(make_int4(bx, by, p, q));
+        p = q;
+      }
+    }
+}
+
+// True when the ADE update of the one-sweep path can run as a separate pass
+// (k_ade_box): the box of dispersive cells lies outside the CPML slabs and
+// contains no TFSF face plane, so no dispersive cell takes a correction that
+// the reference applies after the ADE update.
+inline bool ade_can_defer(const Compiled& c) {
+  const int* b = c.ade_box;
+  if (c.ade_kind == XFB_ADE_NONE || b[1] <= b[0] || b[3] <= b[2] || b[5] <= b[4]) return false;
+  const int n[3] = {c.nx, c.ny, c.nz};
+  for (int a = 0; a < 3; ++a) {
+    if (b[2 * a] < c.pml[2 * a] || b[2 * a + 1] > n[a] - c.pml[2 * a + 1]) return false;
+    if (c.tfsf_on)
+      for (int e = 0; e < 2; ++e) {
+        const int f = c.tf[2 * a + e];
+        if (f >= b[2 * a] - 1 && f <= b[2 * a + 1]) return false;
+      }
   }
-  k_step3<T, 32, TJ><<<grd, S::threads, S::bytes, st>>>(grid_params<T>(h, parity), grid_params<T>(h, 1 - parity), pml_params<T>(h),
-                                             psi_h_set<T>(h, parity), psi_h_set<T>(h, 1 - parity), tfsf_params(h),
-                                             ade_params<T>(h), tp, ich, as<const T>(h->lut8), h->mat_disp, c.n_mat);
+  return true;
+}
+
+inline int upload_step_items(xfb_handle* h) {
+  h->ade_deferred = ade_can_defer(h->c);
+  for (int t = 0; t < 3; ++t) {
+    std::vector<int4> items[4];
+    const int nt = (kStepTiles[t].nwm + 1) * 32;
+    build_step_items(h->c, kStepTiles[t].r * kStepTiles[t].nwm, nt, h->ade_deferred, items);
+    for (int q = 0; q < 4; ++q) {
+      h->n_step_items[t][q] = static_cast<int>(items[q].size());
+      if (items[q].empty()) continue;
+      int rc = alloc(h, &h->step_items[t][q], items[q].size() * sizeof(int4), false);
+      if (rc) return rc;
+      if ((rc = copy(h, h->step_items[t][q], items[q].data(), items[q].size() * sizeof(int4), cudaMemcpyHostToDevice)))
+        return rc;
+    }
+  }
+  return XFB_OK;
+}
+
+template <typename T, int R, int NWM, int KIND>
+void launch_step3(xfb_handle* h, int parity, TimeP tp, cudaStream_t st, const void* items, int n) {
+  using S = StepCfg<T, R, NWM>;
+  // with the ADE update deferred to k_ade_box the step kernels do none
+  AdeP<T> step_ade = ade_params<T>(h);
+  if (h->ade_deferred) step_ade.kind = kAdeNone;
+  static bool attr_set[64] = {};  // per instantiation and device
+  const int dev = h->device & 63;
+  if (!attr_set[dev]) {
+    cudaFuncSetAttribute(k_step3<T, R, NWM, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::bytes));
+    attr_set[dev] = true;
+  }
+  k_step3<T, R, NWM, KIND><<<n, S::NT, S::bytes, st>>>(
+      grid_params<T>(h, parity), grid_params<T>(h, 1 - parity), pml_params<T>(h), psi_h_set<T>(h, parity),
+      psi_h_set<T>(h, 1 - parity), tfsf_params(h), step_ade, tp, static_cast<const int4*>(items),
+      as<const T>(h->lut8), h->mat_disp, h->c.n_mat);
+}
+
+template <typename T, int R, int NWM>
+void launch_step3_kinds(xfb_handle* h, int t, int parity, TimeP tp, cudaStream_t st) {
+  const int* n = h->n_step_items[t];
+  void* const* it = h->step_items[t];
+  if (n[0]) launch_step3<T, R, NWM, kStepKinds[0]>(h, parity, tp, st, it[0], n[0]);
+  if (n[1]) launch_step3<T, R, NWM, kStepKinds[1]>(h, parity, tp, st, it[1], n[1]);
+  if (n[2]) launch_step3<T, R, NWM, kStepKinds[2]>(h, parity, tp, st, it[2], n[2]);
+  if (n[3]) launch_step3<T, R, NWM, kStepKinds[3]>(h, parity, tp, st, it[3], n[3]);
+}
+
+// One-sweep step: one launch per region kind present, for the tile the
+// launch hint's row count picks.
+template <typename T>
+void launch_fused(xfb_handle* h, int parity, TimeP tp, cudaStream_t st) {
+  const int t = step_tile_index(h->tj);
+  if (t == 0) launch_step3_kinds<T, kStepTiles[0].r, kStepTiles[0].nwm>(h, 0, parity, tp, st);
+  else if (t == 1) launch_step3_kinds<T, kStepTiles[1].r, kStepTiles[1].nwm>(h, 1, parity, tp, st);
+  else launch_step3_kinds<T, kStepTiles[2].r, kStepTiles[2].nwm>(h, 2, parity, tp, st);
 }
 
 // ---- plain path (reference kernel structure) ------------------------------
@@ -420,10 +526,13 @@ void enqueue_step(xfb_handle* h, int off, Prof* pf = nullptr) {
       prof_end(h, pf);
     }
     prof_begin(h, pf, XFB_K_STEP);
-    const int tj = h->tj;
-    if (tj <= 4) launch_fused<T, 4>(h, parity, tp, s);
-    else if (tj <= 8) launch_fused<T, 8>(h, parity, tp, s);
-    else launch_fused<T, 16>(h, parity, tp, s);
+    launch_fused<T>(h, parity, tp, s);
+    if (h->ade_deferred) {
+      const int* b = c.ade_box;
+      dim3 grd((b[5] - b[4] + 127) / 128, b[3] - b[2], b[1] - b[0]);
+      k_ade_box<T><<<grd, 128, 0, s>>>(grid_params<T>(h, parity), grid_params<T>(h, 1 - parity), ade_params<T>(h),
+                                       h->mat_disp);
+    }
     prof_end(h, pf);
   } else if (c.dim == 3) {
     const int tj = tile_rows<T>(h);

@@ -75,6 +75,13 @@ struct xfb_handle {
   long long* t_dev = nullptr;
   unsigned long long* scratch_u64 = nullptr;
   void* plain_c[18] = {};  // per-cell coefficient arrays of the plain path
+  // one-sweep step work items per tile configuration and region kind
+  // (int4: k tile, j tile, first plane, end plane)
+  void* step_items[3][4] = {};
+  int n_step_items[3][4] = {};
+  // ADE applied by k_ade_box after the one-sweep step (no dispersive cell
+  // takes a TFSF or CPML correction)
+  bool ade_deferred = false;
 };
 
 namespace xfb {
@@ -112,6 +119,8 @@ int upload(xfb_handle* h, void** out, const std::vector<double>& v, bool state =
 
 long long roundup(long long v, long long m);
 bool fused(const xfb_handle* h);
+// tile configuration of the one-sweep kernel picked by the launch hint's rows
+inline int step_tile_index(int tj) { return tj <= 8 ? 0 : tj <= 16 ? 1 : 2; }
 bool plain(const xfb_handle* h);
 int cur_set(const xfb_handle* h);
 void* field_ptr(const xfb_handle* h, int set, int q);

@@ -283,69 +283,24 @@ __device__ __forceinline__ T ade_e(const AdeP<T>& a, int comp, long long bi, int
   return e_new;
 }
 
-// ADE state of one cell held in registers (up to kAdeRegPoles poles), so its
-// loads can be issued well before the E update that consumes them.
-constexpr int kAdeRegPoles = 2;
+// Deferred ADE update of the dispersive box after a one-sweep step.  The step
+// kernel stored the plain eNext value of every cell in `d`; this applies the
+// TemplateADEUpdateScheme::updateE recursion (ade_e: same arithmetic, same
+// order) with E^n from `s`, one thread per box cell, k fastest.  Valid only
+// when no dispersive cell also takes a TFSF or CPML correction, which the
+// reference applies after the ADE update.
 template <typename T>
-struct AdeRegs {
-  T J[3][kAdeRegPoles], Jp[3][kAdeRegPoles], Ep[3];
-};
-
-template <typename T>
-__device__ __forceinline__ void ade_load(const AdeP<T>& a, long long bi, bool upd_x, bool upd_y, bool upd_z, AdeRegs<T>& r) {
-  const bool upd[3] = {upd_x, upd_y, upd_z};
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    if (!upd[c]) continue;
-#pragma unroll
-    for (int p = 0; p < kAdeRegPoles; ++p)
-      if (p < a.P) {
-        r.J[c][p] = a.J[(static_cast<long long>(c) * a.P + p) * a.bn + bi];
-        if (a.kind == kAdeMLorentz) r.Jp[c][p] = a.Jp[(static_cast<long long>(c) * a.P + p) * a.bn + bi];
-      }
-    if (a.kind == kAdeMLorentz) r.Ep[c] = a.Ep[static_cast<long long>(c) * a.bn + bi];
-  }
-}
-
-// ade_e on register-held state (same arithmetic and order); stores the new state.
-template <typename T>
-__device__ __forceinline__ T ade_e_reg(const AdeP<T>& a, int comp, long long bi, int m, T e_cur, T plain,
-                                       const AdeRegs<T>& r) {
-  const T* am = a.mat + 3 * m;
-  const T* ap = a.pole + static_cast<long long>(m) * a.P * 7;
-  T* J = a.J + static_cast<long long>(comp) * a.P * a.bn + bi;
-  if (a.kind == kAdeMLorentz) {
-    T* Jp = a.Jp + static_cast<long long>(comp) * a.P * a.bn + bi;
-    T jsum = 0;
-#pragma unroll
-    for (int p = 0; p < kAdeRegPoles; ++p)
-      if (p < a.P) jsum = jsum + (ap[7 * p + 5] * r.J[comp][p] + ap[7 * p + 6] * r.Jp[comp][p]);
-    const T e_prev = r.Ep[comp];
-    const T e_new = am[1] * e_prev + plain + am[2] * jsum;
-#pragma unroll
-    for (int p = 0; p < kAdeRegPoles; ++p)
-      if (p < a.P) {
-        const T* q = ap + 7 * p;
-        const T jn = q[2] * e_new + q[3] * e_cur + q[4] * e_prev + q[0] * r.J[comp][p] + q[1] * r.Jp[comp][p];
-        Jp[p * a.bn] = r.J[comp][p];
-        J[p * a.bn] = jn;
-      }
-    a.Ep[static_cast<long long>(comp) * a.bn + bi] = e_cur;
-    return e_new;
-  }
-  T jsum = 0;
-#pragma unroll
-  for (int p = 0; p < kAdeRegPoles; ++p)
-    if (p < a.P) jsum = jsum + ap[7 * p + 5] * r.J[comp][p];
-  const T e_new = plain + am[2] * jsum;
-#pragma unroll
-  for (int p = 0; p < kAdeRegPoles; ++p)
-    if (p < a.P) {
-      const T* q = ap + 7 * p;
-      J[p * a.bn] = (a.kind == kAdeDrude) ? q[0] * r.J[comp][p] + q[3] * (e_new + e_cur)
-                                          : q[0] * r.J[comp][p] + q[3] * (e_new - e_cur);
-    }
-  return e_new;
+__global__ void k_ade_box(GridP<T> s, GridP<T> d, AdeP<T> ad, const uint8_t* disp) {
+  const int k = ad.b4 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ad.b5) return;
+  const int j = ad.b2 + blockIdx.y, i = ad.b0 + blockIdx.z;
+  const long long idx = static_cast<long long>(i) * s.sx + static_cast<long long>(j) * s.sy + k;
+  const int m = s.mid[idx];
+  if (!disp[m]) return;
+  const long long bi = static_cast<long long>(i - ad.b0) * ad.bsx + static_cast<long long>(j - ad.b2) * ad.bsy + (k - ad.b4);
+  if (j > 0 && k > 0) d.ex[idx] = ade_e(ad, 0, bi, m, s.ex[idx], d.ex[idx]);
+  if (i > 0 && k > 0) d.ey[idx] = ade_e(ad, 1, bi, m, s.ey[idx], d.ey[idx]);
+  if (i > 0 && j > 0) d.ez[idx] = ade_e(ad, 2, bi, m, s.ez[idx], d.ez[idx]);
 }
 
 // E half-step, 3-D.  Same tiling as k_h3; H values of plane i are carried to
