@@ -230,7 +230,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--path", choices=["auto", "split", "fused", "plain"], default="auto")
     ap.add_argument("--scene", choices=["dispersive", "vacuum", "pml", "tfsf", "nf2ff"], default="dispersive")
-    ap.add_argument("--tile-rows", type=int, default=8)
+    ap.add_argument("--tile-rows", type=int, default=16)
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 plain-form comparison")
     args = ap.parse_args()
 

@@ -7,6 +7,7 @@ point raises.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -159,7 +160,8 @@ def load(path: Path | str | None = None) -> C.CDLL:
     global _lib
     if _lib is not None and path is None:
         return _lib
-    p = Path(path) if path else LIB_PATH
+    # XFB_LIBRARY selects another build of the same library (same C-ABI)
+    p = Path(path) if path else Path(os.environ.get("XFB_LIBRARY", LIB_PATH))
     if not p.exists():
         raise RuntimeError(
             f"{p} is missing: build it with `python -m xfdtd_cuda_b200.build` "

@@ -114,9 +114,7 @@ int launches_per_step(const xfb_handle* h) {
   }
   int bulk = 2;
   if (fused(h)) {
-    bulk = 0;
-    for (int q = 0; q < 4; ++q) bulk += h->n_step_items[step_tile_index(h->tj)][q] > 0;
-    bulk += h->ade_deferred ? 1 : 0;
+    bulk = (h->n_step_items[step_tile_index(h->tj)] > 0 ? 1 : 0) + (h->ade_deferred ? 1 : 0);
   }
   return bulk + (c.tfsf_on ? 1 : 0) + (c.nf_on ? 1 : 0) + (c.probes.empty() ? 0 : 1) +
          static_cast<int>(c.movies.size());

@@ -289,14 +289,17 @@ PsiH<T> psi_h_set(xfb_handle* h, int set) {
 // Tile configurations of the one-sweep kernel: rows per thread R, row warps
 // NWM (tile rows TJ = R * NWM), picked by the launch hint's row count.
 struct StepTile { int r, nwm; };
-constexpr StepTile kStepTiles[3] = {{2, 4}, {2, 8}, {4, 4}};
-constexpr int kStepKinds[4] = {0, 1, 4, 7};  // lean, x-slab planes, ADE box, y/z-slab columns (all)
+constexpr StepTile kStepTiles[2] = {{2, 4}, {2, 8}};
+// region kinds (kStepKinds, bits: 1 x-slab planes, 2 y-slab columns, 8
+// z-slab columns, 4 ADE box): lean, x planes, ADE box, y columns, z columns,
+// y+z corner columns, anything with ADE next to a slab
+constexpr int kStepKindCount = 7;
 
 // Work items of the one-sweep kernel for tiles of TJ x 32 cells: every tile
 // column is cut along i into plane ranges whose cells (with the H halo plane
 // below the range and the halo row and column of the tile) need no more than
 // the range's kind handles.  Ranges are at most `ich` planes long.
-inline void build_step_items(const Compiled& c, int TJ, int NT, bool ade_deferred, std::vector<int4> (&out)[4]) {
+inline void build_step_items(const Compiled& c, int TJ, int NT, bool ade_deferred, std::vector<int4> (&out)[kStepKindCount]) {
   const int nx = c.nx, ny = c.ny, nz = c.nz;
   const int* L = c.pml;
   const int gx = (nz + 31) / 32, gy = (ny + TJ - 1) / TJ;
@@ -305,20 +308,31 @@ inline void build_step_items(const Compiled& c, int TJ, int NT, bool ade_deferre
   auto xs = [&](int p) { return p < L[0] || p >= nx - L[1]; };
   const int* b = c.ade_box;
   const bool ade = !ade_deferred && c.ade_kind != XFB_ADE_NONE && b[1] > b[0];
-  auto kind_of = [](int bits) { return bits == 0 ? 0 : bits == 1 ? 1 : bits == 4 ? 2 : 3; };
+  auto kind_of = [](int bits) {
+    switch (bits) {
+      case 0: return 0;
+      case 1: return 1;
+      case 4: return 2;
+      case 3: return 3;
+      case 9: return 4;
+      case 11: return 5;
+      default: return 6;
+    }
+  };
   for (int by = 0; by < gy; ++by)
     for (int bx = 0; bx < gx; ++bx) {
       const int j0 = by * TJ, k0 = bx * 32;
       const int rlo = std::max(j0 - 1, 0), rhi = std::min(j0 + TJ - 1, ny - 1);
       const int clo = std::max(k0 - 1, 0), chi = std::min(k0 + 31, nz - 1);
-      const bool yz = rlo < L[2] || rhi >= ny - L[3] || clo < L[4] || chi >= nz - L[5];
+      const bool ycol = rlo < L[2] || rhi >= ny - L[3], zcol = clo < L[4] || chi >= nz - L[5];
+      const bool yz = ycol || zcol;
       const bool adecol = ade && j0 < b[3] && j0 + TJ > b[2] && k0 < b[5] && k0 + 32 > b[4];
       auto need = [&](int p) { return (xs(p) ? 1 : 0) | (adecol && p >= b[0] && p < b[1] ? 4 : 0); };
       int p = 0;
       while (p < nx) {
         int q = p + 1, bits;
         if (yz) {
-          bits = 7;
+          bits = 1 | (ycol ? 2 : 0) | (zcol ? 8 : 0) | (adecol ? 4 : 0);
           q = std::min(nx, p + ich);
         } else {
           const int nd = need(p), halo = p > 0 && xs(p - 1) ? 1 : 0;
@@ -353,58 +367,53 @@ inline bool ade_can_defer(const Compiled& c) {
 
 inline int upload_step_items(xfb_handle* h) {
   h->ade_deferred = ade_can_defer(h->c);
-  for (int t = 0; t < 3; ++t) {
-    std::vector<int4> items[4];
+  for (int t = 0; t < 2; ++t) {
+    std::vector<int4> items[kStepKindCount];
     const int nt = (kStepTiles[t].nwm + 1) * 32;
     build_step_items(h->c, kStepTiles[t].r * kStepTiles[t].nwm, nt, h->ade_deferred, items);
-    for (int q = 0; q < 4; ++q) {
-      h->n_step_items[t][q] = static_cast<int>(items[q].size());
-      if (items[q].empty()) continue;
-      int rc = alloc(h, &h->step_items[t][q], items[q].size() * sizeof(int4), false);
-      if (rc) return rc;
-      if ((rc = copy(h, h->step_items[t][q], items[q].data(), items[q].size() * sizeof(int4), cudaMemcpyHostToDevice)))
-        return rc;
-    }
+    // one list, the kind in the high half of .x, the costliest kinds first so
+    // the long items start early and the short ones fill the tail
+    static const int order[kStepKindCount] = {6, 5, 4, 3, 2, 1, 0};
+    std::vector<int4> all;
+    for (int q : order)
+      for (int4 v : items[q]) all.push_back(make_int4(v.x | (q << 16), v.y, v.z, v.w));
+    h->n_step_items[t] = static_cast<int>(all.size());
+    if (all.empty()) continue;
+    int rc = alloc(h, &h->step_items[t], all.size() * sizeof(int4), false);
+    if (rc) return rc;
+    if ((rc = copy(h, h->step_items[t], all.data(), all.size() * sizeof(int4), cudaMemcpyHostToDevice))) return rc;
   }
   return XFB_OK;
 }
 
-template <typename T, int R, int NWM, int KIND>
-void launch_step3(xfb_handle* h, int parity, TimeP tp, cudaStream_t st, const void* items, int n) {
-  using S = StepCfg<T, R, NWM>;
-  // with the ADE update deferred to k_ade_box the step kernels do none
-  AdeP<T> step_ade = ade_params<T>(h);
-  if (h->ade_deferred) step_ade.kind = kAdeNone;
+template <typename T, int R, int NWM>
+void launch_step3(xfb_handle* h, int t, int parity, TimeP tp, cudaStream_t st) {
+  constexpr int NS = 4;
+  using S = StepCfg<T, R, NWM, NS>;
+  if (!h->n_step_items[t]) return;
   static bool attr_set[64] = {};  // per instantiation and device
   const int dev = h->device & 63;
   if (!attr_set[dev]) {
-    cudaFuncSetAttribute(k_step3<T, R, NWM, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::bytes));
+    cudaFuncSetAttribute(k_step3<T, R, NWM, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(S::bytes));
     attr_set[dev] = true;
   }
-  k_step3<T, R, NWM, KIND><<<n, S::NT, S::bytes, st>>>(
+  // with the ADE update deferred to k_ade_box the step kernel does none
+  AdeP<T> step_ade = ade_params<T>(h);
+  if (h->ade_deferred) step_ade.kind = kAdeNone;
+  k_step3<T, R, NWM, NS><<<h->n_step_items[t], S::NT, S::bytes, st>>>(
       grid_params<T>(h, parity), grid_params<T>(h, 1 - parity), pml_params<T>(h), psi_h_set<T>(h, parity),
-      psi_h_set<T>(h, 1 - parity), tfsf_params(h), step_ade, tp, static_cast<const int4*>(items),
+      psi_h_set<T>(h, 1 - parity), tfsf_params(h), step_ade, tp, static_cast<const int4*>(h->step_items[t]),
       as<const T>(h->lut8), h->mat_disp, h->c.n_mat);
 }
 
-template <typename T, int R, int NWM>
-void launch_step3_kinds(xfb_handle* h, int t, int parity, TimeP tp, cudaStream_t st) {
-  const int* n = h->n_step_items[t];
-  void* const* it = h->step_items[t];
-  if (n[0]) launch_step3<T, R, NWM, kStepKinds[0]>(h, parity, tp, st, it[0], n[0]);
-  if (n[1]) launch_step3<T, R, NWM, kStepKinds[1]>(h, parity, tp, st, it[1], n[1]);
-  if (n[2]) launch_step3<T, R, NWM, kStepKinds[2]>(h, parity, tp, st, it[2], n[2]);
-  if (n[3]) launch_step3<T, R, NWM, kStepKinds[3]>(h, parity, tp, st, it[3], n[3]);
-}
-
-// One-sweep step: one launch per region kind present, for the tile the
-// launch hint's row count picks.
+// One-sweep step: one launch over all work items, for the tile the launch
+// hint's row count picks (up to 8 rows: 8-row tiles, else 16 rows).
 template <typename T>
 void launch_fused(xfb_handle* h, int parity, TimeP tp, cudaStream_t st) {
   const int t = step_tile_index(h->tj);
-  if (t == 0) launch_step3_kinds<T, kStepTiles[0].r, kStepTiles[0].nwm>(h, 0, parity, tp, st);
-  else if (t == 1) launch_step3_kinds<T, kStepTiles[1].r, kStepTiles[1].nwm>(h, 1, parity, tp, st);
-  else launch_step3_kinds<T, kStepTiles[2].r, kStepTiles[2].nwm>(h, 2, parity, tp, st);
+  if (t == 0) launch_step3<T, kStepTiles[0].r, kStepTiles[0].nwm>(h, 0, parity, tp, st);
+  else launch_step3<T, kStepTiles[1].r, kStepTiles[1].nwm>(h, 1, parity, tp, st);
 }
 
 // ---- plain path (reference kernel structure) ------------------------------

@@ -71,17 +71,17 @@ __device__ __forceinline__ C4<double> ld_c4(const double* p) {
 }
 
 // Geometry and shared-memory layout of k_step3 (dynamic shared memory).
-template <typename T, int R, int NWM>
+template <typename T, int R, int NWM, int NS_>
 struct StepCfg {
   static constexpr int TK = 32, TJ = R * NWM;
-  static constexpr int NS = 4;               // staging ring depth (power of two)
+  static constexpr int NS = NS_;             // staging ring depth (planes)
   static constexpr int HP = 16 / sizeof(T);  // elements per 16-byte copy
   static constexpr int RW = TK + 2 * HP;     // staged row width: k0-HP .. k0+TK+HP
   static constexpr int RH = TJ + 2;          // staged rows j0-1 .. j0+TJ
   static constexpr int MW = TK + 32;         // material-id row window [k0-16, k0+TK+16)
   static constexpr int HW = TK + 1, HH = TJ + 1;  // shared H plane: row 0 = j0-1, column 0 = k0-1
   static constexpr int HPL = HH * HW;
-  static constexpr int LUTM = 256;           // every material fits (ids are bytes)
+  static constexpr int LUTM = 16;            // materials whose coefficients sit in shared memory
   static constexpr int CW = RW / HP;         // 16-byte chunks per staged field row
   static constexpr int MC = MW / 16;         // 16-byte chunks per material row
   static constexpr int PL = RH * RW;         // elements of one staged component plane
@@ -97,6 +97,7 @@ struct StepCfg {
   static constexpr int min_blocks = fit < 1 ? 1 : fit > 4 ? 4 : fit;
   static_assert(TJ <= 32, "the halo warp covers the k0-1 column with one lane per row");
   static_assert(R >= 2, "the halo warp computes two H cells per plane");
+  static_assert(NS >= 3, "planes i and i+1 in use while one more is in flight");
 };
 
 // Everything an H-cell update reads, gathered once per CTA.
@@ -116,6 +117,7 @@ struct Cell {
   int go;  // global offset inside a field plane (j * sy + k)
   int j, k;
   int py, pz;  // y / z CPML slab index of the cell, or -1
+  int tfl;     // bit 0: on a TFSF H correction line (j = js-1, je or k = ks-1, ke); bit 1: E line (js, je, ks, ke)
 };
 
 // H^{n+1/2} of cell c at plane i: hNext from the staged E^n planes i and i+1
@@ -125,14 +127,15 @@ struct Cell {
 // (pa, p0, p1): the old H psi pair of one slab axis (0 x, 1 y, 2 z; -1 none),
 // loaded one plane ahead; psi of any other slab axis is loaded here.
 template <typename T, int KIND, class Cfg>
-__device__ __forceinline__ void h_cell(const HCtx<T>& x, const T* Fc, const T* Fn, const uint8_t* Mc, const T* sL,
+__device__ __forceinline__ void h_cell(const HCtx<T>& x, const T* Fc, const T* Fn, const uint8_t* Mc, const T* lut,
                                        T* Hc, int i, const Cell& c, bool own, T* ox, T* oy, T* oz, int sxp,
-                                       bool tf_hplane, int pa, T p0, T p1, T& hxv, T& hyv, T& hzv) {
+                                       bool tf_hplane, int pa, T p0, T p1, T& hxv, T& hyv, T& hzv, T& ex_c,
+                                       T& ey_c, T& ez_c, int& m) {
   constexpr int PL = Cfg::PL, RW = Cfg::RW;
-  const int m = Mc[c.mo];
-  const C4<T> cf = ld_c4(sL + 8 * m + 4);  // ch, db/dx, db/dy, db/dz
+  m = Mc[c.mo];
+  const C4<T> cf = ld_c4(lut + 8 * m + 4);  // ch, db/dx, db/dy, db/dz
   const T* f = Fc + c.wf;
-  const T ex_c = f[0], ey_c = f[PL], ez_c = f[2 * PL];
+  ex_c = f[0]; ey_c = f[PL]; ez_c = f[2 * PL];
   const T d_hx_a = f[PL + 1] - ey_c;          // Hx: Ey along z
   const T d_hx_b = f[2 * PL + RW] - ez_c;     // Hx: Ez along y
   const T d_hy_a = Fn[c.wf + 2 * PL] - ez_c;  // Hy: Ez along x
@@ -146,7 +149,7 @@ __device__ __forceinline__ void h_cell(const HCtx<T>& x, const T* Fc, const T* F
   hzv = cf.c * f[5 * PL] + cf.y * d_hz_a - cf.x * d_hz_b;
   const TfsfP& tf = x.tf;
   const int j = c.j, k = c.k;
-  if (tf.on && (tf_hplane || j == tf.js - 1 || j == tf.je || k == tf.ks - 1 || k == tf.ke)) {
+  if (tf_hplane || (c.tfl & 1)) {
     const int jj = j, kk = k;
     const bool iin = i >= tf.is && i <= tf.ie, jin = jj >= tf.js && jj <= tf.je, kin = kk >= tf.ks && kk <= tf.ke;
     if (jin && jj < tf.je && kin) {
@@ -174,12 +177,12 @@ __device__ __forceinline__ void h_cell(const HCtx<T>& x, const T* Fc, const T* F
       if (i == tf.ie) add_inc(hyv, ez_inc(tf, tf.ie, jj, kk), tf.cb[0]);
     }
   }
-  constexpr bool PX = (KIND & 1) != 0, PYZ = (KIND & 2) != 0;
-  if (PX || PYZ) {
+  constexpr bool PX = (KIND & 1) != 0, PY = (KIND & 2) != 0, PZ = (KIND & 8) != 0;
+  if (PX || PY || PZ) {
     const PmlP<T>& pm = x.pm;
     const long long sx = x.s.sx, sy = x.s.sy;
-    const int hsy = PYZ ? c.py : -1;
-    const int hsz = PYZ ? c.pz : -1;
+    const int hsy = PY ? c.py : -1;
+    const int hsz = PZ ? c.pz : -1;
     if (!PX) sxp = -1;
     if (sxp >= 0 || hsy >= 0 || hsz >= 0) {
       if (sxp >= 0) {
@@ -224,15 +227,15 @@ __device__ __forceinline__ void h_cell(const HCtx<T>& x, const T* Fc, const T* F
 // returns the axis or -1.
 template <typename T, int KIND>
 __device__ __forceinline__ int prefetch_h_psi(const HCtx<T>& x, int ip, int sxp, const Cell& c, bool valid, T& v0, T& v1) {
-  constexpr bool PX = (KIND & 1) != 0, PYZ = (KIND & 2) != 0;
+  constexpr bool PX = (KIND & 1) != 0, PY = (KIND & 2) != 0, PZ = (KIND & 8) != 0;
   if (!valid) return -1;
   const PmlP<T>& pm = x.pm;
-  if (PYZ && c.py >= 0) {
+  if (PY && c.py >= 0) {
     const long long p = static_cast<long long>(ip) * pm.ysx + c.py * x.s.sy + c.k;
     v0 = x.ps.hz_y[p]; v1 = x.ps.hx_y[p];
     return 1;
   }
-  if (PYZ && c.pz >= 0) {
+  if (PZ && c.pz >= 0) {
     const long long p = static_cast<long long>(ip) * pm.zsx + static_cast<long long>(c.j) * pm.zsy + c.pz;
     v0 = x.ps.hx_z[p]; v1 = x.ps.hy_z[p];
     return 2;
@@ -250,14 +253,14 @@ __device__ __forceinline__ int prefetch_h_psi(const HCtx<T>& x, int ip, int sxp,
 template <typename T, int KIND>
 __device__ __forceinline__ int prefetch_e_psi(const PmlP<T>& pm, const GridP<T>& s, int ip, int sxe, const Cell& c,
                                               bool valid, T& v0, T& v1) {
-  constexpr bool PX = (KIND & 1) != 0, PYZ = (KIND & 2) != 0;
+  constexpr bool PX = (KIND & 1) != 0, PY = (KIND & 2) != 0, PZ = (KIND & 8) != 0;
   if (!valid) return -1;
-  if (PYZ && c.py >= 0) {
+  if (PY && c.py >= 0) {
     const long long p = static_cast<long long>(ip) * pm.ysx + c.py * s.sy + c.k;
     v0 = pm.ez_y[p]; v1 = pm.ex_y[p];
     return 1;
   }
-  if (PYZ && c.pz >= 0) {
+  if (PZ && c.pz >= 0) {
     const long long p = static_cast<long long>(ip) * pm.zsx + static_cast<long long>(c.j) * pm.zsy + c.pz;
     v0 = pm.ex_z[p]; v1 = pm.ey_z[p];
     return 2;
@@ -270,12 +273,13 @@ __device__ __forceinline__ int prefetch_e_psi(const PmlP<T>& pm, const GridP<T>&
   return -1;
 }
 
-template <typename T, int R, int NWM, int KIND>
-__global__ void __launch_bounds__(StepCfg<T, R, NWM>::NT, StepCfg<T, R, NWM>::min_blocks)
-    k_step3(GridP<T> s, GridP<T> d, PmlP<T> pm, PsiH<T> ps, PsiH<T> pd, TfsfP tf_in, AdeP<T> ad, TimeP tp,
-            const int4* items, const T* lut8, const uint8_t* disp, int n_mat) {
-  constexpr bool PX = (KIND & 1) != 0, PYZ = (KIND & 2) != 0, PML = PX || PYZ;
-  using L = StepCfg<T, R, NWM>;
+// One work item of the one-sweep step, compiled for region kind KIND.
+template <typename T, int R, int NWM, int NS_, int KIND>
+__device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, const PmlP<T>& pm, const PsiH<T>& ps,
+                                          const PsiH<T>& pd, const TfsfP& tf_in, const AdeP<T>& ad, const TimeP& tp,
+                                          int4 item, const T* lut8, const uint8_t* disp, int n_mat) {
+  constexpr bool PX = (KIND & 1) != 0, PY = (KIND & 2) != 0, PZ = (KIND & 8) != 0, PML = PX || PY || PZ;
+  using L = StepCfg<T, R, NWM, NS_>;
   constexpr int NS = L::NS, HP = L::HP, RW = L::RW, RH = L::RH, MW = L::MW, HW = L::HW, TK = L::TK, TJ = L::TJ;
   constexpr int CW = L::CW, MC = L::MC, NT = L::NT, PL = L::PL, HPL = L::HPL;
   constexpr int NFC = (RH * CW + NT - 1) / NT;  // staged field chunks per thread
@@ -290,14 +294,18 @@ __global__ void __launch_bounds__(StepCfg<T, R, NWM>::NT, StepCfg<T, R, NWM>::mi
   HCtx<T> x{s, d, pm, ps, pd, tfsf_at_step(tf_in, cur_step(tp))};
   const TfsfP& tf = x.tf;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int4 item = items[blockIdx.x];  // (k tile, j tile, first plane, end plane)
-  const int k0 = item.x * TK, j0 = item.y * TJ;
+  const int k0 = (item.x & 0xffff) * TK, j0 = item.y * TJ;
   const int i_start = item.z, i_end = item.w;
   const int i_first = i_start > 0 ? i_start - 1 : 0;
   const long long sx = s.sx;
   const int sy = static_cast<int>(s.sy);
-  for (int q = tid; q < n_mat * 8; q += NT) sL[q] = lut8[q];
-  for (int q = tid; q < n_mat; q += NT) sD[q] = disp[q];
+  const bool lut_shared = n_mat <= L::LUTM;
+  if (lut_shared) {
+    for (int q = tid; q < n_mat * 8; q += NT) sL[q] = lut8[q];
+    for (int q = tid; q < n_mat; q += NT) sD[q] = disp[q];
+  }
+  const T* lut = lut_shared ? sL : lut8;          // compact coefficients per material
+  const uint8_t* dtab = lut_shared ? sD : disp;   // dispersive flag per material
   for (int q = tid; q < 2 * 3 * HPL; q += NT) sH[q] = T(0);
 
   // staging chunks of this thread (shared and global offsets inside a plane):
@@ -318,9 +326,8 @@ __global__ void __launch_bounds__(StepCfg<T, R, NWM>::NT, StepCfg<T, R, NWM>::mi
     mso[c] = r * MW + cc * 16;
     mgo[c] = (j0 - 1 + r) * sy + (k0 - 16) + cc * 16;
   }
-  auto stage = [&](int plane) {
+  auto stage = [&](int plane, int st) {
     if (plane <= s.nx) {
-      const int st = plane & (NS - 1);
       const long long pb = static_cast<long long>(plane) * sx;
       const T* gex = s.ex + pb; const T* gey = s.ey + pb; const T* gez = s.ez + pb;
       const T* ghx = s.hx + pb; const T* ghy = s.hy + pb; const T* ghz = s.hz + pb;
@@ -343,7 +350,8 @@ __global__ void __launch_bounds__(StepCfg<T, R, NWM>::NT, StepCfg<T, R, NWM>::mi
     }
     cp_async_commit();
   };
-  for (int q = 0; q < NS - 1; ++q) stage(i_first + q);
+  for (int q = 0; q < NS - 1; ++q) stage(i_first + q, (i_first + q) % NS);
+  int slot = i_first % NS;  // ring slot of plane i
 
   // H cells of this thread: a row warp's R rows at column `lane`; the halo
   // warp's row j0-1 at column `lane` (u = 0) and column k0-1 at row `lane`
@@ -367,13 +375,18 @@ __global__ void __launch_bounds__(StepCfg<T, R, NWM>::NT, StepCfg<T, R, NWM>::mi
     cell[u].go = j * sy + k;
     cell[u].j = j;
     cell[u].k = k;
-    cell[u].py = PYZ ? slab(j, s.ny, pm.L[2], pm.L[3]) : -1;
-    cell[u].pz = PYZ ? slab(k, s.nz, pm.L[4], pm.L[5]) : -1;
+    cell[u].py = PY ? slab(j, s.ny, pm.L[2], pm.L[3]) : -1;
+    cell[u].pz = PZ ? slab(k, s.nz, pm.L[4], pm.L[5]) : -1;
+    cell[u].tfl = tf.on ? ((j == tf.js - 1 || j == tf.je || k == tf.ks - 1 || k == tf.ke) ? 1 : 0) |
+                              ((j == tf.js || j == tf.je || k == tf.ks || k == tf.ke) ? 2 : 0)
+                        : 0;
   }
   // registers: H of the thread's own cells at planes i (new), i-1, i-2 (y, z only)
   T hnx[R], hny[R], hnz[R], hpx[R], hpy[R], hpz[R], hqy[R], hqz[R];
   T eox[R], eoy[R], eoz[R];  // E^n of plane i-1, taken from the ring one iteration earlier
   int em[R];                 // material of those cells
+  T enx[R], eny[R], enz[R];  // E^n of plane i, read by the H pass
+  int enm[R];
   // CPML psi pairs loaded one plane ahead (axis -1: none)
   T ph0[R], ph1[R], pe0[R], pe1[R];
   int pha[R], pea[R];
@@ -381,6 +394,8 @@ __global__ void __launch_bounds__(StepCfg<T, R, NWM>::NT, StepCfg<T, R, NWM>::mi
   for (int u = 0; u < R; ++u) {
     hnx[u] = hny[u] = hnz[u] = hpx[u] = hpy[u] = hpz[u] = hqy[u] = hqz[u] = T(0);
     eox[u] = eoy[u] = eoz[u] = T(0);
+    enx[u] = eny[u] = enz[u] = T(0);
+    enm[u] = 0;
     ph0[u] = ph1[u] = pe0[u] = pe1[u] = T(0);
     pha[u] = pea[u] = -1;
     em[u] = 0;
@@ -399,12 +414,15 @@ __global__ void __launch_bounds__(StepCfg<T, R, NWM>::NT, StepCfg<T, R, NWM>::mi
     const int ie = i - 1;
     const bool do_h = i < i_end;
     const bool write_h = do_h && i >= i_start && row_warp;
+    const int slot_n = slot + 1 == NS ? 0 : slot + 1;      // plane i+1
+    const int slot_p = slot == 0 ? NS - 1 : slot - 1;      // plane i-1, refilled with plane i+NS-1
     cp_async_wait<NS - 3>();  // planes i and i+1 have landed (this thread's copies)
     __syncthreads();          // ... everyone's copies; iteration i-1 is complete everywhere
-    stage(i + NS - 1);        // into the slot of plane i-1, whose last readers finished iteration i-1
-    const T* Fc = sF + (i & (NS - 1)) * 6 * PL;
-    const T* Fn = sF + ((i + 1) & (NS - 1)) * 6 * PL;
-    const uint8_t* Mc = sM + (i & (NS - 1)) * RH * MW;
+    stage(i + NS - 1, slot_p);  // whose last readers finished iteration i-1
+    const T* Fc = sF + slot * 6 * PL;
+    const T* Fn = sF + slot_n * 6 * PL;
+    const uint8_t* Mc = sM + slot * RH * MW;
+    slot = slot_n;
     T* Hc = sH + (i & 1) * 3 * HPL;              // H plane i (written here)
     const T* Hq = sH + ((i + 1) & 1) * 3 * HPL;  // H plane i-1
     // ---- H pass, plane i ----------------------------------------------------
@@ -416,8 +434,8 @@ __global__ void __launch_bounds__(StepCfg<T, R, NWM>::NT, StepCfg<T, R, NWM>::mi
 #pragma unroll
       for (int u = 0; u < R; ++u)
         if ((valid >> u) & 1u)
-          h_cell<T, KIND, L>(x, Fc, Fn, Mc, sL, Hc, i, cell[u], write_h, ox, oy, oz, sxp, tf_hplane, pha[u], ph0[u],
-                             ph1[u], hnx[u], hny[u], hnz[u]);
+          h_cell<T, KIND, L>(x, Fc, Fn, Mc, lut, Hc, i, cell[u], write_h, ox, oy, oz, sxp, tf_hplane, pha[u], ph0[u],
+                             ph1[u], hnx[u], hny[u], hnz[u], enx[u], eny[u], enz[u], enm[u]);
     }
     // ---- E pass, plane ie = i-1 ----------------------------------------------
     if (row_warp && ie >= i_start) {
@@ -434,7 +452,7 @@ __global__ void __launch_bounds__(StepCfg<T, R, NWM>::NT, StepCfg<T, R, NWM>::mi
         const bool jpos = j > 0, kpos = k > 0;
         const bool upd_x = jpos && kpos, upd_y = ipos && kpos, upd_z = ipos && jpos;
         const int m = em[u];
-        const C4<T> cf = ld_c4(sL + 8 * m);  // ce, cb/dx, cb/dy, cb/dz
+        const C4<T> cf = ld_c4(lut + 8 * m);  // ce, cb/dx, cb/dy, cb/dz
         const int hs = c.hs;
         // H^{n+1/2} of plane ie: own value from registers, k-1 from the shared
         // plane, j-1 from the previous row of this thread or the shared plane
@@ -455,13 +473,13 @@ __global__ void __launch_bounds__(StepCfg<T, R, NWM>::NT, StepCfg<T, R, NWM>::mi
         T exv = cf.c * ex_o - cf.z * d_ex_a + cf.y * d_ex_b;
         T eyv = cf.c * ey_o - cf.x * d_ey_a + cf.z * d_ey_b;
         T ezv = cf.c * ez_o - cf.y * d_ez_a + cf.x * d_ez_b;
-        if (has_ade && sD[m]) {
+        if (has_ade && dtab[m]) {
           const long long abi = static_cast<long long>(ie - ad.b0) * ad.bsx + static_cast<long long>(j - ad.b2) * ad.bsy + (k - ad.b4);
           if (upd_x) exv = ade_e(ad, 0, abi, m, ex_o, exv);
           if (upd_y) eyv = ade_e(ad, 1, abi, m, ey_o, eyv);
           if (upd_z) ezv = ade_e(ad, 2, abi, m, ez_o, ezv);
         }
-        if (tf.on && (tf_eplane || j == tf.js || j == tf.je || k == tf.ks || k == tf.ke)) {
+        if (tf_eplane || (c.tfl & 2)) {
           const int i = ie;
           const bool iin = i >= tf.is && i <= tf.ie, jin = j >= tf.js && j <= tf.je, kin = k >= tf.ks && k <= tf.ke;
           if (jin && kin && k < tf.ke) {
@@ -525,9 +543,8 @@ __global__ void __launch_bounds__(StepCfg<T, R, NWM>::NT, StepCfg<T, R, NWM>::mi
       for (int u = 0; u < R; ++u) {
         hqy[u] = hpy[u]; hqz[u] = hpz[u];
         hpx[u] = hnx[u]; hpy[u] = hny[u]; hpz[u] = hnz[u];
-        em[u] = Mc[cell[u].mo];
-        const T* f = Fc + cell[u].wf;
-        eox[u] = f[0]; eoy[u] = f[PL]; eoz[u] = f[2 * PL];
+        em[u] = enm[u];
+        eox[u] = enx[u]; eoy[u] = eny[u]; eoz[u] = enz[u];
       }
     }
     // CPML psi of the next iteration: H of plane i+1, E of plane i
@@ -547,6 +564,27 @@ __global__ void __launch_bounds__(StepCfg<T, R, NWM>::NT, StepCfg<T, R, NWM>::mi
     }
   }
   cp_async_wait<0>();
+}
+
+// The one-sweep step kernel: one CTA per work item (x: k tile | kind << 16,
+// y: j tile, z: first plane, w: end plane); every kind runs its own
+// specialised body, so one launch covers the whole grid.
+constexpr int kStepKinds[7] = {0, 1, 4, 3, 9, 11, 15};
+
+template <typename T, int R, int NWM, int NS_>
+__global__ void __launch_bounds__(StepCfg<T, R, NWM, NS_>::NT, StepCfg<T, R, NWM, NS_>::min_blocks)
+    k_step3(GridP<T> s, GridP<T> d, PmlP<T> pm, PsiH<T> ps, PsiH<T> pd, TfsfP tf_in, AdeP<T> ad, TimeP tp,
+            const int4* items, const T* lut8, const uint8_t* disp, int n_mat) {
+  const int4 item = items[blockIdx.x];
+  switch (item.x >> 16) {
+    case 0: step_item<T, R, NWM, NS_, kStepKinds[0]>(s, d, pm, ps, pd, tf_in, ad, tp, item, lut8, disp, n_mat); break;
+    case 1: step_item<T, R, NWM, NS_, kStepKinds[1]>(s, d, pm, ps, pd, tf_in, ad, tp, item, lut8, disp, n_mat); break;
+    case 2: step_item<T, R, NWM, NS_, kStepKinds[2]>(s, d, pm, ps, pd, tf_in, ad, tp, item, lut8, disp, n_mat); break;
+    case 3: step_item<T, R, NWM, NS_, kStepKinds[3]>(s, d, pm, ps, pd, tf_in, ad, tp, item, lut8, disp, n_mat); break;
+    case 4: step_item<T, R, NWM, NS_, kStepKinds[4]>(s, d, pm, ps, pd, tf_in, ad, tp, item, lut8, disp, n_mat); break;
+    case 5: step_item<T, R, NWM, NS_, kStepKinds[5]>(s, d, pm, ps, pd, tf_in, ad, tp, item, lut8, disp, n_mat); break;
+    default: step_item<T, R, NWM, NS_, kStepKinds[6]>(s, d, pm, ps, pd, tf_in, ad, tp, item, lut8, disp, n_mat); break;
+  }
 }
 
 }  // namespace xfb

@@ -28,7 +28,7 @@ struct xfb_handle {
   bool inited = false;
   long long step = 0;
   unsigned hint_grid[3] = {1, 1, 1}, hint_block[3] = {1, 1, 1};
-  int tk = 32, tj = 8;
+  int tk = 32, tj = 16;
   int path = XFB_PATH_AUTO;  // resolved at init: XFB_PATH_SPLIT or XFB_PATH_FUSED
   int graph_on = 1, graph_steps = 64;
   std::map<int, cudaGraphExec_t> graphs;
@@ -75,10 +75,10 @@ struct xfb_handle {
   long long* t_dev = nullptr;
   unsigned long long* scratch_u64 = nullptr;
   void* plain_c[18] = {};  // per-cell coefficient arrays of the plain path
-  // one-sweep step work items per tile configuration and region kind
-  // (int4: k tile, j tile, first plane, end plane)
-  void* step_items[3][4] = {};
-  int n_step_items[3][4] = {};
+  // one-sweep step work items per tile configuration
+  // (int4: k tile | region kind << 16, j tile, first plane, end plane)
+  void* step_items[2] = {};
+  int n_step_items[2] = {};
   // ADE applied by k_ade_box after the one-sweep step (no dispersive cell
   // takes a TFSF or CPML correction)
   bool ade_deferred = false;
@@ -120,7 +120,7 @@ int upload(xfb_handle* h, void** out, const std::vector<double>& v, bool state =
 long long roundup(long long v, long long m);
 bool fused(const xfb_handle* h);
 // tile configuration of the one-sweep kernel picked by the launch hint's rows
-inline int step_tile_index(int tj) { return tj <= 8 ? 0 : tj <= 16 ? 1 : 2; }
+inline int step_tile_index(int tj) { return tj <= 8 ? 0 : 1; }
 bool plain(const xfb_handle* h);
 int cur_set(const xfb_handle* h);
 void* field_ptr(const xfb_handle* h, int set, int q);

@@ -285,12 +285,15 @@ __device__ __forceinline__ T ade_e(const AdeP<T>& a, int comp, long long bi, int
 
 // Deferred ADE update of the dispersive box after a one-sweep step.  The step
 // kernel stored the plain eNext value of every cell in `d`; this applies the
-// TemplateADEUpdateScheme::updateE recursion (ade_e: same arithmetic, same
-// order) with E^n from `s`, one thread per box cell, k fastest.  Valid only
-// when no dispersive cell also takes a TFSF or CPML correction, which the
+// TemplateADEUpdateScheme::updateE recursion with E^n from `s`, one thread per
+// box cell, k fastest.  All inputs of a cell (E^n, plain values, J, J_prev,
+// E_prev of the three components) are loaded before any update, so the loads
+// overlap; the arithmetic and its order are those of ade_e.  Valid only when
+// no dispersive cell also takes a TFSF or CPML correction, which the
 // reference applies after the ADE update.
 template <typename T>
 __global__ void k_ade_box(GridP<T> s, GridP<T> d, AdeP<T> ad, const uint8_t* disp) {
+  constexpr int MP = 4;  // XFB_MAX_POLES
   const int k = ad.b4 + blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= ad.b5) return;
   const int j = ad.b2 + blockIdx.y, i = ad.b0 + blockIdx.z;
@@ -298,9 +301,62 @@ __global__ void k_ade_box(GridP<T> s, GridP<T> d, AdeP<T> ad, const uint8_t* dis
   const int m = s.mid[idx];
   if (!disp[m]) return;
   const long long bi = static_cast<long long>(i - ad.b0) * ad.bsx + static_cast<long long>(j - ad.b2) * ad.bsy + (k - ad.b4);
-  if (j > 0 && k > 0) d.ex[idx] = ade_e(ad, 0, bi, m, s.ex[idx], d.ex[idx]);
-  if (i > 0 && k > 0) d.ey[idx] = ade_e(ad, 1, bi, m, s.ey[idx], d.ey[idx]);
-  if (i > 0 && j > 0) d.ez[idx] = ade_e(ad, 2, bi, m, s.ez[idx], d.ez[idx]);
+  const bool upd[3] = {j > 0 && k > 0, i > 0 && k > 0, i > 0 && j > 0};
+  T* dd[3] = {d.ex, d.ey, d.ez};
+  const T* ss[3] = {s.ex, s.ey, s.ez};
+  const bool ml = ad.kind == kAdeMLorentz;
+  const int P = ad.P;
+  T ec[3], pl[3], J[3][MP], Jp[3][MP], Ep[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    ec[c] = ss[c][idx];
+    pl[c] = dd[c][idx];
+    Ep[c] = ml ? ad.Ep[c * ad.bn + bi] : T(0);
+#pragma unroll
+    for (int p = 0; p < MP; ++p) {
+      const long long o = (static_cast<long long>(c) * P + p) * ad.bn + bi;
+      J[c][p] = p < P ? ad.J[o] : T(0);
+      Jp[c][p] = (p < P && ml) ? ad.Jp[o] : T(0);
+    }
+  }
+  const T* am = ad.mat + 3 * m;
+  const T* ap = ad.pole + static_cast<long long>(m) * P * 7;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    if (!upd[c]) continue;
+    T e_new;
+    if (ml) {
+      T jsum = 0;
+#pragma unroll
+      for (int p = 0; p < MP; ++p)
+        if (p < P) jsum = jsum + (ap[7 * p + 5] * J[c][p] + ap[7 * p + 6] * Jp[c][p]);
+      e_new = am[1] * Ep[c] + pl[c] + am[2] * jsum;
+#pragma unroll
+      for (int p = 0; p < MP; ++p)
+        if (p < P) {
+          const T* q = ap + 7 * p;
+          const long long o = (static_cast<long long>(c) * P + p) * ad.bn + bi;
+          const T jn = q[2] * e_new + q[3] * ec[c] + q[4] * Ep[c] + q[0] * J[c][p] + q[1] * Jp[c][p];
+          ad.Jp[o] = J[c][p];
+          ad.J[o] = jn;
+        }
+      ad.Ep[c * ad.bn + bi] = ec[c];
+    } else {
+      T jsum = 0;
+#pragma unroll
+      for (int p = 0; p < MP; ++p)
+        if (p < P) jsum = jsum + ap[7 * p + 5] * J[c][p];
+      e_new = pl[c] + am[2] * jsum;
+#pragma unroll
+      for (int p = 0; p < MP; ++p)
+        if (p < P) {
+          const T* q = ap + 7 * p;
+          const long long o = (static_cast<long long>(c) * P + p) * ad.bn + bi;
+          ad.J[o] = (ad.kind == kAdeDrude) ? q[0] * J[c][p] + q[3] * (e_new + ec[c]) : q[0] * J[c][p] + q[3] * (e_new - ec[c]);
+        }
+    }
+    dd[c][idx] = e_new;
+  }
 }
 
 // E half-step, 3-D.  Same tiling as k_h3; H values of plane i are carried to
