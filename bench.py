@@ -215,6 +215,50 @@ def plain_compare(local: int, steps: int, warmup: int):
             "unit": UNIT, "steps": steps, **res, "fp32_fused_over_fp64_plain": res["fp32_fused"] / res["fp64_plain"]}
 
 
+def batched_compare(local: int, steps: int, warmup: int, solo_steps: int = 8):
+    """C4: 64 seeded 3-D scenes (64^3..256^3 inner cells + 8-cell CPML, random
+    sphere/cube scatterer, TFSF Gaussian, FP32) stepped as one batch (one
+    launch of the one-sweep kernel per step, CUDA-graph replay, autotuned
+    tile), device-timed; next to the same scenes stepped one after another
+    through their own handles (each a separate launch sequence)."""
+    import xfdtd_cuda_b200 as X
+    from xfdtd_cuda_b200 import configs
+    sims = configs.batched_sweep()
+    # one scene at a time: device time of solo_steps steps per scene, summed
+    solo_ms, cells = 0.0, 0
+    for s in sims:
+        sc, keep = s.lower()
+        h = X.Handle(sc, keep)
+        h.set_device(local)
+        h.init(solo_steps + 2)
+        h.step(2)
+        solo_ms += h.timed_step(solo_steps)
+        gi = h.info()
+        cells += gi.nx * gi.ny * gi.nz
+        h.close()
+    hs = []
+    for s in sims:
+        sc, keep = s.lower()
+        h = X.Handle(sc, keep)
+        h.set_device(local)
+        hs.append(h)
+    b = X.Batch(hs)
+    b.init(warmup + steps)
+    b.step(warmup)
+    b.sync()
+    ms = b.timed_step(steps)
+    info = b.info()
+    b.close()
+    for h in hs:
+        h.close()
+    return {"workload": "batched sweep: 64 scenes, inner sides U{64..256} (seed 4) + 8-cell CPML, random sphere/cube "
+                        "scatterer (eps_r 1..10, sigma 0..0.1 S/m), TFSF Gaussian, FP32",
+            "unit": UNIT, "cells_per_step": cells, "steps": steps, "value": cells * steps / (ms / 1e3) / 1e6,
+            "ms_per_step": ms / steps, "tile_rows": info["tile_rows"], "work_items_per_step": info["work_items"],
+            "one_at_a_time": {"value": cells * solo_steps / (solo_ms / 1e3) / 1e6, "steps": solo_steps,
+                              "ms_per_step": solo_ms / solo_steps}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -232,6 +276,7 @@ def main():
     ap.add_argument("--scene", choices=["dispersive", "vacuum", "pml", "tfsf", "nf2ff"], default="dispersive")
     ap.add_argument("--tile-rows", type=int, default=16)
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 plain-form comparison")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched 64-scene leg")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -340,9 +385,16 @@ def main():
                "path": "Handle(scene) + init + step + read-back (SimulationHD.run flow), wall clock"}
         h2.close()
 
+    h.close()
     plain = None
     if not args.no_plain and world == 1:
         plain = plain_compare(local, 50, 3)
+    batched = None
+    if not args.no_batch and world == 1:
+        try:
+            batched = batched_compare(local, 30, 10)
+        except Exception as exc:  # reported, not fatal for the headline
+            batched = {"error": str(exc)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -357,9 +409,9 @@ def main():
                           "cells_per_step": cells, "parallelism": f"scene-replica x{world}" if world > 1 else "1 GPU",
                           "l2": "resident state 3.3 GB >> 126 MB L2 (no flush needed)"},
                "e2e": e2e, "roofline": roofline, "step_roofline": step_roof, "cpu_baseline": cpu,
-               "clocks": clk.summary(), "gpu_launches": launches, "kernels": kernels, "vs_fp64_plain": plain}
+               "clocks": clk.summary(), "gpu_launches": launches, "kernels": kernels, "vs_fp64_plain": plain,
+               "batched": batched}
         print(json.dumps(out))
-    h.close()
     if dist:
         dist[1].barrier()
         dist[1].destroy_process_group()

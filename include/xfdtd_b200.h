@@ -291,6 +291,33 @@ int xfb_far_field(xfb_handle* h, int freq, int n_angles, const double* theta,
 int xfb_far_field_static(xfb_handle* h, int freq, int n_angles, const double* theta,
                          const double* phi, double* out);
 
+/* ---- batches of scenes ---------------------------------------------------
+ * No counterpart in the reference (whose SimulationHD runs one scene per
+ * object).  A batch steps many 3-D scenes of one precision together: every
+ * step is one launch of the one-sweep kernel over the work items of all
+ * scenes, plus one launch for all TFSF auxiliary grids, replayed from CUDA
+ * graphs.  Results are identical to stepping each scene alone.  The handles
+ * stay owned by the caller and are read as usual (xfb_read_field, ...) after
+ * xfb_batch_sync; while in a batch they cannot be stepped, initialised or
+ * destroyed on their own (XFB_ERR_STATE). */
+typedef struct xfb_batch xfb_batch;
+/* Group n created handles (same precision, 3-D, one device). */
+int xfb_batch_create(xfb_handle* const* handles, int n, xfb_batch** out);
+/* Tile rows of the one-sweep kernel: 0 = autotune on the first steps (default), 8 or 16. */
+int xfb_batch_set_tile(xfb_batch* b, int rows);
+/* xfb_init every scene for total_steps steps (one-sweep path) and build the batch's work list. */
+int xfb_batch_init(xfb_batch* b, long long total_steps);
+/* Advance every scene n steps (asynchronous). */
+int xfb_batch_step(xfb_batch* b, long long n);
+int xfb_batch_sync(xfb_batch* b);
+/* n steps between CUDA events on the batch's stream; *ms = device time. */
+int xfb_batch_timed_step(xfb_batch* b, long long n, double* ms);
+/* Cells per step over all scenes, tile rows in use (0 before the first step), work items per step. */
+int xfb_batch_info(const xfb_batch* b, long long* cells, int* tile_rows, int* work_items);
+const char* xfb_batch_last_error(const xfb_batch* b);
+/* Release the batch; its handles become independent again. */
+int xfb_batch_destroy(xfb_batch* b);
+
 /* ---- checkpoint / resume ------------------------------------------------ */
 /* Byte size of the full solver state (fields, CPML psi, ADE state, TFSF
  * auxiliary grid, NF2FF accumulators, monitors, step counter). */

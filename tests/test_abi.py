@@ -100,3 +100,41 @@ def test_init_without_device_fails_loudly():
 def test_missing_library_raises(tmp_path):
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         L.load(tmp_path / "libxfdtd_b200.so")
+
+
+def _handle(sim):
+    sc, keep = sim.lower()
+    return X.Handle(sc, keep)
+
+
+def test_batch_validates_its_scenes():
+    a = _handle(configs.dielectric_sphere(cells=20, dl=5e-3, pml=4, precision="fp32", tfsf_inset=3, freqs=()))
+    b = _handle(configs.dielectric_sphere(cells=24, dl=5e-3, pml=4, precision="fp32", tfsf_inset=3, freqs=()))
+    c64 = _handle(configs.dielectric_sphere(cells=20, dl=5e-3, pml=4, precision="fp64", tfsf_inset=3, freqs=()))
+    flat = _handle(configs.cylinder_2d(cells=32, dl=1e-3, pml=4, precision="fp32", radius=0.004, tfsf_inset=3, n_probes=1))
+    with pytest.raises(X.XfbError, match="one precision"):
+        X.Batch([a, c64])
+    with pytest.raises(X.XfbError, match="3-D"):
+        X.Batch([a, flat])
+    with pytest.raises(X.XfbError, match="twice"):
+        X.Batch([a, a])
+    batch = X.Batch([a, b])
+    with pytest.raises(X.XfbError, match="already belongs"):
+        X.Batch([b])
+    with pytest.raises(X.XfbError, match="tile rows"):
+        batch._c(batch.lib.xfb_batch_set_tile(batch.b, 12))
+    # a batched handle refuses to be destroyed on its own; the batch releases it
+    assert a.lib.xfb_destroy(a.h) == L.XFB_ERR_STATE
+    with pytest.raises(X.XfbError, match="not initialised"):
+        batch.step(1)
+    batch.close()
+    assert a.lib.xfb_destroy(a.h) == L.XFB_OK
+    a.h = None
+
+
+def test_batched_sweep_config_is_seeded():
+    s1 = configs.batched_sweep(n=8, seed=4)
+    s2 = configs.batched_sweep(n=8, seed=4)
+    sides = [s.objects[0].shape.size.x for s in s1]
+    assert sides == [s.objects[0].shape.size.x for s in s2]
+    assert all(0.064 - 1e-12 <= x <= 0.256 + 1e-12 for x in sides)

@@ -1,0 +1,79 @@
+"""Batches of scenes (xfb_batch_*): every scene stepped in a batch ends in the
+same state as the same scene stepped alone, bit for bit (the batch runs the
+same kernel bodies on the same inputs), in FP32 and FP64, with CPML, TFSF,
+ADE (deferred box pass), probes and NF2FF; and an FP64 batch agrees with the
+CPU restatement bit for bit."""
+import numpy as np
+import pytest
+
+import xfdtd_cuda_b200 as X
+from xfdtd_cuda_b200 import configs
+from helpers import bit_equal, fields_of, oracle_of
+
+pytestmark = pytest.mark.gpu
+
+
+def _scenes(precision):
+    return [
+        configs.dielectric_sphere(cells=28, dl=5e-3, pml=6, precision=precision, tfsf_inset=5, nf2ff_inset=3,
+                                  freqs=(1.5e9,), radius=0.03, probes=[((0.0, 0.0, 0.0), 2)]),
+        configs.dispersive_sphere(cells=30, dl=4e-3, pml=5, precision=precision, freqs=(2e9,), tfsf_inset=4,
+                                  nf2ff_inset=2, radius=0.02, probes=[((0.01, 0.0, 0.0), 1)]),
+        *configs.batched_sweep(n=3, seed=11, lo=20, hi=44, pml=5, dl=2e-3, precision=precision),
+    ]
+
+
+def _handle(sim, n, path=2):
+    sc, keep = sim.lower()
+    h = X.Handle(sc, keep)
+    h.set_kernel_path(path)
+    h.init(n)
+    return h
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+@pytest.mark.parametrize("tile", [0, 8, 16])
+def test_batch_matches_scenes_stepped_alone(precision, tile):
+    n = 45
+    sims = _scenes(precision)
+    alone = []
+    for s in sims:
+        h = _handle(s, n)
+        h.step(n)
+        h.sync()
+        alone.append(h)
+    hs = [X.Handle(*s.lower()) for s in sims]
+    b = X.Batch(hs, tile_rows=tile)
+    b.init(n)
+    b.step(7)   # the first call autotunes the tile when tile == 0
+    b.step(n - 7)
+    b.sync()
+    info = b.info()
+    assert info["tile_rows"] in (8, 16) and info["work_items"] > 0
+    for h, a in zip(hs, alone):
+        assert bit_equal(fields_of(h, 3), fields_of(a, 3))
+        for p in range(len(h.probe_desc)):
+            assert np.array_equal(h.read_probe(p), a.read_probe(p))
+        if h.info().n_freqs:
+            assert np.array_equal(h.read_nf2ff(0, 1, 2), a.read_nf2ff(0, 1, 2))
+    b.close()
+    # released handles step on their own from where the batch left them
+    with pytest.raises(X.XfbError):
+        hs[0].step(1)  # the run was sized for n steps
+    for h in hs + alone:
+        h.close()
+
+
+def test_fp64_batch_against_oracle():
+    n = 40
+    sims = _scenes("fp64")[:2]
+    hs = [X.Handle(*s.lower()) for s in sims]
+    b = X.Batch(hs)
+    b.init(n)
+    b.step(n)
+    b.sync()
+    for s, h in zip(sims, hs):
+        o = oracle_of(s, n)
+        o.run(n)
+        assert bit_equal(fields_of(h, 3), fields_of(o, 3))
+    b.close()

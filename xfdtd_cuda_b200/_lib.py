@@ -144,6 +144,15 @@ SIGNATURES = [
     ("xfb_read_nf2ff", C.c_int, [_H, C.c_int, C.c_int, C.c_int, _dp, C.c_size_t]),
     ("xfb_far_field", C.c_int, [_H, C.c_int, C.c_int, _dp, _dp, _dp]),
     ("xfb_far_field_static", C.c_int, [_H, C.c_int, C.c_int, _dp, _dp, _dp]),
+    ("xfb_batch_create", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]),
+    ("xfb_batch_set_tile", C.c_int, [C.c_void_p, C.c_int]),
+    ("xfb_batch_init", C.c_int, [C.c_void_p, C.c_longlong]),
+    ("xfb_batch_step", C.c_int, [C.c_void_p, C.c_longlong]),
+    ("xfb_batch_sync", C.c_int, [C.c_void_p]),
+    ("xfb_batch_timed_step", C.c_int, [C.c_void_p, C.c_longlong, C.POINTER(C.c_double)]),
+    ("xfb_batch_info", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("xfb_batch_last_error", C.c_char_p, [C.c_void_p]),
+    ("xfb_batch_destroy", C.c_int, [C.c_void_p]),
     ("xfb_state_size", C.c_int, [_H, C.POINTER(C.c_size_t)]),
     ("xfb_get_state", C.c_int, [_H, C.c_void_p, C.c_size_t]),
     ("xfb_set_state", C.c_int, [_H, C.c_void_p, C.c_size_t]),

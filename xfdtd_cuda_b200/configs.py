@@ -92,3 +92,36 @@ def dispersive_sphere(cells: int = 384, dl: float = 1e-3, pml: int = 12, precisi
     for p, f in probes:
         s.addMonitor(PointMonitor(Vector(*p), f))
     return s
+
+
+def batched_sweep(n: int = 64, seed: int = 4, lo: int = 64, hi: int = 256, pml: int = 8, dl: float = 1e-3,
+                  precision: str = "fp32"):
+    """C4: `n` 3-D scenes with inner sides drawn uniformly from [lo, hi] cells
+    (seeded), each holding one random sphere or cube scatterer (eps_r in
+    [1, 10], sigma in [0, 0.1] S/m) inside an 8-cell CPML, lit by a TFSF
+    Gaussian pulse.  Returns the list of Simulation objects."""
+    rng = np.random.default_rng(seed)
+    sims = []
+    for q in range(n):
+        side_cells = int(rng.integers(lo, hi + 1))
+        side = side_cells * dl
+        s = Simulation(dl, dl, dl, 0.9, precision=precision)
+        h = side / 2
+        s.addObject(Object("domain", Cube(Vector(-h, -h, -h), Vector(side, side, side)), Material.createAir()))
+        eps = float(rng.uniform(1, 10))
+        sig = float(rng.uniform(0, 0.1))
+        size = float(rng.uniform(0.15, 0.35)) * side
+        c = [float(rng.uniform(-0.1, 0.1)) * side for _ in range(3)]
+        mat = Material(f"m{q}", ElectroMagneticProperty(eps, 1.0, sig, 0.0))
+        if rng.integers(2):
+            shape = Sphere(Vector(*c), size / 2)
+        else:
+            shape = Cube(Vector(*(x - size / 2 for x in c)), Vector(size, size, size))
+        s.addObject(Object(f"scatterer{q}", shape, mat))
+        inset = max(3, side_cells // 16)
+        s.addWaveformSource(TFSF3D(inset, inset, inset, float(rng.uniform(0, math.pi)), float(rng.uniform(0, 2 * math.pi)),
+                                   float(rng.uniform(0, math.pi)), _gaussian(dl)))
+        for d in range(6):
+            s.addBoundary(PML(pml, d))
+        sims.append(s)
+    return sims

@@ -120,6 +120,29 @@ int launches_per_step(const xfb_handle* h) {
          static_cast<int>(c.movies.size());
 }
 
+int batch_err(xfb_batch* b, int code, const std::string& m) {
+  if (b) b->err = m;
+  g_err = m;
+  return code;
+}
+
+void batch_free(xfb_batch* b) {
+  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  b->graphs.clear();
+  void* ps[5] = {b->scenes, b->aux, b->items[0], b->items[1], b->t_dev};
+  for (void* p : ps) cudaFree(p);
+  b->scenes = b->aux = b->items[0] = b->items[1] = nullptr;
+  b->t_dev = nullptr;
+  b->n_items[0] = b->n_items[1] = b->n_aux = 0;
+  b->inited = false;
+}
+
+// A handle that a batch steps may only be read, not stepped or re-sized.
+int not_batched(xfb_handle* h) {
+  if (h && h->batch) return set_err(h, XFB_ERR_STATE, "the handle is stepped by a batch (xfb_batch_destroy releases it)");
+  return XFB_OK;
+}
+
 int check_handle(xfb_handle* h, bool need_init) {
   if (!h) return set_err(nullptr, XFB_ERR_INVALID, "null handle");
   if (need_init && !h->inited) return set_err(h, XFB_ERR_STATE, "handle not initialised (call xfb_init or xfb_run)");
@@ -203,6 +226,7 @@ int xfb_create(const xfb_scene* scene, xfb_handle** out) {
 
 int xfb_destroy(xfb_handle* h) {
   if (!h) return XFB_OK;
+  if (int rc = not_batched(h)) return rc;
   if (h->device >= 0) {
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
@@ -269,6 +293,7 @@ int xfb_prepare_tables(xfb_handle* h, long long total_steps) {
 
 int xfb_init(xfb_handle* h, long long total_steps) {
   if (!h) return set_err(nullptr, XFB_ERR_INVALID, "null handle");
+  if (int rc = not_batched(h)) return rc;
   if (total_steps < 0 || total_steps > (1LL << 31)) return set_err(h, XFB_ERR_INVALID, "total_steps out of range");
   if (h->device < 0) {
     int n = 0;
@@ -305,7 +330,7 @@ int xfb_init(xfb_handle* h, long long total_steps) {
 
 int xfb_step(xfb_handle* h, long long n) {
   int rc = check_handle(h, true);
-  if (rc) return rc;
+  if (rc || (rc = not_batched(h))) return rc;
   if (n < 0) return set_err(h, XFB_ERR_INVALID, "negative step count");
   if (h->step + n > h->c.total_steps)
     return set_err(h, XFB_ERR_RANGE, "steps beyond the count xfb_init sized the run for");
@@ -322,7 +347,7 @@ int xfb_sync(xfb_handle* h) {
 
 int xfb_timed_step(xfb_handle* h, long long n, double* ms) {
   int rc = check_handle(h, true);
-  if (rc) return rc;
+  if (rc || (rc = not_batched(h))) return rc;
   if (!ms) return set_err(h, XFB_ERR_INVALID, "null output");
   cudaEvent_t a, b;
   XFB_CUDA(h, cudaEventCreate(&a));
@@ -344,7 +369,7 @@ int xfb_timed_step(xfb_handle* h, long long n, double* ms) {
 
 int xfb_profile_kernels(xfb_handle* h, long long n, double* ms, long long* launches) {
   int rc = check_handle(h, true);
-  if (rc) return rc;
+  if (rc || (rc = not_batched(h))) return rc;
   if (!ms || !launches || n < 0) return set_err(h, XFB_ERR_INVALID, "bad arguments");
   if (h->step + n > h->c.total_steps) return set_err(h, XFB_ERR_RANGE, "steps beyond the count xfb_init sized the run for");
   XFB_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -560,7 +585,7 @@ int xfb_get_state(xfb_handle* h, void* dst, size_t len) {
 
 int xfb_set_state(xfb_handle* h, const void* src, size_t len) {
   int rc = check_handle(h, true);
-  if (rc) return rc;
+  if (rc || (rc = not_batched(h))) return rc;
   size_t need;
   if ((rc = xfb_state_size(h, &need))) return rc;
   if (!src || len < need) return set_err(h, XFB_ERR_RANGE, "state buffer too small");
@@ -628,6 +653,151 @@ int xfb_compiled_view_get(const xfb_handle* h, xfb_compiled_view* v) {
   v->freqs = c.freqs.data();
   v->nf2ff_te = c.te.data();
   v->nf2ff_th = c.th.data();
+  return XFB_OK;
+}
+
+
+// ---- batches of scenes -------------------------------------------------------
+
+int xfb_batch_create(xfb_handle* const* handles, int n, xfb_batch** out) {
+  if (!handles || n <= 0 || !out) return set_err(nullptr, XFB_ERR_INVALID, "null handles or output, or n <= 0");
+  *out = nullptr;
+  for (int q = 0; q < n; ++q) {
+    xfb_handle* h = handles[q];
+    if (!h) return set_err(nullptr, XFB_ERR_INVALID, "null handle in the batch");
+    if (h->batch) return set_err(h, XFB_ERR_STATE, "handle already belongs to a batch");
+    if (h->c.dim != 3) return set_err(h, XFB_ERR_INVALID, "batches hold 3-D scenes only");
+    if (h->c.prec != handles[0]->c.prec) return set_err(h, XFB_ERR_INVALID, "all scenes of a batch share one precision");
+    for (int r = 0; r < q; ++r)
+      if (handles[r] == h) return set_err(h, XFB_ERR_INVALID, "a handle appears twice in the batch");
+  }
+  xfb_batch* b = new (std::nothrow) xfb_batch();
+  if (!b) return set_err(nullptr, XFB_ERR_OOM, "host allocation failed");
+  b->hs.assign(handles, handles + n);
+  b->prec = handles[0]->c.prec;
+  for (xfb_handle* h : b->hs) h->batch = b;
+  *out = b;
+  return XFB_OK;
+}
+
+int xfb_batch_set_tile(xfb_batch* b, int rows) {
+  if (!b) return set_err(nullptr, XFB_ERR_INVALID, "null batch");
+  if (rows != 0 && rows != 8 && rows != 16) return batch_err(b, XFB_ERR_INVALID, "tile rows must be 0 (autotune), 8 or 16");
+  b->tile_req = rows;
+  b->tile = -1;
+  return XFB_OK;
+}
+
+int xfb_batch_init(xfb_batch* b, long long total_steps) {
+  if (!b) return set_err(nullptr, XFB_ERR_INVALID, "null batch");
+  if (b->inited) {
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->stream);
+    batch_free(b);
+  }
+  int dev = b->hs[0]->device;
+  if (dev < 0) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+      cudaGetLastError();
+      return batch_err(b, XFB_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    if (cudaGetDevice(&dev) != cudaSuccess) return batch_err(b, XFB_ERR_CUDA, "cudaGetDevice");
+  }
+  b->device = dev;
+  b->cells = 0;
+  for (xfb_handle* h : b->hs) {
+    if (h->device >= 0 && h->device != dev) return batch_err(b, XFB_ERR_INVALID, "all scenes of a batch run on one device");
+    h->batch = nullptr;  // xfb_init is refused for batched handles
+    if (h->device < 0) cudaSetDevice(dev);  // xfb_init adopts the current device
+    h->path = XFB_PATH_FUSED;
+    int rc = xfb_init(h, total_steps);
+    h->batch = b;
+    if (rc) return batch_err(b, rc, "scene init failed: " + h->err);
+    b->cells += static_cast<long long>(h->c.nx) * h->c.ny * h->c.nz;
+  }
+  if (cudaSetDevice(dev) != cudaSuccess) return batch_err(b, XFB_ERR_CUDA, "cudaSetDevice");
+  if (!b->stream && cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return batch_err(b, XFB_ERR_CUDA, "cudaStreamCreate");
+  int rc;
+  try {
+    rc = b->prec == XFB_FP64 ? batch_init<double>(b) : batch_init<float>(b);
+  } catch (const std::bad_alloc&) {
+    rc = batch_err(b, XFB_ERR_OOM, "host allocation failed during batch init");
+  }
+  if (rc) return rc;
+  b->step = 0;
+  b->total = total_steps;
+  b->tile = -1;
+  b->inited = true;
+  return XFB_OK;
+}
+
+int xfb_batch_step(xfb_batch* b, long long n) {
+  if (!b) return set_err(nullptr, XFB_ERR_INVALID, "null batch");
+  if (!b->inited) return batch_err(b, XFB_ERR_STATE, "batch not initialised (call xfb_batch_init)");
+  if (n < 0) return batch_err(b, XFB_ERR_INVALID, "negative step count");
+  if (b->step + n > b->total) return batch_err(b, XFB_ERR_RANGE, "steps beyond the count xfb_batch_init sized the run for");
+  if (cudaSetDevice(b->device) != cudaSuccess) return batch_err(b, XFB_ERR_CUDA, "cudaSetDevice");
+  return b->prec == XFB_FP64 ? batch_run<double>(b, n) : batch_run<float>(b, n);
+}
+
+int xfb_batch_sync(xfb_batch* b) {
+  if (!b) return set_err(nullptr, XFB_ERR_INVALID, "null batch");
+  if (!b->inited) return batch_err(b, XFB_ERR_STATE, "batch not initialised");
+  cudaSetDevice(b->device);
+  cudaError_t e = cudaStreamSynchronize(b->stream);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return batch_err(b, XFB_ERR_CUDA, cudaGetErrorString(e));
+  return XFB_OK;
+}
+
+int xfb_batch_timed_step(xfb_batch* b, long long n, double* ms) {
+  int rc = xfb_batch_sync(b);
+  if (rc) return rc;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, b->stream);
+  rc = xfb_batch_step(b, n);
+  cudaEventRecord(e1, b->stream);
+  cudaEventSynchronize(e1);
+  float t = 0;
+  cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (ms) *ms = t;
+  return rc ? rc : xfb_batch_sync(b);
+}
+
+int xfb_batch_info(const xfb_batch* b, long long* cells, int* tile_rows, int* work_items) {
+  if (!b) return set_err(nullptr, XFB_ERR_INVALID, "null batch");
+  if (cells) *cells = b->cells;
+  const int t = b->tile < 0 ? 1 : b->tile;
+  if (tile_rows) *tile_rows = b->tile < 0 ? 0 : kStepTileRows[t];
+  if (work_items) *work_items = b->n_items[t];
+  return XFB_OK;
+}
+
+const char* xfb_batch_last_error(const xfb_batch* b) { return b ? b->err.c_str() : g_err.c_str(); }
+
+int xfb_batch_destroy(xfb_batch* b) {
+  if (!b) return XFB_OK;
+  if (b->inited) {
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->stream);
+  }
+  for (xfb_handle* h : b->hs) {
+    h->batch = nullptr;
+    // the handle's own step counter continues from where the batch left it
+    if (h->inited && h->t_dev) {
+      cudaMemcpyAsync(h->t_dev, &h->step, sizeof(long long), cudaMemcpyHostToDevice, h->stream);
+      cudaStreamSynchronize(h->stream);
+    }
+  }
+  batch_free(b);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
   return XFB_OK;
 }
 

@@ -299,12 +299,13 @@ constexpr int kStepKindCount = 7;
 // column is cut along i into plane ranges whose cells (with the H halo plane
 // below the range and the halo row and column of the tile) need no more than
 // the range's kind handles.  Ranges are at most `ich` planes long.
-inline void build_step_items(const Compiled& c, int TJ, int NT, bool ade_deferred, std::vector<int4> (&out)[kStepKindCount]) {
+inline void build_step_items(const Compiled& c, int TJ, int NT, bool ade_deferred, std::vector<int4> (&out)[kStepKindCount],
+                             int plane_chunk = 0) {
   const int nx = c.nx, ny = c.ny, nz = c.nz;
   const int* L = c.pml;
   const int gx = (nz + 31) / 32, gy = (ny + TJ - 1) / TJ;
   const int nch = chunks_for(gx * gy, nx, NT);
-  const int ich = std::max(8, (nx + nch - 1) / nch);
+  const int ich = plane_chunk > 0 ? plane_chunk : std::max(8, (nx + nch - 1) / nch);
   auto xs = [&](int p) { return p < L[0] || p >= nx - L[1]; };
   const int* b = c.ade_box;
   const bool ade = !ade_deferred && c.ade_kind != XFB_ADE_NONE && b[1] > b[0];
@@ -497,6 +498,42 @@ void plain_pml(xfb_handle* h, const GridP<T>& g) {
   }
 }
 
+// Monitors of one step (NF2FF accumulation, probes, movie frames) on the
+// fields after the step, enqueued on stream s.
+template <typename T>
+void enqueue_records(xfb_handle* h, int parity, TimeP tp, cudaStream_t s, Prof* pf) {
+  const Compiled& c = h->c;
+  GridP<T> g = grid_params<T>(h, fused(h) ? 1 - parity : 0);
+  if (c.nf_on) {
+    NfP nf{};
+    nf.nfreq = static_cast<int>(c.freqs.size());
+    for (int q = 0; q < 6; ++q) nf.box[q] = c.nf[q];
+    for (int q = 0; q < 7; ++q) nf.off[q] = h->nf_off[q];
+    nf.npts = h->nf_npts;
+    nf.acc = h->nf_acc; nf.te = h->te; nf.th = h->th;
+    nf.total_steps = c.total_steps;
+    prof_begin(h, pf, XFB_K_NF2FF);
+    k_nf2ff<T><<<static_cast<unsigned>((h->nf_npts + 255) / 256), 256, 0, s>>>(g, nf, tp);
+    prof_end(h, pf);
+  }
+  if (!c.probes.empty()) {
+    ProbeP pr{static_cast<int>(c.probes.size()), h->probe_idx, h->probe_field, h->probe_out, c.total_steps};
+    prof_begin(h, pf, XFB_K_PROBE);
+    k_probe<T><<<(pr.n + 127) / 128, 128, 0, s>>>(g, pr, tp);
+    prof_end(h, pf);
+  }
+  for (size_t m = 0; m < c.movies.size(); ++m) {
+    const xfb_movie& mv = c.movies[m];
+    const int n0 = mv.hi[0] - mv.lo[0], n1 = mv.hi[1] - mv.lo[1], n2 = mv.hi[2] - mv.lo[2];
+    const long long per = static_cast<long long>(n0) * n1 * n2;
+    const int blocks = static_cast<int>(std::min<long long>((per + 255) / 256, 1024));
+    prof_begin(h, pf, XFB_K_MOVIE);
+    k_movie<T><<<blocks, 256, 0, s>>>(as<const T>(field_ptr(h, fused(h) ? 1 - parity : 0, mv.field)), h->sx, h->sy, mv.lo[0], mv.lo[1], mv.lo[2], n0, n1, n2,
+                                      mv.interval, h->movie_out[m], h->movie_frames[m], tp);
+    prof_end(h, pf);
+  }
+}
+
 template <typename T>
 void enqueue_step(xfb_handle* h, int off, Prof* pf = nullptr) {
   const Compiled& c = h->c;
@@ -579,34 +616,7 @@ void enqueue_step(xfb_handle* h, int off, Prof* pf = nullptr) {
     k_e2<T><<<grd, bx, 0, s>>>(g, pm, tf, tp, ich);
     prof_end(h, pf);
   }
-  if (c.nf_on) {
-    NfP nf{};
-    nf.nfreq = static_cast<int>(c.freqs.size());
-    for (int q = 0; q < 6; ++q) nf.box[q] = c.nf[q];
-    for (int q = 0; q < 7; ++q) nf.off[q] = h->nf_off[q];
-    nf.npts = h->nf_npts;
-    nf.acc = h->nf_acc; nf.te = h->te; nf.th = h->th;
-    nf.total_steps = c.total_steps;
-    prof_begin(h, pf, XFB_K_NF2FF);
-    k_nf2ff<T><<<static_cast<unsigned>((h->nf_npts + 255) / 256), 256, 0, s>>>(g, nf, tp);
-    prof_end(h, pf);
-  }
-  if (!c.probes.empty()) {
-    ProbeP pr{static_cast<int>(c.probes.size()), h->probe_idx, h->probe_field, h->probe_out, c.total_steps};
-    prof_begin(h, pf, XFB_K_PROBE);
-    k_probe<T><<<(pr.n + 127) / 128, 128, 0, s>>>(g, pr, tp);
-    prof_end(h, pf);
-  }
-  for (size_t m = 0; m < c.movies.size(); ++m) {
-    const xfb_movie& mv = c.movies[m];
-    const int n0 = mv.hi[0] - mv.lo[0], n1 = mv.hi[1] - mv.lo[1], n2 = mv.hi[2] - mv.lo[2];
-    const long long per = static_cast<long long>(n0) * n1 * n2;
-    const int blocks = static_cast<int>(std::min<long long>((per + 255) / 256, 1024));
-    prof_begin(h, pf, XFB_K_MOVIE);
-    k_movie<T><<<blocks, 256, 0, s>>>(as<const T>(field_ptr(h, fused(h) ? 1 - parity : 0, mv.field)), h->sx, h->sy, mv.lo[0], mv.lo[1], mv.lo[2], n0, n1, n2,
-                                      mv.interval, h->movie_out[m], h->movie_frames[m], tp);
-    prof_end(h, pf);
-  }
+  enqueue_records<T>(h, parity, tp, s, pf);
 }
 
 template <typename T>
@@ -712,6 +722,190 @@ void launch_nonfinite(xfb_handle* h) {
   }
 }
 
+// ---- batches of scenes -----------------------------------------------------
+template <typename T>
+BatchScene<T> batch_scene(xfb_handle* h) {
+  BatchScene<T> b{};
+  b.g[0] = grid_params<T>(h, 0);
+  b.g[1] = grid_params<T>(h, 1);
+  b.psh[0] = psi_h_set<T>(h, 0);
+  b.psh[1] = psi_h_set<T>(h, 1);
+  b.pm = pml_params<T>(h);
+  b.tf = tfsf_params(h);
+  b.ad = ade_params<T>(h);
+  if (h->ade_deferred) b.ad.kind = kAdeNone;
+  b.lut8 = as<const T>(h->lut8);
+  b.disp = h->mat_disp;
+  b.n_mat = h->c.n_mat;
+  return b;
+}
+
+inline int batch_upload(xfb_batch* b, void** dst, const void* src, size_t bytes) {
+  cudaError_t e = cudaMalloc(dst, bytes);
+  if (e != cudaSuccess) return batch_err(b, XFB_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  e = cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return batch_err(b, XFB_ERR_CUDA, std::string("batch upload: ") + cudaGetErrorString(e));
+  return XFB_OK;
+}
+
+// Device tables of an initialised batch: scene parameters, TFSF auxiliary
+// grids, and for both tile configurations one work list over all scenes
+// (costliest region kinds first; whole columns per item when the batch has
+// enough columns to fill the GPU several times over).
+template <typename T>
+int batch_init(xfb_batch* b) {
+  std::vector<BatchScene<T>> sc;
+  std::vector<AuxScene> aux;
+  for (xfb_handle* h : b->hs) {
+    sc.push_back(batch_scene<T>(h));
+    const Compiled& c = h->c;
+    if (c.tfsf_on)
+      aux.push_back(AuxScene{h->e_aux, h->e_aux + (c.aux_nl + 1), h->h_aux, h->src, c.aux_ceih, c.aux_chie, c.aux_abc,
+                             c.aux_nl});
+  }
+  int rc;
+  if ((rc = batch_upload(b, &b->scenes, sc.data(), sc.size() * sizeof(BatchScene<T>)))) return rc;
+  b->n_aux = static_cast<int>(aux.size());
+  if (b->n_aux && (rc = batch_upload(b, &b->aux, aux.data(), aux.size() * sizeof(AuxScene)))) return rc;
+  for (int t = 0; t < 2; ++t) {
+    const int TJ = kStepTiles[t].r * kStepTiles[t].nwm, NT = (kStepTiles[t].nwm + 1) * 32;
+    long long columns = 0;
+    for (xfb_handle* h : b->hs) columns += static_cast<long long>((h->c.nz + 31) / 32) * ((h->c.ny + TJ - 1) / TJ);
+    const bool whole = columns >= 8LL * 148 * 2;
+    std::vector<int4> per_kind[kStepKindCount];
+    for (size_t q = 0; q < b->hs.size(); ++q) {
+      const xfb_handle* h = b->hs[q];
+      std::vector<int4> items[kStepKindCount];
+      build_step_items(h->c, TJ, NT, h->ade_deferred, items, whole ? h->c.nx : 0);
+      for (int k = 0; k < kStepKindCount; ++k)
+        for (int4 v : items[k]) per_kind[k].push_back(make_int4(v.x | (k << 12) | (static_cast<int>(q) << 16), v.y, v.z, v.w));
+    }
+    std::vector<int4> all;
+    for (int k = kStepKindCount - 1; k >= 0; --k) {
+      // within a kind, longer plane ranges first
+      std::stable_sort(per_kind[k].begin(), per_kind[k].end(), [](const int4& a, const int4& c) { return a.w - a.z > c.w - c.z; });
+      all.insert(all.end(), per_kind[k].begin(), per_kind[k].end());
+    }
+    b->n_items[t] = static_cast<int>(all.size());
+    if (!all.empty() && (rc = batch_upload(b, &b->items[t], all.data(), all.size() * sizeof(int4)))) return rc;
+  }
+  cudaError_t e = cudaMalloc(&b->t_dev, sizeof(long long));
+  if (e != cudaSuccess) return batch_err(b, XFB_ERR_OOM, "cudaMalloc (batch step counter)");
+  e = cudaMemsetAsync(b->t_dev, 0, sizeof(long long), b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return batch_err(b, XFB_ERR_CUDA, cudaGetErrorString(e));
+  return XFB_OK;
+}
+
+template <typename T, int R, int NWM>
+void batch_step3(xfb_batch* b, int t, TimeP tp, int parity) {
+  constexpr int NS = 4;
+  using S = StepCfg<T, R, NWM, NS>;
+  static bool attr_set[64] = {};
+  if (!attr_set[b->device & 63]) {
+    cudaFuncSetAttribute(k_step3_batch<T, R, NWM, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(S::bytes));
+    attr_set[b->device & 63] = true;
+  }
+  k_step3_batch<T, R, NWM, NS><<<b->n_items[t], S::NT, S::bytes, b->stream>>>(
+      static_cast<const BatchScene<T>*>(b->scenes), static_cast<const int4*>(b->items[t]), tp, parity);
+}
+
+// One step of every scene: TFSF auxiliary grids, the one-sweep kernel over
+// all work items, deferred ADE passes, monitors.
+template <typename T>
+void batch_enqueue_step(xfb_batch* b, int off, int t) {
+  TimeP tp{b->t_dev, off};
+  const int parity = static_cast<int>((b->step + off) & 1);
+  if (b->n_aux) k_aux_batch<<<b->n_aux, 1024, 0, b->stream>>>(static_cast<const AuxScene*>(b->aux), tp);
+  if (b->n_items[t]) {
+    if (t == 0) batch_step3<T, kStepTiles[0].r, kStepTiles[0].nwm>(b, 0, tp, parity);
+    else batch_step3<T, kStepTiles[1].r, kStepTiles[1].nwm>(b, 1, tp, parity);
+  }
+  for (xfb_handle* h : b->hs) {
+    const Compiled& c = h->c;
+    if (h->ade_deferred) {
+      const int* bx = c.ade_box;
+      dim3 grd((bx[5] - bx[4] + 127) / 128, bx[3] - bx[2], bx[1] - bx[0]);
+      k_ade_box<T><<<grd, 128, 0, b->stream>>>(grid_params<T>(h, parity), grid_params<T>(h, 1 - parity),
+                                               ade_params<T>(h), h->mat_disp);
+    }
+    if (c.nf_on || !c.probes.empty() || !c.movies.empty()) enqueue_records<T>(h, parity, tp, b->stream, nullptr);
+  }
+}
+
+template <typename T>
+int batch_chunk(xfb_batch* b, int n, int t, bool graph) {
+  auto enqueue = [&]() {
+    for (int q = 0; q < n; ++q) batch_enqueue_step<T>(b, q, t);
+    k_bump<<<1, 1, 0, b->stream>>>(b->t_dev, n);
+  };
+  cudaError_t e = cudaSuccess;
+  if (graph) {
+    const int key = (n * 2 + static_cast<int>(b->step & 1)) * 2 + t;
+    auto it = b->graphs.find(key);
+    if (it == b->graphs.end()) {
+      cudaGraph_t g;
+      e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+      if (e != cudaSuccess) return batch_err(b, XFB_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+      enqueue();
+      e = cudaStreamEndCapture(b->stream, &g);
+      if (e != cudaSuccess) return batch_err(b, XFB_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+      cudaGraphExec_t ex;
+      e = cudaGraphInstantiate(&ex, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return batch_err(b, XFB_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+      it = b->graphs.emplace(key, ex).first;
+    }
+    e = cudaGraphLaunch(it->second, b->stream);
+  } else {
+    enqueue();
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) return batch_err(b, XFB_ERR_CUDA, cudaGetErrorString(e));
+  b->step += n;
+  for (xfb_handle* h : b->hs) h->step += n;
+  return XFB_OK;
+}
+
+// Advance every scene n steps.  With tile autotuning on, the first call
+// times one chunk with each tile configuration (results do not depend on the
+// tile) and keeps the faster for the rest of the run.
+template <typename T>
+int batch_run(xfb_batch* b, long long n) {
+  int rc;
+  if (b->tile < 0) {
+    if (b->tile_req == 8 || b->tile_req == 16 || n < 2) {
+      b->tile = b->tile_req == 8 ? 0 : 1;
+    } else {
+      const int probe = static_cast<int>(std::min<long long>(4, n / 2));
+      float ms[2] = {0, 0};
+      cudaEvent_t e0, e1;
+      cudaEventCreate(&e0);
+      cudaEventCreate(&e1);
+      for (int t = 0; t < 2; ++t) {
+        cudaEventRecord(e0, b->stream);
+        if ((rc = batch_chunk<T>(b, probe, t, false))) return rc;
+        cudaEventRecord(e1, b->stream);
+        cudaError_t e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) return batch_err(b, XFB_ERR_CUDA, cudaGetErrorString(e));
+        cudaEventElapsedTime(&ms[t], e0, e1);
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      b->tile = ms[0] <= ms[1] ? 0 : 1;
+      n -= 2 * probe;
+    }
+  }
+  while (n > 0) {
+    const int chunk = static_cast<int>(std::min<long long>(n, b->graph_steps));
+    if ((rc = batch_chunk<T>(b, chunk, b->tile, true))) return rc;
+    n -= chunk;
+  }
+  return XFB_OK;
+}
+
 }  // namespace xfb
 
 #define XFB_INSTANTIATE_ENGINE(T)                                                          \
@@ -722,4 +916,6 @@ void launch_nonfinite(xfb_handle* h) {
   template int read_field_t<T>(xfb_handle*, int, double*);                                 \
   template int write_field_t<T>(xfb_handle*, int, const double*);                          \
   template void launch_nonfinite<T>(xfb_handle*);                                          \
+  template int batch_init<T>(xfb_batch*);                                                  \
+  template int batch_run<T>(xfb_batch*, long long);                                        \
   }

@@ -100,13 +100,16 @@ struct StepCfg {
   static_assert(NS >= 3, "planes i and i+1 in use while one more is in flight");
 };
 
-// Everything an H-cell update reads, gathered once per CTA.
+// Everything an H-cell update reads (references to the launch's parameters,
+// so nothing is copied to local memory).
 template <typename T>
 struct HCtx {
-  GridP<T> s, d;
-  PmlP<T> pm;
-  PsiH<T> ps, pd;
-  TfsfP tf;
+  const GridP<T>& s;
+  const GridP<T>& d;
+  const PmlP<T>& pm;
+  const PsiH<T>& ps;
+  const PsiH<T>& pd;
+  const TfsfP& tf;
 };
 
 // Per-thread constants of one cell of the tile, computed once per CTA.
@@ -276,8 +279,8 @@ __device__ __forceinline__ int prefetch_e_psi(const PmlP<T>& pm, const GridP<T>&
 // One work item of the one-sweep step, compiled for region kind KIND.
 template <typename T, int R, int NWM, int NS_, int KIND>
 __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, const PmlP<T>& pm, const PsiH<T>& ps,
-                                          const PsiH<T>& pd, const TfsfP& tf_in, const AdeP<T>& ad, const TimeP& tp,
-                                          int4 item, const T* lut8, const uint8_t* disp, int n_mat) {
+                                          const PsiH<T>& pd, const TfsfP& tf, const AdeP<T>& ad, int4 item,
+                                          const T* lut8, const uint8_t* disp, int n_mat) {
   constexpr bool PX = (KIND & 1) != 0, PY = (KIND & 2) != 0, PZ = (KIND & 8) != 0, PML = PX || PY || PZ;
   using L = StepCfg<T, R, NWM, NS_>;
   constexpr int NS = L::NS, HP = L::HP, RW = L::RW, RH = L::RH, MW = L::MW, HW = L::HW, TK = L::TK, TJ = L::TJ;
@@ -291,8 +294,7 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
   uint8_t* sD = smem_raw + L::f_bytes + L::h_bytes + L::l_bytes;                // [LUTM]
   uint8_t* sM = smem_raw + L::f_bytes + L::h_bytes + L::l_bytes + L::d_bytes;   // [NS][RH][MW]
 
-  HCtx<T> x{s, d, pm, ps, pd, tfsf_at_step(tf_in, cur_step(tp))};
-  const TfsfP& tf = x.tf;
+  const HCtx<T> x{s, d, pm, ps, pd, tf};
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int k0 = (item.x & 0xffff) * TK, j0 = item.y * TJ;
   const int i_start = item.z, i_end = item.w;
@@ -572,19 +574,65 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
 constexpr int kStepKinds[7] = {0, 1, 4, 3, 9, 11, 15};
 
 template <typename T, int R, int NWM, int NS_>
+__device__ __forceinline__ void step_dispatch(const GridP<T>& s, const GridP<T>& d, const PmlP<T>& pm,
+                                              const PsiH<T>& ps, const PsiH<T>& pd, const TfsfP& tf,
+                                              const AdeP<T>& ad, int4 item, const T* lut8, const uint8_t* disp,
+                                              int n_mat) {
+  switch (item.x >> 16) {
+    case 0: step_item<T, R, NWM, NS_, kStepKinds[0]>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat); break;
+    case 1: step_item<T, R, NWM, NS_, kStepKinds[1]>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat); break;
+    case 2: step_item<T, R, NWM, NS_, kStepKinds[2]>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat); break;
+    case 3: step_item<T, R, NWM, NS_, kStepKinds[3]>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat); break;
+    case 4: step_item<T, R, NWM, NS_, kStepKinds[4]>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat); break;
+    case 5: step_item<T, R, NWM, NS_, kStepKinds[5]>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat); break;
+    default: step_item<T, R, NWM, NS_, kStepKinds[6]>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat); break;
+  }
+}
+
+template <typename T, int R, int NWM, int NS_>
 __global__ void __launch_bounds__(StepCfg<T, R, NWM, NS_>::NT, StepCfg<T, R, NWM, NS_>::min_blocks)
     k_step3(GridP<T> s, GridP<T> d, PmlP<T> pm, PsiH<T> ps, PsiH<T> pd, TfsfP tf_in, AdeP<T> ad, TimeP tp,
             const int4* items, const T* lut8, const uint8_t* disp, int n_mat) {
-  const int4 item = items[blockIdx.x];
-  switch (item.x >> 16) {
-    case 0: step_item<T, R, NWM, NS_, kStepKinds[0]>(s, d, pm, ps, pd, tf_in, ad, tp, item, lut8, disp, n_mat); break;
-    case 1: step_item<T, R, NWM, NS_, kStepKinds[1]>(s, d, pm, ps, pd, tf_in, ad, tp, item, lut8, disp, n_mat); break;
-    case 2: step_item<T, R, NWM, NS_, kStepKinds[2]>(s, d, pm, ps, pd, tf_in, ad, tp, item, lut8, disp, n_mat); break;
-    case 3: step_item<T, R, NWM, NS_, kStepKinds[3]>(s, d, pm, ps, pd, tf_in, ad, tp, item, lut8, disp, n_mat); break;
-    case 4: step_item<T, R, NWM, NS_, kStepKinds[4]>(s, d, pm, ps, pd, tf_in, ad, tp, item, lut8, disp, n_mat); break;
-    case 5: step_item<T, R, NWM, NS_, kStepKinds[5]>(s, d, pm, ps, pd, tf_in, ad, tp, item, lut8, disp, n_mat); break;
-    default: step_item<T, R, NWM, NS_, kStepKinds[6]>(s, d, pm, ps, pd, tf_in, ad, tp, item, lut8, disp, n_mat); break;
+  const TfsfP tf = tfsf_at_step(tf_in, cur_step(tp));
+  step_dispatch<T, R, NWM, NS_>(s, d, pm, ps, pd, tf, ad, items[blockIdx.x], lut8, disp, n_mat);
+}
+
+// Everything the one-sweep step reads of one scene of a batch.  Both field
+// and H-psi buffer sets are listed; the launch's parity picks read and write.
+template <typename T>
+struct BatchScene {
+  GridP<T> g[2];
+  PsiH<T> psh[2];
+  PmlP<T> pm;
+  TfsfP tf;
+  AdeP<T> ad;
+  const T* lut8;
+  const uint8_t* disp;
+  int n_mat;
+  int pad;
+};
+
+// The one-sweep step of a batch of scenes in one launch: one CTA per work
+// item (x: k tile | kind << 12 | scene << 16, y: j tile, z/w: plane range).
+// The CTA copies its scene's parameters into shared memory and runs the same
+// region-specialised body as k_step3, so every scene's result is identical
+// to stepping it alone.
+template <typename T, int R, int NWM, int NS_>
+__global__ void __launch_bounds__(StepCfg<T, R, NWM, NS_>::NT, StepCfg<T, R, NWM, NS_>::min_blocks)
+    k_step3_batch(const BatchScene<T>* scenes, const int4* items, TimeP tp, int parity) {
+  __shared__ BatchScene<T> sp;
+  const int4 it = items[blockIdx.x];
+  {
+    const int* src = reinterpret_cast<const int*>(scenes + (it.x >> 16));
+    int* dst = reinterpret_cast<int*>(&sp);
+    for (int q = threadIdx.x; q < static_cast<int>(sizeof(BatchScene<T>) / 4); q += blockDim.x) dst[q] = src[q];
   }
+  __syncthreads();
+  if (threadIdx.x == 0) sp.tf.e_aux = (cur_step(tp) & 1) ? sp.tf.e_aux1 : sp.tf.e_aux0;  // E_inc of this step
+  __syncthreads();
+  const int4 item = make_int4((it.x & 0xfff) | (((it.x >> 12) & 0xf) << 16), it.y, it.z, it.w);
+  step_dispatch<T, R, NWM, NS_>(sp.g[parity], sp.g[1 - parity], sp.pm, sp.psh[parity], sp.psh[1 - parity], sp.tf,
+                                sp.ad, item, sp.lut8, sp.disp, sp.n_mat);
 }
 
 }  // namespace xfb

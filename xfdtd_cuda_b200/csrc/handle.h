@@ -19,6 +19,7 @@ struct Buf {
 
 }  // namespace xfb
 
+struct xfb_batch;
 struct xfb_handle {
   using Buf = xfb::Buf;
   xfb::Compiled c;
@@ -82,6 +83,31 @@ struct xfb_handle {
   // ADE applied by k_ade_box after the one-sweep step (no dispersive cell
   // takes a TFSF or CPML correction)
   bool ade_deferred = false;
+  // set while a batch steps this handle (xfb_batch_*)
+  xfb_batch* batch = nullptr;
+};
+
+// A batch of scenes stepped together: one launch of the one-sweep kernel per
+// step over the work items of every scene.  The handles stay owned by the
+// caller; the batch owns only its tables, stream, counter and graphs.
+struct xfb_batch {
+  std::vector<xfb_handle*> hs;
+  std::string err;
+  int device = 0;
+  int prec = XFB_FP32;
+  cudaStream_t stream = nullptr;
+  bool inited = false;
+  long long step = 0, total = 0, cells = 0;
+  int tile_req = 0;   // 0: autotune, 8 or 16 rows
+  int tile = -1;      // tile configuration in use (-1 until chosen)
+  int graph_steps = 64;
+  void* scenes = nullptr;   // BatchScene<T>[n]
+  void* aux = nullptr;      // AuxScene[n_aux]
+  int n_aux = 0;
+  void* items[2] = {};      // per tile configuration
+  int n_items[2] = {};
+  long long* t_dev = nullptr;
+  std::map<int, cudaGraphExec_t> graphs;
 };
 
 namespace xfb {
@@ -121,6 +147,7 @@ long long roundup(long long v, long long m);
 bool fused(const xfb_handle* h);
 // tile configuration of the one-sweep kernel picked by the launch hint's rows
 inline int step_tile_index(int tj) { return tj <= 8 ? 0 : 1; }
+constexpr int kStepTileRows[2] = {8, 16};
 bool plain(const xfb_handle* h);
 int cur_set(const xfb_handle* h);
 void* field_ptr(const xfb_handle* h, int set, int q);
@@ -137,5 +164,9 @@ template <typename T> int profile_steps(xfb_handle* h, long long n, double* ms, 
 template <typename T> int read_field_t(xfb_handle* h, int f, double* dst);
 template <typename T> int write_field_t(xfb_handle* h, int f, const double* src);
 template <typename T> void launch_nonfinite(xfb_handle* h);
+template <typename T> int batch_init(xfb_batch* b);
+template <typename T> int batch_run(xfb_batch* b, long long n);
+void batch_free(xfb_batch* b);
+int batch_err(xfb_batch* b, int code, const std::string& m);
 
 }  // namespace xfb

@@ -596,9 +596,8 @@ __global__ void k_e2(GridP<T> g, PmlP<T> pm, TfsfP tf, TimeP tp, int i_chunk) {
 // and a first-order Mur boundary at node nl.
 // E^t lives in e_buf[t & 1]; E^{t+1} is written to the other buffer so the
 // bulk kernels of step t can still read E^t after this kernel ran.
-static __global__ void k_aux(double* e0, double* e1, double* h, int nl, double ceih, double chie, double abc,
-                      const double* src, TimeP tp) {
-  const long long t = cur_step(tp);
+__device__ __forceinline__ void aux_step(double* e0, double* e1, double* h, int nl, double ceih, double chie,
+                                         double abc, const double* src, long long t) {
   const double* e = (t & 1) ? e1 : e0;
   double* en = (t & 1) ? e0 : e1;
   for (int l = threadIdx.x; l < nl; l += blockDim.x) h[l] = h[l] + chie * (e[l + 1] - e[l]);
@@ -607,6 +606,24 @@ static __global__ void k_aux(double* e0, double* e1, double* h, int nl, double c
   if (threadIdx.x == 0) en[0] = src[t + 1];
   __syncthreads();
   if (threadIdx.x == 0) en[nl] = e[nl - 1] + abc * (en[nl - 1] - e[nl]);
+}
+
+static __global__ void k_aux(double* e0, double* e1, double* h, int nl, double ceih, double chie, double abc,
+                             const double* src, TimeP tp) {
+  aux_step(e0, e1, h, nl, ceih, chie, abc, src, cur_step(tp));
+}
+
+// TFSF auxiliary grids of a batch of scenes, one CTA per scene.
+struct AuxScene {
+  double* e0; double* e1; double* h;
+  const double* src;
+  double ceih, chie, abc;
+  int nl;
+};
+
+static __global__ void k_aux_batch(const AuxScene* a, TimeP tp) {
+  const AuxScene& s = a[blockIdx.x];
+  aux_step(s.e0, s.e1, s.h, s.nl, s.ceih, s.chie, s.abc, s.src, cur_step(tp));
 }
 
 static __global__ void k_bump(long long* t, int n) { *t += n; }

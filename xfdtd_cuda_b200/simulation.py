@@ -673,6 +673,57 @@ class Handle:
         self._c(self.lib.xfb_prepare_tables(self.h, int(n)))
 
 
+class Batch:
+    """Steps many 3-D scenes of one precision together (xfb_batch_*): one
+    launch of the one-sweep kernel per step over the work items of every
+    scene.  The Handles stay usable for read-back after ``sync()``."""
+
+    def __init__(self, handles, tile_rows: int = 0):
+        self.lib = L.load()
+        self.handles = list(handles)
+        arr = (C.c_void_p * len(self.handles))(*[h.h for h in self.handles])
+        b = C.c_void_p()
+        st = self.lib.xfb_batch_create(arr, len(self.handles), C.byref(b))
+        if st != L.XFB_OK:
+            raise L.XfbError(st, self.lib.xfb_last_error(None).decode())
+        self.b = b
+        self._c(self.lib.xfb_batch_set_tile(self.b, tile_rows))
+
+    def _c(self, status):
+        if status != L.XFB_OK:
+            raise L.XfbError(status, self.lib.xfb_batch_last_error(self.b).decode())
+
+    def init(self, total_steps: int):
+        self._c(self.lib.xfb_batch_init(self.b, total_steps))
+
+    def step(self, n: int):
+        self._c(self.lib.xfb_batch_step(self.b, n))
+
+    def sync(self):
+        self._c(self.lib.xfb_batch_sync(self.b))
+
+    def timed_step(self, n: int) -> float:
+        ms = C.c_double()
+        self._c(self.lib.xfb_batch_timed_step(self.b, n, C.byref(ms)))
+        return ms.value
+
+    def info(self):
+        cells, rows, items = C.c_longlong(), C.c_int(), C.c_int()
+        self._c(self.lib.xfb_batch_info(self.b, C.byref(cells), C.byref(rows), C.byref(items)))
+        return {"cells": cells.value, "tile_rows": rows.value, "work_items": items.value}
+
+    def close(self):
+        if getattr(self, "b", None):
+            self.lib.xfb_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class SimulationHD:
     """Drop-in for ``xfdtd::cuda::SimulationHD`` (simulation_hd.cuh:37-88)."""
 
