@@ -259,6 +259,40 @@ def batched_compare(local: int, steps: int, warmup: int, solo_steps: int = 8):
                               "ms_per_step": solo_ms / solo_steps}}
 
 
+def learned_abc_compare(local: int, steps: int, warmup: int, side: int = 768):
+    """C5: a side^3 FP32 scattering domain whose walls use the learned
+    absorbing boundary (shipped weights) against the same interior wrapped in
+    a 12-cell CPML ((side+24)^3), device-timed; with the probe error of the
+    learned boundary, of the plain Mur boundary and of bare PEC walls against
+    the CPML judge on a 48^3 validation scene."""
+    import xfdtd_cuda_b200 as X
+    from xfdtd_cuda_b200 import _lib as L
+    from xfdtd_cuda_b200 import labc
+    w = labc.shipped_weights()
+    out = {"workload": f"scatterer in {side}^3 FP32, learned 3-cell boundary vs 12-cell CPML ({side + 24}^3)",
+           "unit": UNIT}
+    for mode in ("learned", "cpml"):
+        sim = labc.scatter_scene(5, interior=side, pml=12 if mode == "cpml" else 0, dl=1e-3, inset=64)
+        sc, keep = sim.lower()
+        h = X.Handle(sc, keep)
+        h.set_device(local)
+        h.set_kernel_path(L.PATH_FUSED)
+        h.init(warmup + steps)
+        if mode == "learned":
+            h.set_learned_abc(w)
+        h.step(warmup)
+        h.sync()
+        ms = h.timed_step(steps)
+        gi = h.info()
+        cells = gi.nx * gi.ny * gi.nz
+        out[mode] = {"cells": cells, "value": cells * steps / (ms / 1e3) / 1e6, "ms_per_step": ms / steps,
+                     "interior_cell_updates_per_s": side ** 3 * steps / (ms / 1e3) / 1e6}
+        h.close()
+    out["probe_error_vs_cpml"] = labc.reflection_errors(w, seed=10, interior=48, steps=300, device=local,
+                                                        modes=("pec", "mur", "learned"))
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -277,6 +311,7 @@ def main():
     ap.add_argument("--tile-rows", type=int, default=16)
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 plain-form comparison")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 64-scene leg")
+    ap.add_argument("--no-labc", action="store_true", help="skip the learned-boundary leg")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -395,6 +430,12 @@ def main():
             batched = batched_compare(local, 30, 10)
         except Exception as exc:  # reported, not fatal for the headline
             batched = {"error": str(exc)}
+    learned = None
+    if not args.no_labc and world == 1:
+        try:
+            learned = learned_abc_compare(local, 20, 3)
+        except Exception as exc:
+            learned = {"error": str(exc)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -410,7 +451,7 @@ def main():
                           "l2": "resident state 3.3 GB >> 126 MB L2 (no flush needed)"},
                "e2e": e2e, "roofline": roofline, "step_roofline": step_roof, "cpu_baseline": cpu,
                "clocks": clk.summary(), "gpu_launches": launches, "kernels": kernels, "vs_fp64_plain": plain,
-               "batched": batched}
+               "batched": batched, "learned_abc": learned}
         print(json.dumps(out))
     if dist:
         dist[1].barrier()

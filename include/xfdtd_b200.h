@@ -291,6 +291,32 @@ int xfb_far_field(xfb_handle* h, int freq, int n_angles, const double* theta,
 int xfb_far_field_static(xfb_handle* h, int freq, int n_angles, const double* theta,
                          const double* phi, double* out);
 
+/* ---- learned absorbing boundary --------------------------------------------
+ * No counterpart in the reference.  A small MLP (8 -> 64 -> 64 -> 1, tanh,
+ * BF16 weights, FP32 accumulation) corrects the first-order Mur value of the
+ * tangential E of every outer wall cell at step n+1, from a 3-cell-deep
+ * stencil (the wall plane and the two planes inside it at steps n-1, n, n+1,
+ * plus a transverse Laplacian, all divided by their largest magnitude), in
+ * place of a CPML layer; all-zero weights give the plain Mur boundary.  The network
+ * is trained on the device by xfb_mlp_train on samples taken from the
+ * engine's own CPML runs (xfdtd_cuda_b200/labc.py builds them). */
+/* Number of MLP parameters (layout W1[64][8], b1[64], W2[64][64], b2[64], w3[64], b3). */
+int xfb_mlp_param_count(void);
+/* Mean squared error of the network with weights w (rounded to BF16 for the
+ * forward pass) over n samples (x: [n][8], y: [n]) and its gradient with
+ * respect to the weights; computed on the device. */
+int xfb_mlp_loss_grad(const float* x, const float* y, int n, const float* w, double* loss, float* grad);
+/* Full-batch Adam on the device for iters steps from w_init; w_out gets the
+ * FP32 master weights, loss_curve (may be NULL) the loss before each step. */
+int xfb_mlp_train(const float* x, const float* y, int n, int iters, float lr, const float* w_init, float* w_out,
+                  double* loss_curve);
+const char* xfb_mlp_last_error(void);
+/* Use the network on every wall of a 3-D one-sweep scene without CPML (after
+ * xfb_init; NULL weights switch it off).  The walls stay PEC without it. */
+int xfb_set_learned_abc(xfb_handle* h, const float* weights, int n_weights);
+/* Wall cells the learned boundary updates per step. */
+int xfb_labc_wall_cells(const xfb_handle* h, long long* cells);
+
 /* ---- batches of scenes ---------------------------------------------------
  * No counterpart in the reference (whose SimulationHD runs one scene per
  * object).  A batch steps many 3-D scenes of one precision together: every

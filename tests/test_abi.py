@@ -23,7 +23,7 @@ def declared():
 def test_every_declared_symbol_is_exported_and_bound():
     lib = C.CDLL(str(L.LIB_PATH))
     names = declared()
-    assert len(names) >= 29
+    assert len(names) >= 45
     for n in names:
         assert hasattr(lib, n), f"{n} not exported"
     bound = {s[0] for s in L.SIGNATURES}

@@ -1,0 +1,39 @@
+"""Learned absorbing boundary on the device: the hand-written forward and
+backward kernels agree with the float64 CPU restatement (oracle/); training
+on the engine's own CPML data lowers the loss; and the trained boundary beats
+both the method without the network (first-order Mur: the same boundary with
+an all-zero network) and the bare PEC walls, judged by the CPML run of the
+same scene."""
+import numpy as np
+import pytest
+
+import mlp_oracle as M
+from xfdtd_cuda_b200 import labc
+
+pytestmark = pytest.mark.gpu
+
+
+def test_device_gradient_matches_oracle():
+    rng = np.random.default_rng(7)
+    x = rng.standard_normal((1000, 8)).astype(np.float32)
+    y = (0.3 * x[:, 1] - 0.2 * x[:, 3] + 0.05 * rng.standard_normal(1000)).astype(np.float32)
+    w = labc.init_weights(11)
+    loss, g = labc.loss_grad(x, y, w)
+    lo, go = M.loss_grad(x, y, w)
+    assert abs(loss - lo) <= 1e-5 * lo
+    assert np.linalg.norm(g - go) <= 1e-4 * np.linalg.norm(go)
+
+
+def test_training_and_gain_over_mur_and_pec():
+    w, curve = labc.train_default()
+    assert np.isfinite(curve).all() and curve[-1] < 0.3 * curve[0]
+    err = labc.reflection_errors(w, seed=9, interior=40, steps=260, modes=("pec", "mur", "learned"))
+    print("probe error vs CPML judge:", err)
+    assert err["learned"] < 0.85 * err["mur"]
+    assert err["learned"] < 0.3 * err["pec"]
+
+
+def test_shipped_weights_are_stable_and_absorb():
+    err = labc.reflection_errors(labc.shipped_weights(), seed=10, interior=48, steps=300, modes=("pec", "mur", "learned"))
+    print("probe error vs CPML judge:", err)
+    assert np.isfinite(err["learned"]) and err["learned"] < 0.3 * err["pec"]

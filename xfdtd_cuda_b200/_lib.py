@@ -144,6 +144,14 @@ SIGNATURES = [
     ("xfb_read_nf2ff", C.c_int, [_H, C.c_int, C.c_int, C.c_int, _dp, C.c_size_t]),
     ("xfb_far_field", C.c_int, [_H, C.c_int, C.c_int, _dp, _dp, _dp]),
     ("xfb_far_field_static", C.c_int, [_H, C.c_int, C.c_int, _dp, _dp, _dp]),
+    ("xfb_mlp_param_count", C.c_int, []),
+    ("xfb_mlp_loss_grad", C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_float),
+                                    C.POINTER(C.c_double), C.POINTER(C.c_float)]),
+    ("xfb_mlp_train", C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int, C.c_int, C.c_float,
+                                C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_double)]),
+    ("xfb_mlp_last_error", C.c_char_p, []),
+    ("xfb_set_learned_abc", C.c_int, [_H, C.POINTER(C.c_float), C.c_int]),
+    ("xfb_labc_wall_cells", C.c_int, [_H, C.POINTER(C.c_longlong)]),
     ("xfb_batch_create", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]),
     ("xfb_batch_set_tile", C.c_int, [C.c_void_p, C.c_int]),
     ("xfb_batch_init", C.c_int, [C.c_void_p, C.c_longlong]),

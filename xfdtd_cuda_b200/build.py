@@ -31,7 +31,8 @@ def nvcc() -> str:
 
 
 # (source, fmad) pairs
-UNITS = [("api.cu", False), ("engine_f64.cu", False), ("engine_f32.cu", True), ("scene_compile.cpp", False)]
+UNITS = [("api.cu", False), ("engine_f64.cu", False), ("engine_f32.cu", True), ("labc_train.cu", True),
+         ("scene_compile.cpp", False)]
 
 
 def sources() -> list[Path]:

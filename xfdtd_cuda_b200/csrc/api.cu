@@ -22,6 +22,7 @@
 
 #include "handle.h"
 #include "kernels.cuh"
+#include "labc.cuh"
 #include "xfb_internal.h"
 
 using namespace xfb;
@@ -52,6 +53,9 @@ void free_device(xfb_handle* h) {
   h->bytes = 0;
   h->movie_out.clear();
   h->movie_frames.clear();
+  h->labc_on = false;
+  h->labc_w = nullptr;
+  h->labc_hist = nullptr;
   h->inited = false;
 }
 
@@ -656,6 +660,46 @@ int xfb_compiled_view_get(const xfb_handle* h, xfb_compiled_view* v) {
   return XFB_OK;
 }
 
+
+// ---- learned absorbing boundary -----------------------------------------------
+
+int xfb_labc_wall_cells(const xfb_handle* h, long long* cells) {
+  if (!h || !cells) return set_err(nullptr, XFB_ERR_INVALID, "null argument");
+  *cells = labc_layout(h->c.nx, h->c.ny, h->c.nz).off[12];
+  return XFB_OK;
+}
+
+int xfb_set_learned_abc(xfb_handle* h, const float* weights, int n_weights) {
+  int rc = check_handle(h, true);
+  if (rc || (rc = not_batched(h))) return rc;
+  for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);  // the step's launch list changes
+  h->graphs.clear();
+  if (!weights) {
+    h->labc_on = false;
+    return XFB_OK;
+  }
+  if (n_weights != kMlpParams) return set_err(h, XFB_ERR_INVALID, "weight count must be xfb_mlp_param_count()");
+  if (!fused(h) || h->c.dim != 3) return set_err(h, XFB_ERR_STATE, "the learned boundary runs on the 3-D one-sweep path");
+  for (int f = 0; f < 6; ++f)
+    if (h->c.pml[f]) return set_err(h, XFB_ERR_INVALID, "the learned boundary replaces the CPML: the scene must have none");
+  // BF16 weights, round to nearest even
+  std::vector<uint16_t> wb(kMlpParams);
+  for (int q = 0; q < kMlpParams; ++q) {
+    uint32_t u;
+    std::memcpy(&u, &weights[q], 4);
+    if ((u & 0x7f800000u) == 0x7f800000u && (u & 0x7fffffu)) wb[q] = 0x7fc0;
+    else wb[q] = static_cast<uint16_t>((u + 0x7fffu + ((u >> 16) & 1u)) >> 16);
+  }
+  if (!h->labc_w) {
+    if ((rc = alloc(h, &h->labc_w, kMlpParams * sizeof(uint16_t), false))) return rc;
+    void* p = nullptr;
+    if ((rc = alloc(h, &p, 2 * labc_layout(h->c.nx, h->c.ny, h->c.nz).off[12] * sizeof(float), true))) return rc;
+    h->labc_hist = static_cast<float*>(p);
+  }
+  if ((rc = copy(h, h->labc_w, wb.data(), wb.size() * sizeof(uint16_t), cudaMemcpyHostToDevice))) return rc;
+  h->labc_on = true;
+  return XFB_OK;
+}
 
 // ---- batches of scenes -------------------------------------------------------
 

@@ -10,6 +10,7 @@
 #include "fused3d.cuh"
 #include "handle.h"
 #include "kernels.cuh"
+#include "labc.cuh"
 #include "plain.cuh"
 
 namespace xfb {
@@ -417,6 +418,16 @@ void launch_fused(xfb_handle* h, int parity, TimeP tp, cudaStream_t st) {
   else launch_step3<T, kStepTiles[1].r, kStepTiles[1].nwm>(h, 1, parity, tp, st);
 }
 
+// ---- learned absorbing boundary ---------------------------------------------
+inline LabcP labc_params(const xfb_handle* h) {
+  LabcP p = labc_layout(h->c.nx, h->c.ny, h->c.nz);
+  const double cdt = c0() * h->c.dt, d[3] = {h->c.dx, h->c.dy, h->c.dz};
+  for (int a = 0; a < 3; ++a) p.mur_k[a] = static_cast<float>((cdt - d[a]) / (cdt + d[a]));
+  p.w = static_cast<const __nv_bfloat16*>(h->labc_w);
+  p.hist = h->labc_hist;
+  return p;
+}
+
 // ---- plain path (reference kernel structure) ------------------------------
 constexpr int kPlainBlocks = 148 * 8, kPlainThreads = 256;
 
@@ -578,6 +589,11 @@ void enqueue_step(xfb_handle* h, int off, Prof* pf = nullptr) {
       dim3 grd((b[5] - b[4] + 127) / 128, b[3] - b[2], b[1] - b[0]);
       k_ade_box<T><<<grd, 128, 0, s>>>(grid_params<T>(h, parity), grid_params<T>(h, 1 - parity), ade_params<T>(h),
                                        h->mat_disp);
+    }
+    if (h->labc_on) {
+      const LabcP lp = labc_params(h);
+      k_labc_apply<T><<<static_cast<unsigned>((lp.off[12] + 127) / 128), 128, 0, s>>>(
+          grid_params<T>(h, parity), grid_params<T>(h, 1 - parity), lp);
     }
     prof_end(h, pf);
   } else if (c.dim == 3) {

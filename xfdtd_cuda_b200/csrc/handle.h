@@ -85,6 +85,11 @@ struct xfb_handle {
   bool ade_deferred = false;
   // set while a batch steps this handle (xfb_batch_*)
   xfb_batch* batch = nullptr;
+  // learned absorbing boundary (xfb_set_learned_abc): BF16 weights and the
+  // E(w, n-1), E(w+s, n-1) history planes of every wall
+  bool labc_on = false;
+  void* labc_w = nullptr;
+  float* labc_hist = nullptr;
 };
 
 // A batch of scenes stepped together: one launch of the one-sweep kernel per

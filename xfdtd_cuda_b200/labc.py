@@ -1,0 +1,261 @@
+"""Learned absorbing boundary: data from the engine's own CPML runs, training
+on the device through the C-ABI (xfb_mlp_train), and evaluation against CPML.
+
+The network and its 3-cell stencil are described in csrc/labc.cuh.  Training
+samples come from a scattering scene run with a thick CPML: at a "virtual
+wall" a few cells inside the CPML interface the fields keep propagating
+outward undisturbed, so the wall value E(w, n+1) recorded there is what an
+ideal absorbing wall would produce from the same stencil.  Movie monitors
+record the three planes of every virtual wall each step on the device.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib as L
+from .simulation import (Cube, ElectroMagneticProperty, FieldMonitor, Handle, Material, MovieMonitor, Object, PML,
+                         PointMonitor, Simulation, Sphere, TFSF3D, Vector, Waveform)
+
+N_PARAMS = 8 * 64 + 64 + 64 * 64 + 64 + 64 + 1
+_F = C.POINTER(C.c_float)
+
+
+def init_weights(seed: int = 0) -> np.ndarray:
+    """Layout W1[64][8], b1[64], W2[64][64], b2[64], w3[64], b3; scaled
+    Gaussian initialisation (seeded)."""
+    rng = np.random.default_rng(seed)
+    w = np.zeros(N_PARAMS, np.float32)
+    o = 0
+    w[o:o + 512] = rng.standard_normal(512) / math.sqrt(8); o += 512 + 64
+    w[o:o + 4096] = rng.standard_normal(4096) / math.sqrt(64); o += 4096 + 64
+    w[o:o + 64] = rng.standard_normal(64) * 0.1 / math.sqrt(64)
+    return w
+
+
+def _gaussian(dl: float) -> Waveform:
+    tau = 20 * dl / 6e8
+    return Waveform(0, tau, 4.5 * tau)
+
+
+def scatter_scene(seed: int, interior: int = 40, pml: int = 12, dl: float = 5e-3, inset: int = 8,
+                  precision: str = "fp32", probes=(), courant: float = 0.9) -> Simulation:
+    """A seeded scattering scene: random dielectric sphere inside a TFSF box
+    lit from a random direction; `pml` CPML cells outside `interior` cells
+    (pml = 0: bare PEC walls, the domain the learned boundary runs on)."""
+    rng = np.random.default_rng(seed)
+    side = interior * dl
+    s = Simulation(dl, dl, dl, courant, precision=precision)
+    h = side / 2
+    s.addObject(Object("domain", Cube(Vector(-h, -h, -h), Vector(side, side, side)), Material.createAir()))
+    r = float(rng.uniform(0.12, 0.22)) * side
+    c = [float(rng.uniform(-0.05, 0.05)) * side for _ in range(3)]
+    s.addObject(Object("sphere", Sphere(Vector(*c), r),
+                       Material("d", ElectroMagneticProperty(float(rng.uniform(2, 8)), 1.0, 0.0, 0.0))))
+    s.addWaveformSource(TFSF3D(inset, inset, inset, float(rng.uniform(0.2, math.pi - 0.2)),
+                               float(rng.uniform(0, 2 * math.pi)), float(rng.uniform(0, math.pi)), _gaussian(dl)))
+    for d in range(6):
+        if pml:
+            s.addBoundary(PML(pml, d))
+    for p in probes:
+        s.addMonitor(PointMonitor(Vector(*p[0]), p[1]))
+    return s
+
+
+_FIELD = {0: 0, 1: 1, 2: 2}  # E component -> field id
+
+
+def _walls(n, gap, pml):
+    """(face, c, side, wall plane, inward step, comp, other) for every face and
+    tangential component of a box with n cells per axis and `pml` CPML cells."""
+    out = []
+    for face in range(6):
+        c, side = face // 2, face % 2
+        a, b = (c + 1) % 3, (c + 2) % 3
+        w = n[c] - pml - gap if side else pml + gap
+        s = -1 if side else 1
+        for comp, other in ((a, b), (b, a)):
+            out.append((face, c, side, w, s, comp, other))
+    return out
+
+
+def recording_monitors(sim: Simulation, n, gap: int = 2, pml: int = 12):
+    """Movie monitors recording the three planes of every virtual wall each
+    step (added to `sim`); returns their descriptions."""
+    desc = []
+    for face, c, side, w, s, comp, other in _walls(n, gap, pml):
+        lo, hi = [0, 0, 0], [n[0] + 1, n[1] + 1, n[2] + 1]
+        lo[c], hi[c] = (w - 2, w + 1) if side else (w, w + 3)
+        m = MovieMonitor(FieldMonitor(Cube(Vector(0, 0, 0), Vector(1, 1, 1)), _FIELD[comp]), 1, index_box=(lo, hi))
+        sim.addMonitor(m)
+        desc.append((face, c, side, w, s, comp, other, m))
+    return desc
+
+
+def features(planes: np.ndarray, margin: int, thresh: float):
+    """Samples of one wall from its three planes `planes[t, q, u, v]` (q = 0:
+    the wall, 1: one cell inside, 2: two cells inside; u along the
+    component's axis, v along the other tangential axis), in the feature
+    definition of csrc/labc.cuh.  Cells within `margin` of the plane's edge
+    are left out; samples whose scale is below `thresh` are dropped."""
+    P0, P1, P2 = planes[:, 0], planes[:, 1], planes[:, 2]
+    t = slice(1, planes.shape[0] - 1)
+    tp, tm = slice(2, planes.shape[0]), slice(0, planes.shape[0] - 2)
+    u = slice(margin, planes.shape[2] - margin)
+    v = slice(margin, planes.shape[3] - margin)
+    up, um = slice(margin + 1, planes.shape[2] - margin + 1), slice(margin - 1, planes.shape[2] - margin - 1)
+    vp, vm = slice(margin + 1, planes.shape[3] - margin + 1), slice(margin - 1, planes.shape[3] - margin - 1)
+    lap = P1[t, up, v] + P1[t, um, v] + P1[t, u, vp] + P1[t, u, vm] - 4 * P1[t, u, v]
+    f = np.stack([P0[t, u, v], P1[t, u, v], P2[t, u, v], P1[tp, u, v], P2[tp, u, v], P0[tm, u, v], P1[tm, u, v], lap],
+                 axis=-1).reshape(-1, 8)
+    y = P0[tp, u, v].reshape(-1)
+    scale = np.abs(f[:, :7]).max(axis=1)
+    keep = scale > thresh
+    return (f[keep] / scale[keep, None]).astype(np.float32), (y[keep] / scale[keep]).astype(np.float32)
+
+
+def mur_k(courant: float = 0.9) -> float:
+    """First-order Mur coefficient (c dt - d)/(c dt + d) of a cubic-cell 3-D
+    grid at the given Courant number (c dt = courant * d / sqrt(3))."""
+    r = courant / math.sqrt(3)
+    return (r - 1) / (r + 1)
+
+
+def mur_weights() -> np.ndarray:
+    """All-zero network: the learned boundary reduces to the Mur boundary."""
+    return np.zeros(N_PARAMS, np.float32)
+
+
+def residual_targets(x: np.ndarray, y: np.ndarray, k: float | None = None) -> np.ndarray:
+    """What the network learns: the wall value minus its Mur estimate."""
+    k = mur_k() if k is None else k
+    return (y - (x[:, 1] + k * (x[:, 3] - x[:, 0]))).astype(np.float32)
+
+
+def training_samples(seeds=(1, 2, 3), steps: int = 260, interior: int = 40, pml: int = 12, gap: int = 2,
+                     max_samples: int = 250000, rng_seed: int = 0, device: int = 0, noise: float = 0.0):
+    """Run the seeded CPML scattering scenes on the device, record every
+    virtual wall and return (x [n, 8], r [n]) float32 samples: features and
+    the residual of the Mur estimate.  With `noise` > 0 the features are
+    perturbed by Gaussian noise of that standard deviation (relative to the
+    unit scale) and the residual is taken against the perturbed Mur estimate,
+    which keeps the network from relying on high-gain extrapolation."""
+    xs, ys = [], []
+    for sd in seeds:
+        sim = scatter_scene(sd, interior=interior, pml=pml)
+        n = [interior + 2 * pml] * 3
+        desc = recording_monitors(sim, n, gap=gap, pml=pml)
+        sc, keep = sim.lower()
+        h = Handle(sc, keep)
+        h.set_device(device)
+        h.init(steps)
+        h.step(steps)
+        h.sync()
+        movies = [h.read_movie(q) for q in range(len(desc))]
+        h.close()
+        peak = max(np.abs(m).max() for m in movies)
+        for (face, c, side, w, s, comp, other, _), m in zip(desc, movies):
+            # m[t, i, j, k] -> planes[t, q, u(comp axis), v(other axis)], q ordered inward
+            arr = np.moveaxis(m, (1 + c, 1 + comp, 1 + other), (1, 2, 3))
+            if side:
+                arr = arr[:, ::-1]
+            x, y = features(arr, margin=pml + 2, thresh=1e-3 * peak)
+            xs.append(x)
+            ys.append(y)
+    x = np.concatenate(xs)
+    y = np.concatenate(ys)
+    rng = np.random.default_rng(rng_seed)
+    if len(x) > max_samples:
+        sel = rng.choice(len(x), max_samples, replace=False)
+        x, y = x[sel], y[sel]
+    if noise > 0:
+        x = (x + noise * rng.standard_normal(x.shape)).astype(np.float32)
+    return np.ascontiguousarray(x), residual_targets(x, y)
+
+
+def loss_grad(x: np.ndarray, y: np.ndarray, w: np.ndarray):
+    """(loss, gradient) of the network on the device (xfb_mlp_loss_grad)."""
+    lib = L.load()
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    w = np.ascontiguousarray(w, np.float32)
+    g = np.zeros(N_PARAMS, np.float32)
+    loss = C.c_double()
+    st = lib.xfb_mlp_loss_grad(x.ctypes.data_as(_F), y.ctypes.data_as(_F), len(y), w.ctypes.data_as(_F),
+                               C.byref(loss), g.ctypes.data_as(_F))
+    if st:
+        raise L.XfbError(st, lib.xfb_mlp_last_error().decode())
+    return loss.value, g
+
+
+def train(x: np.ndarray, y: np.ndarray, iters: int = 3000, lr: float = 2e-3, w0: np.ndarray | None = None,
+          seed: int = 0):
+    """Full-batch Adam on the device; returns (weights, loss curve)."""
+    lib = L.load()
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    w0 = np.ascontiguousarray(init_weights(seed) if w0 is None else w0, np.float32)
+    w = np.zeros(N_PARAMS, np.float32)
+    curve = np.zeros(iters, np.float64)
+    st = lib.xfb_mlp_train(x.ctypes.data_as(_F), y.ctypes.data_as(_F), len(y), iters, lr, w0.ctypes.data_as(_F),
+                           w.ctypes.data_as(_F), curve.ctypes.data_as(C.POINTER(C.c_double)))
+    if st:
+        raise L.XfbError(st, lib.xfb_mlp_last_error().decode())
+    return w, curve
+
+
+def train_default(device: int = 0, iters: int = 3000):
+    """The recipe the shipped weights come from: samples from three seeded
+    40^3 + 12-cell CPML scattering runs of 260 steps (200 000 samples), input
+    noise 0.03, full-batch Adam (lr 1e-3) from a damped seeded start."""
+    x, r = training_samples(seeds=(1, 2, 3), steps=260, interior=40, pml=12, max_samples=200000, noise=0.03,
+                            device=device)
+    return train(x, r, iters=iters, lr=1e-3, w0=init_weights(0) * np.float32(0.3))
+
+
+WEIGHTS_FILE = __import__("pathlib").Path(__file__).resolve().parent / "data" / "labc_weights.npy"
+
+
+def shipped_weights() -> np.ndarray:
+    """Weights trained by train_default (python -m xfdtd_cuda_b200.labc)."""
+    return np.load(WEIGHTS_FILE).astype(np.float32)
+
+
+def reflection_errors(weights: np.ndarray, seed: int = 9, interior: int = 40, steps: int = 240, pml: int = 12,
+                      device: int = 0, courant: float = 0.9, modes=("pec", "learned")):
+    """Probe error against the CPML judge of the same scene (relative L2 over
+    all probe series) for each of `modes`: "pec" (bare walls), "mur" (the
+    boundary with an all-zero network), "learned" (the given weights).
+    Probes sit in the scattered-field region two cells inside every wall."""
+    dl = 5e-3
+    h_ = interior * dl / 2
+    q = h_ - 2.5 * dl
+    probes = [((sx * q, 0.3 * q, -0.2 * q), 1) for sx in (-1, 1)] + [((0.2 * q, sy * q, 0.1 * q), 2) for sy in (-1, 1)] + \
+             [((-0.1 * q, 0.25 * q, sz * q), 0) for sz in (-1, 1)]
+    series = {}
+    for mode in ("cpml",) + tuple(modes):
+        sim = scatter_scene(seed, interior=interior, pml=pml if mode == "cpml" else 0, probes=probes, courant=courant)
+        sc, keep = sim.lower()
+        h = Handle(sc, keep)
+        h.set_device(device)
+        h.set_kernel_path(L.PATH_FUSED)
+        h.init(steps)
+        if mode == "learned":
+            h.set_learned_abc(weights)
+        elif mode == "mur":
+            h.set_learned_abc(mur_weights())
+        h.step(steps)
+        h.sync()
+        series[mode] = np.concatenate([h.read_probe(p) for p in range(len(probes))])
+        h.close()
+    ref = series["cpml"]
+    return {m: float(np.linalg.norm(series[m] - ref) / np.linalg.norm(ref)) for m in modes}
+
+
+if __name__ == "__main__":
+    w, curve = train_default()
+    WEIGHTS_FILE.parent.mkdir(exist_ok=True)
+    np.save(WEIGHTS_FILE, w)
+    print("loss", curve[0], "->", curve[-1], "saved", WEIGHTS_FILE)

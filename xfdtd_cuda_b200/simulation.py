@@ -293,10 +293,15 @@ class PointMonitor:
 
 
 class MovieMonitor:
-    def __init__(self, frame: FieldMonitor, frame_interval: int, name: str = "", out_dir: str = ""):
+    """Frames of one field component on a box every `frame_interval` steps.
+    `index_box=(lo, hi)` gives the box in component indices (half-open)
+    instead of the frame's physical shape."""
+
+    def __init__(self, frame: FieldMonitor, frame_interval: int, name: str = "", out_dir: str = "", index_box=None):
         self._frame, self._interval, self.name, self.out_dir = frame, int(frame_interval), name, out_dir
         self.data: np.ndarray | None = None
         self.box = None
+        self.index_box = index_box
 
     def frame(self):
         return self._frame
@@ -494,7 +499,7 @@ class Simulation:
                 cube = fm.shape
                 shp = comp_shape(fm.field())
                 lo_i, hi_i = [], []
-                for a in range(3):
+                for a in range(3 if m.index_box is None else 0):
                     if dim == 2 and a == 2:
                         lo_i.append(0); hi_i.append(1)
                         continue
@@ -505,6 +510,11 @@ class Simulation:
                     l0 = min(max(0, l0), shp[a] - 1)
                     h0 = min(max(l0 + 1, h0), shp[a])
                     lo_i.append(l0); hi_i.append(h0)
+                if m.index_box is not None:
+                    for a in range(3):
+                        l0 = min(max(0, int(m.index_box[0][a])), shp[a] - 1)
+                        lo_i.append(l0)
+                        hi_i.append(min(max(l0 + 1, int(m.index_box[1][a])), shp[a]))
                 m.box = (lo_i, hi_i)
                 movies.append(L.Movie(field=fm.field(), lo=(C.c_int * 3)(*lo_i), hi=(C.c_int * 3)(*hi_i),
                                       interval=m.frameInterval()))
@@ -635,6 +645,15 @@ class Handle:
         self._c(self.lib.xfb_far_field(self.h, freq, len(th), th.ctypes.data_as(L._dp), ph.ctypes.data_as(L._dp),
                                        out.ctypes.data_as(L._dp)))
         return out[:, 0] + 1j * out[:, 1], out[:, 2] + 1j * out[:, 3]
+
+    def set_learned_abc(self, weights):
+        """Learned absorbing boundary on every wall (3-D one-sweep scene
+        without CPML, after init); None switches it off."""
+        if weights is None:
+            self._c(self.lib.xfb_set_learned_abc(self.h, None, 0))
+            return
+        w = np.ascontiguousarray(weights, dtype=np.float32)
+        self._c(self.lib.xfb_set_learned_abc(self.h, w.ctypes.data_as(C.POINTER(C.c_float)), w.size))
 
     def far_field_static(self, freq, theta, phi):
         """xfb_far_field without device allocation (fixed device scratch of the
