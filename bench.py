@@ -370,9 +370,11 @@ def main():
     tot = sum(kms)
     kernels = {L.KERNEL_NAMES[q]: {"launches": kcnt[q], "ms_per_launch": kms[q] / kcnt[q], "share": kms[q] / tot}
                for q in range(L.K_COUNT) if kcnt[q]}
-    dom = max(range(L.K_COUNT), key=lambda q: kms[q])
+    # roofline of the costliest kernel class that has a byte model
+    modelled = [q for q in range(L.K_COUNT) if kcnt[q] and algorithmic_bytes(gi, q, args.precision)]
+    dom = max(modelled or [max(range(L.K_COUNT), key=lambda q: kms[q])], key=lambda q: kms[q])
     peak, peak_kind = peaks()
-    alg = algorithmic_bytes(gi, dom, args.precision)
+    alg = algorithmic_bytes(gi, dom, args.precision) or 0.0
     launch_ms = kms[dom] / kcnt[dom]
     achieved = alg / (launch_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
