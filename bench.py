@@ -259,6 +259,35 @@ def batched_compare(local: int, steps: int, warmup: int, solo_steps: int = 8):
                               "ms_per_step": solo_ms / solo_steps}}
 
 
+def cylinder2d_compare(local: int, steps: int = 4000):
+    """C2: 2-D TMz PEC cylinder (r = 50 cells) in 1024^2 cells + 10-cell CPML
+    (1044^2), TFSF Gaussian, 4000 steps, in FP32 and FP64; device-timed
+    Mcell-updates/s of each and the relative L2 error of the FP32 probe
+    series against the FP64 run (the FP64 engine is bit-identical to the CPU
+    restatement of the reference)."""
+    import numpy as np
+    import xfdtd_cuda_b200 as X
+    from xfdtd_cuda_b200 import configs
+    out, series = {"workload": "2-D TMz PEC cylinder, 1044^2 cells (1024^2 + 10-cell CPML), TFSF, 8 probes, "
+                               f"{steps} steps", "unit": UNIT}, {}
+    for prec in ("fp32", "fp64"):
+        sim = configs.cylinder_2d(precision=prec)
+        sc, keep = sim.lower()
+        h = X.Handle(sc, keep)
+        h.set_device(local)
+        h.init(steps)
+        ms = h.timed_step(steps)
+        gi = h.info()
+        cells = gi.nx * gi.ny
+        series[prec] = np.concatenate([h.read_probe(p) for p in range(len(h.probe_desc))])
+        out[prec] = {"value": cells * steps / (ms / 1e3) / 1e6, "ms_per_step": ms / steps,
+                     "launches_per_step": gi.launches_per_step}
+        h.close()
+    out["fp32_probe_rel_l2_vs_fp64"] = float(np.linalg.norm(series["fp32"] - series["fp64"]) /
+                                             np.linalg.norm(series["fp64"]))
+    return out
+
+
 def learned_abc_compare(local: int, steps: int, warmup: int, side: int = 768):
     """C5: a side^3 FP32 scattering domain whose walls use the learned
     absorbing boundary (shipped weights) against the same interior wrapped in
@@ -312,6 +341,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 plain-form comparison")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 64-scene leg")
     ap.add_argument("--no-labc", action="store_true", help="skip the learned-boundary leg")
+    ap.add_argument("--no-2d", action="store_true", help="skip the 2-D cylinder leg")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -432,6 +462,12 @@ def main():
             batched = batched_compare(local, 30, 10)
         except Exception as exc:  # reported, not fatal for the headline
             batched = {"error": str(exc)}
+    cyl2d = None
+    if not args.no_2d and world == 1:
+        try:
+            cyl2d = cylinder2d_compare(local)
+        except Exception as exc:
+            cyl2d = {"error": str(exc)}
     learned = None
     if not args.no_labc and world == 1:
         try:
@@ -453,7 +489,7 @@ def main():
                           "l2": "resident state 3.3 GB >> 126 MB L2 (no flush needed)"},
                "e2e": e2e, "roofline": roofline, "step_roofline": step_roof, "cpu_baseline": cpu,
                "clocks": clk.summary(), "gpu_launches": launches, "kernels": kernels, "vs_fp64_plain": plain,
-               "batched": batched, "learned_abc": learned}
+               "batched": batched, "learned_abc": learned, "cylinder_2d": cyl2d}
         print(json.dumps(out))
     if dist:
         dist[1].barrier()

@@ -251,3 +251,17 @@ def test_plain_path_rejects_dispersive_and_2d():
         h.set_kernel_path(PLAIN)
         with pytest.raises(X.XfbError, match="plain path"):
             h.init(10)
+
+
+def test_fp32_2d_cylinder_against_fp64():
+    # C2 at reduced size: the FP32 engine against the FP64 engine (which is
+    # bit-identical to the CPU restatement) on all probe series
+    n = 900
+    series = {}
+    for prec in ("fp32", "fp64"):
+        sim = configs.cylinder_2d(cells=256, precision=prec, tfsf_inset=10, n_probes=8)
+        h = engine(sim, n)
+        h.step(n)
+        h.sync()
+        series[prec] = np.concatenate([h.read_probe(p) for p in range(8)])
+    assert rel_l2(series["fp32"], series["fp64"]) <= 1e-4
