@@ -292,9 +292,30 @@ PsiH<T> psi_h_set(xfb_handle* h, int set) {
 struct StepTile { int r, nwm; };
 constexpr StepTile kStepTiles[2] = {{2, 4}, {2, 8}};
 // region kinds (kStepKinds, bits: 1 x-slab planes, 2 y-slab columns, 8
-// z-slab columns, 4 ADE box): lean, x planes, ADE box, y columns, z columns,
-// y+z corner columns, anything with ADE next to a slab
-constexpr int kStepKindCount = 7;
+// z-slab columns, 4 ADE box, 16 TFSF): lean, x planes, ADE box, y columns,
+// z columns, y+z corner columns, anything with ADE next to a slab, lean with
+// TFSF corrections
+constexpr int kStepKindCount = 8;
+
+// True when a work item over planes [p, q) of the tile at (j0, k0) may meet a
+// TFSF correction: the cells it updates (H at planes p-1 .. q-1, rows j0-1 ..
+// j0+TJ-1, columns k0-1 .. k0+31, which contain its E cells) meet a face
+// layer of the TFSF box (H at the plane, row or column before a face and on
+// the far face, E on both faces).
+inline bool tfsf_touch(const Compiled& c, int p, int q, int j0, int TJ, int k0) {
+  if (!c.tfsf_on) return false;
+  const int lo[3] = {p - 1, j0 - 1, k0 - 1}, hi[3] = {q - 1, j0 + TJ - 1, k0 + 31};
+  auto meets = [&](int a, int l, int h) { return l <= hi[a] && h >= lo[a]; };
+  for (int a = 0; a < 3; ++a) {
+    const int s0 = c.tf[2 * a], s1 = c.tf[2 * a + 1];
+    const bool layer = meets(a, s0 - 1, s0) || meets(a, s1, s1);
+    bool across = true;
+    for (int b = 0; b < 3; ++b)
+      if (b != a) across = across && meets(b, c.tf[2 * b], c.tf[2 * b + 1]);
+    if (layer && across) return true;
+  }
+  return false;
+}
 
 // Work items of the one-sweep kernel for tiles of TJ x 32 cells: every tile
 // column is cut along i into plane ranges whose cells (with the H halo plane
@@ -342,7 +363,8 @@ inline void build_step_items(const Compiled& c, int TJ, int NT, bool ade_deferre
           if (!(halo & ~nd))  // the halo plane adds nothing: extend over equal needs
             while (q < nx && need(q) == nd && q - p < ich) ++q;
         }
-        out[kind_of(bits)].push_back(make_int4(bx, by, p, q));
+        const int kind = kind_of(bits);
+        out[kind == 0 && tfsf_touch(c, p, q, j0, TJ, k0) ? 7 : kind].push_back(make_int4(bx, by, p, q));
         p = q;
       }
     }
@@ -373,12 +395,24 @@ inline int upload_step_items(xfb_handle* h) {
     std::vector<int4> items[kStepKindCount];
     const int nt = (kStepTiles[t].nwm + 1) * 32;
     build_step_items(h->c, kStepTiles[t].r * kStepTiles[t].nwm, nt, h->ade_deferred, items);
-    // one list, the kind in the high half of .x, the costliest kinds first so
-    // the long items start early and the short ones fill the tail
-    static const int order[kStepKindCount] = {6, 5, 4, 3, 2, 1, 0};
-    std::vector<int4> all;
-    for (int q : order)
+    // one list, the kind in the high half of .x: first the costly kinds (y/z
+    // CPML columns, in-kernel ADE), costliest first, so the long items start
+    // early; then the lean and x-slab items ordered by first plane, then row
+    // and column tile, so CTAs resident together cover neighbouring tiles of
+    // the same plane range and the halo rows and columns one CTA stages are
+    // the ones its neighbours read moments before (L2 hits)
+    static const int costly[] = {6, 5, 4, 3, 2};
+    std::vector<int4> all, rest;
+    for (int q : costly)
       for (int4 v : items[q]) all.push_back(make_int4(v.x | (q << 16), v.y, v.z, v.w));
+    for (int q : {0, 1, 7})
+      for (int4 v : items[q]) rest.push_back(make_int4(v.x | (q << 16), v.y, v.z, v.w));
+    std::stable_sort(rest.begin(), rest.end(), [](const int4& a, const int4& b) {
+      if (a.z != b.z) return a.z < b.z;
+      if (a.y != b.y) return a.y < b.y;
+      return (a.x & 0xffff) < (b.x & 0xffff);
+    });
+    all.insert(all.end(), rest.begin(), rest.end());
     h->n_step_items[t] = static_cast<int>(all.size());
     if (all.empty()) continue;
     int rc = alloc(h, &h->step_items[t], all.size() * sizeof(int4), false);

@@ -152,7 +152,7 @@ __device__ __forceinline__ void h_cell(const HCtx<T>& x, const T* Fc, const T* F
   hzv = cf.c * f[5 * PL] + cf.y * d_hz_a - cf.x * d_hz_b;
   const TfsfP& tf = x.tf;
   const int j = c.j, k = c.k;
-  if (tf_hplane || (c.tfl & 1)) {
+  if (((KIND & 16) != 0) && (tf_hplane || (c.tfl & 1))) {
     const int jj = j, kk = k;
     const bool iin = i >= tf.is && i <= tf.ie, jin = jj >= tf.js && jj <= tf.je, kin = kk >= tf.ks && kk <= tf.ke;
     if (jin && jj < tf.je && kin) {
@@ -282,6 +282,7 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
                                           const PsiH<T>& pd, const TfsfP& tf, const AdeP<T>& ad, int4 item,
                                           const T* lut8, const uint8_t* disp, int n_mat) {
   constexpr bool PX = (KIND & 1) != 0, PY = (KIND & 2) != 0, PZ = (KIND & 8) != 0, PML = PX || PY || PZ;
+  constexpr bool TFC = (KIND & 16) != 0;  // TFSF corrections compiled in
   using L = StepCfg<T, R, NWM, NS_>;
   constexpr int NS = L::NS, HP = L::HP, RW = L::RW, RH = L::RH, MW = L::MW, HW = L::HW, TK = L::TK, TJ = L::TJ;
   constexpr int CW = L::CW, MC = L::MC, NT = L::NT, PL = L::PL, HPL = L::HPL;
@@ -328,8 +329,10 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
     mso[c] = r * MW + cc * 16;
     mgo[c] = (j0 - 1 + r) * sy + (k0 - 16) + cc * 16;
   }
+  // planes i_start-1 .. i_end are read (i_end <= nx); nothing past i_end is
+  // staged, but every call commits a group so the wait counts stay fixed
   auto stage = [&](int plane, int st) {
-    if (plane <= s.nx) {
+    if (plane <= i_end) {
       const long long pb = static_cast<long long>(plane) * sx;
       const T* gex = s.ex + pb; const T* gey = s.ey + pb; const T* gez = s.ez + pb;
       const T* ghx = s.hx + pb; const T* ghy = s.hy + pb; const T* ghz = s.hz + pb;
@@ -379,7 +382,7 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
     cell[u].k = k;
     cell[u].py = PY ? slab(j, s.ny, pm.L[2], pm.L[3]) : -1;
     cell[u].pz = PZ ? slab(k, s.nz, pm.L[4], pm.L[5]) : -1;
-    cell[u].tfl = tf.on ? ((j == tf.js - 1 || j == tf.je || k == tf.ks - 1 || k == tf.ke) ? 1 : 0) |
+    cell[u].tfl = TFC && tf.on ? ((j == tf.js - 1 || j == tf.je || k == tf.ks - 1 || k == tf.ke) ? 1 : 0) |
                               ((j == tf.js || j == tf.je || k == tf.ks || k == tf.ke) ? 2 : 0)
                         : 0;
   }
@@ -430,7 +433,7 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
     // ---- H pass, plane i ----------------------------------------------------
     if (do_h) {
       const int sxp = PX ? slab(i, s.nx, pm.L[0], pm.L[1]) : -1;
-      const bool tf_hplane = tf.on && (i == tf.is - 1 || i == tf.ie);
+      const bool tf_hplane = TFC && tf.on && (i == tf.is - 1 || i == tf.ie);
       const long long pb = static_cast<long long>(i) * sx;
       T* ox = d.hx + pb; T* oy = d.hy + pb; T* oz = d.hz + pb;
 #pragma unroll
@@ -442,7 +445,7 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
     // ---- E pass, plane ie = i-1 ----------------------------------------------
     if (row_warp && ie >= i_start) {
       const int sxe = PX ? slab(ie, s.nx, pm.L[0], pm.L[1]) : -1;
-      const bool tf_eplane = tf.on && (ie == tf.is || ie == tf.ie);
+      const bool tf_eplane = TFC && tf.on && (ie == tf.is || ie == tf.ie);
       const long long pb = static_cast<long long>(ie) * sx;
       T* oex = d.ex + pb; T* oey = d.ey + pb; T* oez = d.ez + pb;
       const bool ipos = ie > 0;
@@ -481,7 +484,7 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
           if (upd_y) eyv = ade_e(ad, 1, abi, m, ey_o, eyv);
           if (upd_z) ezv = ade_e(ad, 2, abi, m, ez_o, ezv);
         }
-        if (tf_eplane || (c.tfl & 2)) {
+        if (TFC && (tf_eplane || (c.tfl & 2))) {
           const int i = ie;
           const bool iin = i >= tf.is && i <= tf.ie, jin = j >= tf.js && j <= tf.je, kin = k >= tf.ks && k <= tf.ke;
           if (jin && kin && k < tf.ke) {
@@ -570,8 +573,10 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
 
 // The one-sweep step kernel: one CTA per work item (x: k tile | kind << 16,
 // y: j tile, z: first plane, w: end plane); every kind runs its own
-// specialised body, so one launch covers the whole grid.
-constexpr int kStepKinds[7] = {0, 1, 4, 3, 9, 11, 15};
+// specialised body, so one launch covers the whole grid.  Kind bits: 1 x-slab
+// planes, 2 y-slab columns, 8 z-slab columns, 4 ADE box, 16 TFSF corrections;
+// only the lean kind (0) leaves the TFSF code out, kind 16 is lean with it.
+constexpr int kStepKinds[8] = {0, 1 | 16, 4 | 16, 3 | 16, 9 | 16, 11 | 16, 15 | 16, 16};
 
 template <typename T, int R, int NWM, int NS_>
 __device__ __forceinline__ void step_dispatch(const GridP<T>& s, const GridP<T>& d, const PmlP<T>& pm,
@@ -585,7 +590,8 @@ __device__ __forceinline__ void step_dispatch(const GridP<T>& s, const GridP<T>&
     case 3: step_item<T, R, NWM, NS_, kStepKinds[3]>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat); break;
     case 4: step_item<T, R, NWM, NS_, kStepKinds[4]>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat); break;
     case 5: step_item<T, R, NWM, NS_, kStepKinds[5]>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat); break;
-    default: step_item<T, R, NWM, NS_, kStepKinds[6]>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat); break;
+    case 6: step_item<T, R, NWM, NS_, kStepKinds[6]>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat); break;
+    default: step_item<T, R, NWM, NS_, kStepKinds[7]>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat); break;
   }
 }
 
