@@ -56,6 +56,7 @@ void free_device(xfb_handle* h) {
   h->labc_on = false;
   h->labc_w = nullptr;
   h->labc_hist = nullptr;
+  h->step_err = nullptr;
   h->inited = false;
 }
 
@@ -346,6 +347,12 @@ int xfb_sync(xfb_handle* h) {
   if (rc) return rc;
   XFB_CUDA(h, cudaStreamSynchronize(h->stream));
   XFB_CUDA(h, cudaGetLastError());
+  if (h->step_err) {
+    int e = 0;
+    XFB_CUDA(h, cudaMemcpyAsync(&e, h->step_err, sizeof(e), cudaMemcpyDeviceToHost, h->stream));
+    XFB_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (e) return set_err(h, XFB_ERR_CUDA, "one-sweep step: a staging copy did not complete (wait limit reached)");
+  }
   return XFB_OK;
 }
 

@@ -4,6 +4,8 @@
 // restatement bit for bit).
 #pragma once
 
+#include <cudaTypedefs.h>  // PFN_cuTensorMapEncodeTiled
+
 #include <algorithm>
 #include <cstring>
 
@@ -16,6 +18,8 @@
 namespace xfb {
 
 inline int upload_step_items(xfb_handle* h);
+template <typename T>
+int encode_stage_maps(xfb_handle* h);
 
 template <typename T>
 int init_device(xfb_handle* h) {
@@ -58,6 +62,12 @@ int init_device(xfb_handle* h) {
   if ((rc = upload<T>(h, &h->lut, c.coeff))) return rc;
   if ((rc = upload<T>(h, &h->lut8, c.coeff8))) return rc;
   if (fused(h) && (rc = upload_step_items(h))) return rc;
+  if (fused(h) && c.dim == 3) {
+    if ((rc = encode_stage_maps<T>(h))) return rc;
+    void* p;
+    if ((rc = alloc(h, &p, sizeof(int), false))) return rc;
+    h->step_err = static_cast<int*>(p);
+  }
   if (plain(h)) {  // per-cell coefficient arrays, expanded from the LUT on the device
     PlainCoef<T> pc;
     for (int q = 0; q < 18; ++q) {
@@ -389,6 +399,63 @@ inline bool ade_can_defer(const Compiled& c) {
   return true;
 }
 
+// The driver's tensor-map encoder, through the runtime's entry-point query
+// (no link to the driver library).
+inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// Staging tensor maps of k_step3 for both tile configurations and field sets:
+// each component (and the material ids) as a (k, j, i) tensor of extents
+// (nzp, ny+1, nx+1) over the padded layout, box = one plane's staged window
+// (RW x RH, resp. MW x RH), zero fill outside the extents.  Box origins are
+// k0 - HP (resp. k0 - 16) with k0 a multiple of 32: 16-byte aligned.  The
+// bulk-store maps of the lean interior items cover the same tensors with a
+// box of one tile (32 x TJ), stored at (k0, j0) >= 0 only.
+template <typename T>
+int encode_stage_maps(xfb_handle* h) {
+  auto enc = tensor_map_encoder();
+  if (!enc) return set_err(h, XFB_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  const Compiled& c = h->c;
+  const cuuint64_t dims[3] = {static_cast<cuuint64_t>(h->nzp), static_cast<cuuint64_t>(c.ny + 1),
+                              static_cast<cuuint64_t>(c.nx + 1)};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUtensorMapDataType ft = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  for (int t = 0; t < 2; ++t) {
+    const int TJ = kStepTiles[t].r * kStepTiles[t].nwm;
+    const cuuint32_t rh = static_cast<cuuint32_t>(TJ + 2);
+    const cuuint32_t fbox[3] = {static_cast<cuuint32_t>(32 + 2 * (16 / sizeof(T))), rh, 1};
+    const cuuint32_t mbox[3] = {64, rh, 1};
+    const cuuint32_t sbox[3] = {32, static_cast<cuuint32_t>(TJ), 1};
+    for (int set = 0; set < 2; ++set) {
+      void* const* f = set ? h->f1 : h->f;
+      const cuuint64_t fstr[2] = {static_cast<cuuint64_t>(h->sy) * sizeof(T), static_cast<cuuint64_t>(h->sx) * sizeof(T)};
+      for (int q = 0; q < 6; ++q) {
+        CUresult r = enc(&h->stage_maps[t][set][q], ft, 3, f[q], dims, fstr, fbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return set_err(h, XFB_ERR_CUDA, "cuTensorMapEncodeTiled (field) failed: " + std::to_string(r));
+        r = enc(&h->store_maps[t][set][q], ft, 3, f[q], dims, fstr, sbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return set_err(h, XFB_ERR_CUDA, "cuTensorMapEncodeTiled (store) failed: " + std::to_string(r));
+      }
+      const cuuint64_t mstr[2] = {static_cast<cuuint64_t>(h->sy), static_cast<cuuint64_t>(h->sx)};
+      CUresult r = enc(&h->stage_maps[t][set][6], CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, h->mid, dims, mstr, mbox, estr,
+                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS) return set_err(h, XFB_ERR_CUDA, "cuTensorMapEncodeTiled (ids) failed: " + std::to_string(r));
+    }
+  }
+  return XFB_OK;
+}
+
 inline int upload_step_items(xfb_handle* h) {
   h->ade_deferred = ade_can_defer(h->c);
   for (int t = 0; t < 2; ++t) {
@@ -437,10 +504,15 @@ void launch_step3(xfb_handle* h, int t, int parity, TimeP tp, cudaStream_t st) {
   // with the ADE update deferred to k_ade_box the step kernel does none
   AdeP<T> step_ade = ade_params<T>(h);
   if (h->ade_deferred) step_ade.kind = kAdeNone;
+  StageMaps maps;
+  std::memcpy(maps.f, h->stage_maps[t][parity], sizeof(maps.f));
+  maps.mid = h->stage_maps[t][parity][6];
+  StoreMaps outs;
+  std::memcpy(outs.f, h->store_maps[t][1 - parity], sizeof(outs.f));
   k_step3<T, R, NWM, NS><<<h->n_step_items[t], S::NT, S::bytes, st>>>(
       grid_params<T>(h, parity), grid_params<T>(h, 1 - parity), pml_params<T>(h), psi_h_set<T>(h, parity),
       psi_h_set<T>(h, 1 - parity), tfsf_params(h), step_ade, tp, static_cast<const int4*>(h->step_items[t]),
-      as<const T>(h->lut8), h->mat_disp, h->c.n_mat);
+      as<const T>(h->lut8), h->mat_disp, h->c.n_mat, maps, outs, h->step_err);
 }
 
 // One-sweep step: one launch over all work items, for the tile the launch

@@ -37,9 +37,76 @@
 // to the CPU restatement bit for bit.
 #pragma once
 
+#include <cuda.h>  // CUtensorMap
+
 #include "kernels.cuh"
 
 namespace xfb {
+
+// Tensor maps of the staging copies of one field set and tile shape: the six
+// components and the material ids as 3-D tensors (k, j, i) over the padded
+// layout, boxes of one plane's staged window (zero fill outside the grid).
+struct StageMaps {
+  CUtensorMap f[6];
+  CUtensorMap mid;
+};
+
+// Tensor maps of the bulk stores of the lean interior body: the six
+// components of the write set (Ex Ey Ez Hx Hy Hz), box 32 x TJ x 1.
+struct StoreMaps {
+  CUtensorMap f[6];
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+// orders this thread's earlier shared-memory accesses before later bulk
+// (async-proxy) copies into or out of the same memory
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for phase `parity` of barrier b: false after 2^22 polls, far
+// beyond the latency of any staging copy (the copies then never completed).
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity) {
+  for (int n = 0; n < (1 << 22); ++n)
+    if (mbar_try_wait(b, parity)) return true;
+  return false;
+}
+// Tiled bulk copy of one box of a 3-D tensor into shared memory, completing
+// on barrier `bar` (no multicast).
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];\n" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+// Tiled bulk store of one box from shared memory (bulk-group completion).
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, const void* src, int x, int y, int z) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];\n" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(smem_u32(src)), "r"(x), "r"(y), "r"(z)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+// the committed bulk stores have read their shared-memory sources
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+// ... and completed their global writes
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
@@ -84,13 +151,34 @@ struct StepCfg {
   static constexpr int LUTM = 16;            // materials whose coefficients sit in shared memory
   static constexpr int CW = RW / HP;         // 16-byte chunks per staged field row
   static constexpr int MC = MW / 16;         // 16-byte chunks per material row
-  static constexpr int PL = RH * RW;         // elements of one staged component plane
+  static constexpr int PLA = 128 / sizeof(T);
+  // elements of one staged component plane, rounded up so every plane of the
+  // ring starts on a 128-byte boundary (bulk-copy destinations)
+  static constexpr int PL = (RH * RW + PLA - 1) / PLA * PLA;
   static constexpr int NT = (NWM + 1) * 32;  // row warps + halo warp
+  // shared memory, from a 128-byte aligned base: field ring [NS][6][PL],
+  // material ring [NS][RH][MW], NS staging barriers, H planes, E planes of
+  // the lean interior body, LUT [LUTM][8], dispersive flags [LUTM]
   static constexpr size_t f_bytes = static_cast<size_t>(NS) * 6 * PL * sizeof(T);
+  static constexpr size_t m_bytes = static_cast<size_t>(NS) * RH * MW;
   static constexpr size_t h_bytes = (2ull * 3 * HPL * sizeof(T) + 15) / 16 * 16;
   static constexpr size_t l_bytes = LUTM * 8 * sizeof(T);
   static constexpr size_t d_bytes = LUTM;
-  static constexpr size_t bytes = f_bytes + h_bytes + l_bytes + d_bytes + static_cast<size_t>(NS) * RH * MW;
+  // lean interior body: H planes [2][3][LCS] (per component a dense TJ x 32
+  // tile, then the halo row j0-1 and the halo column k0-1, 32 slots each) and
+  // E planes [2][3][TJ][32], both the sources of bulk stores
+  static constexpr int LCS = (TJ + 2) * 32;
+  static constexpr size_t lh_bytes = 2ull * 3 * LCS * sizeof(T);
+  static constexpr size_t le_bytes = 2ull * 3 * TJ * 32 * sizeof(T);
+  static constexpr size_t hr_bytes = (h_bytes > lh_bytes ? h_bytes : lh_bytes);
+  static constexpr size_t off_m = f_bytes, off_b = f_bytes + m_bytes;
+  static constexpr size_t off_h = (off_b + 8 * NS + 127) / 128 * 128;
+  static constexpr size_t off_e = off_h + (hr_bytes + 127) / 128 * 128;
+  static constexpr size_t off_l = off_e + le_bytes, off_d = off_l + l_bytes;
+  static constexpr size_t bytes = off_d + d_bytes + 128;  // + alignment slack of the base
+  // bytes one staged plane brings (six field boxes and the material box)
+  static constexpr unsigned tx_bytes = static_cast<unsigned>(6 * RH * RW * sizeof(T) + RH * MW);
+  static_assert((RH * MW) % 128 == 0, "material planes stay 128-byte aligned");
   // CTAs per SM that the 228 KB of shared memory per SM admits (1 KB reserved
   // per CTA), at most 4; the register budget is sized for that residency
   static constexpr int fit = static_cast<int>((228u * 1024u) / (bytes + 1024u));
@@ -277,10 +365,15 @@ __device__ __forceinline__ int prefetch_e_psi(const PmlP<T>& pm, const GridP<T>&
 }
 
 // One work item of the one-sweep step, compiled for region kind KIND.
-template <typename T, int R, int NWM, int NS_, int KIND>
+// TMA: staging by tiled bulk copies from `maps` (one thread issues a plane's
+// seven boxes, a barrier per ring slot counts their bytes); otherwise every
+// thread stages 16-byte chunks with cp.async.  A staging wait that runs out
+// sets *err = 1 and ends the item after the copies in flight have landed.
+template <typename T, int R, int NWM, int NS_, int KIND, bool TMA>
 __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, const PmlP<T>& pm, const PsiH<T>& ps,
                                           const PsiH<T>& pd, const TfsfP& tf, const AdeP<T>& ad, int4 item,
-                                          const T* lut8, const uint8_t* disp, int n_mat) {
+                                          const T* lut8, const uint8_t* disp, int n_mat, const StageMaps* maps,
+                                          int* err) {
   constexpr bool PX = (KIND & 1) != 0, PY = (KIND & 2) != 0, PZ = (KIND & 8) != 0, PML = PX || PY || PZ;
   constexpr bool TFC = (KIND & 16) != 0;  // TFSF corrections compiled in
   using L = StepCfg<T, R, NWM, NS_>;
@@ -289,11 +382,14 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
   constexpr int NFC = (RH * CW + NT - 1) / NT;  // staged field chunks per thread
   constexpr int NMC = (RH * MC + NT - 1) / NT;  // staged material chunks per thread
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* sF = reinterpret_cast<T*>(smem_raw);                                       // [NS][6][RH][RW]
-  T* sH = reinterpret_cast<T*>(smem_raw + L::f_bytes);                          // [2][3][HH][HW]
-  T* sL = reinterpret_cast<T*>(smem_raw + L::f_bytes + L::h_bytes);             // [LUTM][8]
-  uint8_t* sD = smem_raw + L::f_bytes + L::h_bytes + L::l_bytes;                // [LUTM]
-  uint8_t* sM = smem_raw + L::f_bytes + L::h_bytes + L::l_bytes + L::d_bytes;   // [NS][RH][MW]
+  unsigned char* base = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+  T* sF = reinterpret_cast<T*>(base);                               // [NS][6][PL]
+  uint8_t* sM = base + L::off_m;                                    // [NS][RH][MW]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base + L::off_b);     // [NS]
+  T* sH = reinterpret_cast<T*>(base + L::off_h);                    // [2][3][HH][HW]
+  T* sL = reinterpret_cast<T*>(base + L::off_l);                    // [LUTM][8]
+  uint8_t* sD = base + L::off_d;                                    // [LUTM]
+  static_assert(L::off_h + L::h_bytes <= L::off_e, "H planes inside their region");
 
   const HCtx<T> x{s, d, pm, ps, pd, tf};
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -331,7 +427,24 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
   }
   // planes i_start-1 .. i_end are read (i_end <= nx); nothing past i_end is
   // staged, but every call commits a group so the wait counts stay fixed
+  if (TMA && tid == 0) {
+    for (int q = 0; q < NS; ++q) mbar_init(bar + q, 1);
+    fence_mbar_init();
+  }
+  int staged = -1;  // last plane whose copies were issued (thread 0)
   auto stage = [&](int plane, int st) {
+    if (TMA) {
+      if (tid == 0 && plane <= i_end) {
+        staged = plane;
+        fence_proxy_async();
+        mbar_expect_tx(bar + st, L::tx_bytes);
+        T* dst = sF + st * 6 * PL;
+#pragma unroll
+        for (int f = 0; f < 6; ++f) tma_load_3d(dst + f * PL, &maps->f[f], k0 - HP, j0 - 1, plane, bar + st);
+        tma_load_3d(sM + st * RH * MW, &maps->mid, k0 - 16, j0 - 1, plane, bar + st);
+      }
+      return;
+    }
     if (plane <= i_end) {
       const long long pb = static_cast<long long>(plane) * sx;
       const T* gex = s.ex + pb; const T* gey = s.ey + pb; const T* gez = s.ez + pb;
@@ -355,8 +468,17 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
     }
     cp_async_commit();
   };
+  if (TMA) __syncthreads();  // barriers initialised before any copy or wait
   for (int q = 0; q < NS - 1; ++q) stage(i_first + q, (i_first + q) % NS);
   int slot = i_first % NS;  // ring slot of plane i
+  // phase of the ring barrier of plane p (the slots are used in plane order)
+  auto phase = [&](int p) { return static_cast<unsigned>(((p - i_first) / NS) & 1); };
+  int waited = i_first - 1;  // last plane whose staging barrier was passed
+  bool ok = true;
+  if (TMA) {
+    ok = mbar_wait(bar + slot, phase(i_first));
+    if (ok) waited = i_first;
+  }
 
   // H cells of this thread: a row warp's R rows at column `lane`; the halo
   // warp's row j0-1 at column `lane` (u = 0) and column k0-1 at row `lane`
@@ -421,8 +543,20 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
     const bool write_h = do_h && i >= i_start && row_warp;
     const int slot_n = slot + 1 == NS ? 0 : slot + 1;      // plane i+1
     const int slot_p = slot == 0 ? NS - 1 : slot - 1;      // plane i-1, refilled with plane i+NS-1
-    cp_async_wait<NS - 3>();  // planes i and i+1 have landed (this thread's copies)
-    __syncthreads();          // ... everyone's copies; iteration i-1 is complete everywhere
+    if (TMA) {
+      if (i + 1 <= i_end && ok) {  // plane i+1 has landed (plane i did one iteration earlier)
+        ok = mbar_wait(bar + slot_n, phase(i + 1));
+        if (ok) waited = i + 1;
+      }
+      // every thread saw its planes land; iteration i-1 is complete everywhere
+      if (__syncthreads_or(!ok)) {
+        ok = false;
+        break;
+      }
+    } else {
+      cp_async_wait<NS - 3>();  // planes i and i+1 have landed (this thread's copies)
+      __syncthreads();          // ... everyone's copies; iteration i-1 is complete everywhere
+    }
     stage(i + NS - 1, slot_p);  // whose last readers finished iteration i-1
     const T* Fc = sF + slot * 6 * PL;
     const T* Fn = sF + slot_n * 6 * PL;
@@ -568,7 +702,14 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
       }
     }
   }
-  cp_async_wait<0>();
+  if (!TMA) {
+    cp_async_wait<0>();
+  } else if (!ok && tid == 0) {
+    // a staging wait ran out: flag it, then let the copies still in flight
+    // (planes waited+1 .. the last staged one) land before the CTA exits
+    atomicExch(err, 1);
+    for (int p = waited + 1; p <= staged; ++p) mbar_wait(bar + p % NS, phase(p));
+  }
 }
 
 // The one-sweep step kernel: one CTA per work item (x: k tile | kind << 16,
@@ -578,29 +719,39 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
 // only the lean kind (0) leaves the TFSF code out, kind 16 is lean with it.
 constexpr int kStepKinds[8] = {0, 1 | 16, 4 | 16, 3 | 16, 9 | 16, 11 | 16, 15 | 16, 16};
 
-template <typename T, int R, int NWM, int NS_>
+// kind index of the lean interior items (step_item_lean, bulk-copy path only)
+constexpr int kLeanInterior = 8;
+
+template <typename T, int R, int NWM, int NS_, bool TMA>
 __device__ __forceinline__ void step_dispatch(const GridP<T>& s, const GridP<T>& d, const PmlP<T>& pm,
                                               const PsiH<T>& ps, const PsiH<T>& pd, const TfsfP& tf,
                                               const AdeP<T>& ad, int4 item, const T* lut8, const uint8_t* disp,
-                                              int n_mat) {
+                                              int n_mat, const StageMaps* maps, const StoreMaps* outs, int* err) {
+#define XFB_ITEM(q) step_item<T, R, NWM, NS_, kStepKinds[q], TMA>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat, maps, err)
   switch (item.x >> 16) {
-    case 0: step_item<T, R, NWM, NS_, kStepKinds[0]>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat); break;
-    case 1: step_item<T, R, NWM, NS_, kStepKinds[1]>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat); break;
-    case 2: step_item<T, R, NWM, NS_, kStepKinds[2]>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat); break;
-    case 3: step_item<T, R, NWM, NS_, kStepKinds[3]>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat); break;
-    case 4: step_item<T, R, NWM, NS_, kStepKinds[4]>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat); break;
-    case 5: step_item<T, R, NWM, NS_, kStepKinds[5]>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat); break;
-    case 6: step_item<T, R, NWM, NS_, kStepKinds[6]>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat); break;
-    default: step_item<T, R, NWM, NS_, kStepKinds[7]>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat); break;
+    case 0: XFB_ITEM(0); break;
+    case 1: XFB_ITEM(1); break;
+    case 2: XFB_ITEM(2); break;
+    case 3: XFB_ITEM(3); break;
+    case 4: XFB_ITEM(4); break;
+    case 5: XFB_ITEM(5); break;
+    case 6: XFB_ITEM(6); break;
+    default: XFB_ITEM(7); break;
   }
+#undef XFB_ITEM
 }
 
+// The single-scene step stages with tiled bulk copies from the tensor maps of
+// its read set (`maps`, a grid constant); a staging wait that runs out sets
+// *err.
 template <typename T, int R, int NWM, int NS_>
 __global__ void __launch_bounds__(StepCfg<T, R, NWM, NS_>::NT, StepCfg<T, R, NWM, NS_>::min_blocks)
     k_step3(GridP<T> s, GridP<T> d, PmlP<T> pm, PsiH<T> ps, PsiH<T> pd, TfsfP tf_in, AdeP<T> ad, TimeP tp,
-            const int4* items, const T* lut8, const uint8_t* disp, int n_mat) {
+            const int4* items, const T* lut8, const uint8_t* disp, int n_mat, const __grid_constant__ StageMaps maps,
+            const __grid_constant__ StoreMaps outs, int* err) {
   const TfsfP tf = tfsf_at_step(tf_in, cur_step(tp));
-  step_dispatch<T, R, NWM, NS_>(s, d, pm, ps, pd, tf, ad, items[blockIdx.x], lut8, disp, n_mat);
+  step_dispatch<T, R, NWM, NS_, true>(s, d, pm, ps, pd, tf, ad, items[blockIdx.x], lut8, disp, n_mat, &maps, &outs,
+                                      err);
 }
 
 // Everything the one-sweep step reads of one scene of a batch.  Both field
@@ -637,8 +788,8 @@ __global__ void __launch_bounds__(StepCfg<T, R, NWM, NS_>::NT, StepCfg<T, R, NWM
   if (threadIdx.x == 0) sp.tf.e_aux = (cur_step(tp) & 1) ? sp.tf.e_aux1 : sp.tf.e_aux0;  // E_inc of this step
   __syncthreads();
   const int4 item = make_int4((it.x & 0xfff) | (((it.x >> 12) & 0xf) << 16), it.y, it.z, it.w);
-  step_dispatch<T, R, NWM, NS_>(sp.g[parity], sp.g[1 - parity], sp.pm, sp.psh[parity], sp.psh[1 - parity], sp.tf,
-                                sp.ad, item, sp.lut8, sp.disp, sp.n_mat);
+  step_dispatch<T, R, NWM, NS_, false>(sp.g[parity], sp.g[1 - parity], sp.pm, sp.psh[parity], sp.psh[1 - parity],
+                                       sp.tf, sp.ad, item, sp.lut8, sp.disp, sp.n_mat, nullptr, nullptr, nullptr);
 }
 
 }  // namespace xfb

@@ -2,6 +2,7 @@
 // translation units (engine_f32.cu, engine_f64.cu).
 #pragma once
 
+#include <cuda.h>  // CUtensorMap
 #include <cuda_runtime.h>
 
 #include <map>
@@ -80,6 +81,13 @@ struct xfb_handle {
   // (int4: k tile | region kind << 16, j tile, first plane, end plane)
   void* step_items[2] = {};
   int n_step_items[2] = {};
+  // staging tensor maps of the one-sweep kernel per tile configuration and
+  // read set (six field components, then the material ids), the bulk-store
+  // maps of its lean interior items per tile configuration and write set
+  // (Ex Ey Ez Hx Hy Hz), and its error flag (1: a staging wait ran out)
+  CUtensorMap stage_maps[2][2][7];
+  CUtensorMap store_maps[2][2][6];
+  int* step_err = nullptr;
   // ADE applied by k_ade_box after the one-sweep step (no dispersive cell
   // takes a TFSF or CPML correction)
   bool ade_deferred = false;
