@@ -127,6 +127,63 @@ def test_fp64_no_tfsf_no_pml_initial_field(path):
     assert bit_equal(gf, of)
 
 
+def elongated_scene(precision="fp64"):
+    # 36 x 56 x 104 inner cells of 3 mm + 6-cell CPML: the one-sweep tiles at
+    # k0 = 32 and 64 away from the TFSF faces are lean interior work items
+    # (the bulk-copy body); TFSF box, a lossy block and CPML around them
+    sim = X.Simulation(3e-3, 3e-3, 3e-3, 0.9, precision=precision)
+    sim.addObject(X.Object("domain", X.Cube(X.Vector(0, 0, 0), X.Vector(0.108, 0.168, 0.312)), X.Material.createAir()))
+    sim.addObject(X.Object("blk", X.Cube(X.Vector(0.04, 0.06, 0.12), X.Vector(0.02, 0.04, 0.06)),
+                           X.Material("lossy", X.ElectroMagneticProperty(4.0, 1.5, 0.02, 0.0))))
+    tau = 20 * 3e-3 / 6e8
+    sim.addWaveformSource(X.TFSF3D(5, 5, 5, math.pi / 3, math.pi / 5, 0.4, X.Waveform.gaussian(tau, 4.5 * tau)))
+    for d in range(6):
+        sim.addBoundary(X.PML(6, d))
+    sim.addMonitor(X.PointMonitor(X.Vector(0.05, 0.08, 0.15), 2))
+    return sim
+
+
+@pytest.mark.parametrize("rows", [8, 16])
+def test_fp64_lean_interior_bitexact(rows):
+    # random initial fields inside the CPML (H scaled to free-space impedance),
+    # so the interior tiles carry data from the first step; zero on the walls
+    # and in the CPML, whose corrections the reference also applies to wall
+    # cells; both tile heights of the one-sweep kernel
+    sim = elongated_scene()
+    n = 70
+    h = engine(sim, n, path=2, block=(32, rows, 1))
+    o = oracle_of(sim, n)
+    rng = np.random.default_rng(11)
+    for f in range(6):
+        sh = h.shape(f)
+        v = np.zeros(sh)
+        inner = tuple(slice(8, s - 8) for s in sh)
+        v[inner] = rng.standard_normal(v[inner].shape) * (1.0 if f < 3 else 1.0 / 377.0)
+        h.write_field(f, v)
+        o.set_field(f, v)
+    h.step(n)
+    h.sync()
+    o.run(n)
+    gf, of = fields_of(h, 3), fields_of(o, 3)
+    assert compare_fields(gf, of) <= FP64_TOL
+    assert bit_equal(gf, of)
+    assert max_rel(h.read_probe(0), o.probe(0)) == 0.0
+
+
+@pytest.mark.parametrize("rows", [8, 16])
+def test_fp32_lean_interior_against_fp64_oracle(rows):
+    n = 200
+    h = engine(elongated_scene("fp32"), n, path=2, block=(32, rows, 1))
+    h.step(n)
+    h.sync()
+    o = oracle_of(elongated_scene(), n)
+    o.run(n)
+    assert rel_l2(h.read_probe(0), o.probe(0)) <= 1e-4
+    gf, of = fields_of(h, 3), fields_of(o, 3)
+    for f in of:
+        assert rel_l2(gf[f], of[f]) <= 1e-4
+
+
 @pytest.mark.parametrize("path", PATHS + [PLAIN])
 def test_fp32_against_fp64_oracle(path):
     sim32 = small_sphere("fp32")

@@ -24,6 +24,17 @@ def test_device_gradient_matches_oracle():
     assert np.linalg.norm(g - go) <= 1e-4 * np.linalg.norm(go)
 
 
+def test_training_is_reproducible():
+    # the per-block gradients are summed in a fixed order: two runs on the
+    # same samples give the same weights bit for bit
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal((5000, 8)).astype(np.float32)
+    y = (0.3 * x[:, 1] - 0.2 * x[:, 3]).astype(np.float32)
+    w1, c1 = labc.train(x, y, iters=40, lr=1e-3, seed=2)
+    w2, c2 = labc.train(x, y, iters=40, lr=1e-3, seed=2)
+    assert np.array_equal(w1, w2) and np.array_equal(c1, c2)
+
+
 def test_training_and_gain_over_mur_and_pec():
     w, curve = labc.train_default()
     assert np.isfinite(curve).all() and curve[-1] < 0.3 * curve[0]

@@ -305,7 +305,7 @@ constexpr StepTile kStepTiles[2] = {{2, 4}, {2, 8}};
 // z-slab columns, 4 ADE box, 16 TFSF): lean, x planes, ADE box, y columns,
 // z columns, y+z corner columns, anything with ADE next to a slab, lean with
 // TFSF corrections
-constexpr int kStepKindCount = 8;
+constexpr int kStepKindCount = 9;  // + lean interior (the bulk-copy path of single scenes)
 
 // True when a work item over planes [p, q) of the tile at (j0, k0) may meet a
 // TFSF correction: the cells it updates (H at planes p-1 .. q-1, rows j0-1 ..
@@ -332,7 +332,7 @@ inline bool tfsf_touch(const Compiled& c, int p, int q, int j0, int TJ, int k0) 
 // below the range and the halo row and column of the tile) need no more than
 // the range's kind handles.  Ranges are at most `ich` planes long.
 inline void build_step_items(const Compiled& c, int TJ, int NT, bool ade_deferred, std::vector<int4> (&out)[kStepKindCount],
-                             int plane_chunk = 0) {
+                             int plane_chunk = 0, bool lean_interior = false) {
   const int nx = c.nx, ny = c.ny, nz = c.nz;
   const int* L = c.pml;
   const int gx = (nz + 31) / 32, gy = (ny + TJ - 1) / TJ;
@@ -373,8 +373,12 @@ inline void build_step_items(const Compiled& c, int TJ, int NT, bool ade_deferre
           if (!(halo & ~nd))  // the halo plane adds nothing: extend over equal needs
             while (q < nx && need(q) == nd && q - p < ich) ++q;
         }
-        const int kind = kind_of(bits);
-        out[kind == 0 && tfsf_touch(c, p, q, j0, TJ, k0) ? 7 : kind].push_back(make_int4(bx, by, p, q));
+        int kind = kind_of(bits);
+        if (kind == 0 && tfsf_touch(c, p, q, j0, TJ, k0)) kind = 7;
+        // lean and fully inside: the tile, its halo row and column, first plane >= 1
+        if (kind == 0 && lean_interior && p >= 1 && j0 >= 1 && k0 >= 1 && j0 + TJ <= ny && k0 + 32 <= nz)
+          kind = kLeanInterior;
+        out[kind].push_back(make_int4(bx, by, p, q));
         p = q;
       }
     }
@@ -461,7 +465,7 @@ inline int upload_step_items(xfb_handle* h) {
   for (int t = 0; t < 2; ++t) {
     std::vector<int4> items[kStepKindCount];
     const int nt = (kStepTiles[t].nwm + 1) * 32;
-    build_step_items(h->c, kStepTiles[t].r * kStepTiles[t].nwm, nt, h->ade_deferred, items);
+    build_step_items(h->c, kStepTiles[t].r * kStepTiles[t].nwm, nt, h->ade_deferred, items, 0, true);
     // one list, the kind in the high half of .x: first the costly kinds (y/z
     // CPML columns, in-kernel ADE), costliest first, so the long items start
     // early; then the lean and x-slab items ordered by first plane, then row
@@ -472,7 +476,7 @@ inline int upload_step_items(xfb_handle* h) {
     std::vector<int4> all, rest;
     for (int q : costly)
       for (int4 v : items[q]) all.push_back(make_int4(v.x | (q << 16), v.y, v.z, v.w));
-    for (int q : {0, 1, 7})
+    for (int q : {0, 1, 7, kLeanInterior})
       for (int4 v : items[q]) rest.push_back(make_int4(v.x | (q << 16), v.y, v.z, v.w));
     std::stable_sort(rest.begin(), rest.end(), [](const int4& a, const int4& b) {
       if (a.z != b.z) return a.z < b.z;

@@ -712,6 +712,218 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
   }
 }
 
+// Lean interior work item: no CPML, TFSF or ADE cell and no PEC wall within
+// reach, the tile with its halo row and column inside the grid, first plane
+// >= 1.  The arithmetic is step_item's lean kind, term for term; what differs
+// is the data movement.  The H planes live in dense shared tiles (with the
+// halo row j0-1 and halo column k0-1 after them): the E update reads its j-1
+// and k-1 neighbours there at per-thread constant offsets, and the tiles are
+// also the sources of bulk tensor stores.  E^{n+1} goes to dense tiles too.
+// At iteration i one thread issues the stores of H plane i-1 and E plane i-2
+// (both finished before the iteration's barrier) and waits, before the next
+// barrier, until they have read their tiles; so no thread computes a global
+// address or issues a global store.
+template <typename T, int R, int NWM, int NS_>
+__device__ __forceinline__ void step_item_lean(int4 item, const T* lut8, int n_mat, const StageMaps* maps,
+                                               const StoreMaps* outs, int* err) {
+  using L = StepCfg<T, R, NWM, NS_>;
+  constexpr int NS = L::NS, HP = L::HP, RW = L::RW, MW = L::MW, TJ = L::TJ, PL = L::PL, NT = L::NT, RH = L::RH;
+  constexpr int CS = L::LCS, ET = TJ * 32;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned char* base = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+  T* sF = reinterpret_cast<T*>(base);                            // [NS][6][PL]
+  uint8_t* sM = base + L::off_m;                                 // [NS][RH][MW]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base + L::off_b);  // [NS]
+  T* sH = reinterpret_cast<T*>(base + L::off_h);                 // [2][3][CS]
+  T* sE = reinterpret_cast<T*>(base + L::off_e);                 // [2][3][TJ * 32]
+  T* sL = reinterpret_cast<T*>(base + L::off_l);                 // [LUTM][8]
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int k0 = (item.x & 0xffff) * 32, j0 = item.y * TJ;
+  const int i_start = item.z, i_end = item.w, i_first = i_start - 1;
+  const bool lut_shared = n_mat <= L::LUTM;
+  if (lut_shared)
+    for (int q = tid; q < n_mat * 8; q += NT) sL[q] = lut8[q];
+  const T* lut = lut_shared ? sL : lut8;
+  if (tid == 0) {
+    for (int q = 0; q < NS; ++q) mbar_init(bar + q, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  int staged = -1;  // last plane whose copies were issued (thread 0)
+  auto stage = [&](int plane, int st) {
+    if (tid == 0 && plane <= i_end) {
+      staged = plane;
+      fence_proxy_async();
+      mbar_expect_tx(bar + st, L::tx_bytes);
+      T* dst = sF + st * 6 * PL;
+#pragma unroll
+      for (int f = 0; f < 6; ++f) tma_load_3d(dst + f * PL, &maps->f[f], k0 - HP, j0 - 1, plane, bar + st);
+      tma_load_3d(sM + st * RH * MW, &maps->mid, k0 - 16, j0 - 1, plane, bar + st);
+    }
+  };
+  for (int q = 0; q < NS - 1; ++q) stage(i_first + q, (i_first + q) % NS);
+  auto phase = [&](int p) { return static_cast<unsigned>(((p - i_first) / NS) & 1); };
+
+  // cells of this thread: a row warp's R rows at column `lane`; the halo
+  // warp's row j0-1 at column `lane` (u = 0) and column k0-1 at row `lane`
+  // (u = 1, lane < TJ).  wf: staged offset, mo: material offset, hs: slot in
+  // the H tile, km: the k-1 neighbour's slot (row warps).
+  const bool row_warp = warp < NWM;
+  int wf[R], mo[R], hs[R], km[R];
+  bool act[R];
+#pragma unroll
+  for (int u = 0; u < R; ++u) {
+    if (row_warp) {
+      const int r = warp * R + u;
+      wf[u] = (r + 1) * RW + HP + lane;
+      mo[u] = (r + 1) * MW + 16 + lane;
+      hs[u] = r * 32 + lane;
+      km[u] = lane ? r * 32 + lane - 1 : (TJ + 1) * 32 + r;
+      act[u] = true;
+    } else if (u == 0) {
+      wf[u] = HP + lane;
+      mo[u] = 16 + lane;
+      hs[u] = TJ * 32 + lane;
+      km[u] = 0;
+      act[u] = true;
+    } else {
+      wf[u] = (lane + 1) * RW + HP - 1;
+      mo[u] = (lane + 1) * MW + 15;
+      hs[u] = (TJ + 1) * 32 + lane;
+      km[u] = 0;
+      act[u] = u == 1 && lane < TJ;
+    }
+  }
+  const int jm0 = warp * R > 0 ? (warp * R - 1) * 32 + lane : TJ * 32 + lane;  // j-1 of row u = 0
+
+  T hnx[R], hny[R], hnz[R], hpx[R], hpy[R], hpz[R], hqy[R], hqz[R];
+  T eox[R], eoy[R], eoz[R], enx[R], eny[R], enz[R];
+  int em[R], enm[R];
+#pragma unroll
+  for (int u = 0; u < R; ++u) {
+    hnx[u] = hny[u] = hnz[u] = hpx[u] = hpy[u] = hpz[u] = hqy[u] = hqz[u] = T(0);
+    eox[u] = eoy[u] = eoz[u] = enx[u] = eny[u] = enz[u] = T(0);
+    em[u] = enm[u] = 0;
+  }
+  int slot = i_first % NS;
+  int waited = i_first - 1;
+  bool ok = mbar_wait(bar + slot, phase(i_first));
+  if (ok) waited = i_first;
+  for (int i = i_first; i <= i_end; ++i) {
+    const int ie = i - 1;
+    const bool do_h = i < i_end;
+    const int slot_n = slot + 1 == NS ? 0 : slot + 1;
+    const int slot_p = slot == 0 ? NS - 1 : slot - 1;
+    if (i + 1 <= i_end && ok) {
+      ok = mbar_wait(bar + slot_n, phase(i + 1));
+      if (ok) waited = i + 1;
+    }
+    if (__syncthreads_or(!ok)) {
+      ok = false;
+      break;
+    }
+    stage(i + NS - 1, slot_p);
+    if (tid == 0) {  // planes finished by iteration i-1 (fenced by their writers)
+      if (i - 1 >= i_start) {
+        const T* src = sH + ((i - 1) & 1) * 3 * CS;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) tma_store_3d(&outs->f[3 + c], src + c * CS, k0, j0, i - 1);
+      }
+      if (i - 2 >= i_start) {
+        const T* src = sE + ((i - 2) & 1) * 3 * ET;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) tma_store_3d(&outs->f[c], src + c * ET, k0, j0, i - 2);
+      }
+      bulk_commit();
+    }
+    const T* Fc = sF + slot * 6 * PL;
+    const T* Fn = sF + slot_n * 6 * PL;
+    const uint8_t* Mc = sM + slot * RH * MW;
+    slot = slot_n;
+    T* Hc = sH + (i & 1) * 3 * CS;              // H plane i (written here)
+    const T* Hq = sH + ((i + 1) & 1) * 3 * CS;  // H plane i-1
+    // ---- H pass, plane i ------------------------------------------------------
+    if (do_h) {
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        if (!act[u]) continue;
+        const int m = Mc[mo[u]];
+        const C4<T> cf = ld_c4(lut + 8 * m + 4);  // ch, db/dx, db/dy, db/dz
+        const T* f = Fc + wf[u];
+        const T ex_c = f[0], ey_c = f[PL], ez_c = f[2 * PL];
+        const T d_hx_a = f[PL + 1] - ey_c;
+        const T d_hx_b = f[2 * PL + RW] - ez_c;
+        const T d_hy_a = Fn[wf[u] + 2 * PL] - ez_c;
+        const T d_hy_b = f[1] - ex_c;
+        const T d_hz_a = f[RW] - ex_c;
+        const T d_hz_b = Fn[wf[u] + PL] - ey_c;
+        const T hxv = cf.c * f[3 * PL] + cf.z * d_hx_a - cf.y * d_hx_b;
+        const T hyv = cf.c * f[4 * PL] + cf.x * d_hy_a - cf.z * d_hy_b;
+        const T hzv = cf.c * f[5 * PL] + cf.y * d_hz_a - cf.x * d_hz_b;
+        Hc[hs[u]] = hxv;
+        Hc[CS + hs[u]] = hyv;
+        Hc[2 * CS + hs[u]] = hzv;
+        hnx[u] = hxv; hny[u] = hyv; hnz[u] = hzv;
+        enx[u] = ex_c; eny[u] = ey_c; enz[u] = ez_c;
+        enm[u] = m;
+      }
+    }
+    // ---- E pass, plane ie = i-1 ------------------------------------------------
+    if (row_warp && ie >= i_start) {
+      T* Eo = sE + (ie & 1) * 3 * ET;
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const C4<T> cf = ld_c4(lut + 8 * em[u]);  // ce, cb/dx, cb/dy, cb/dz
+        const T hx_c = hpx[u], hy_c = hpy[u], hz_c = hpz[u];
+        const T hx_km = Hq[km[u]], hy_km = Hq[CS + km[u]];
+        const T hx_jm = u > 0 ? hpx[u > 0 ? u - 1 : 0] : Hq[jm0];
+        const T hz_jm = u > 0 ? hpz[u > 0 ? u - 1 : 0] : Hq[2 * CS + jm0];
+        const T hy_p = hqy[u], hz_p = hqz[u];
+        const T d_ex_a = hy_c - hy_km;
+        const T d_ex_b = hz_c - hz_jm;
+        const T d_ey_a = hz_c - hz_p;
+        const T d_ey_b = hx_c - hx_km;
+        const T d_ez_a = hx_c - hx_jm;
+        const T d_ez_b = hy_c - hy_p;
+        const int o = (warp * R + u) * 32 + lane;
+        Eo[o] = cf.c * eox[u] - cf.z * d_ex_a + cf.y * d_ex_b;
+        Eo[ET + o] = cf.c * eoy[u] - cf.x * d_ey_a + cf.z * d_ey_b;
+        Eo[2 * ET + o] = cf.c * eoz[u] - cf.y * d_ez_a + cf.x * d_ez_b;
+      }
+    }
+    if (row_warp && do_h) {
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        hqy[u] = hpy[u]; hqz[u] = hpz[u];
+        hpx[u] = hnx[u]; hpy[u] = hny[u]; hpz[u] = hnz[u];
+        em[u] = enm[u];
+        eox[u] = enx[u]; eoy[u] = eny[u]; eoz[u] = enz[u];
+      }
+    }
+    fence_proxy_async();             // this thread's tile writes before the next iteration's bulk stores
+    if (tid == 0) bulk_wait_read();  // this iteration's stores have read their tiles
+  }
+  if (ok) {
+    __syncthreads();  // E plane i_end-1 is complete
+    if (tid == 0) {
+      if (i_end - 1 >= i_start) {
+        const T* src = sE + ((i_end - 1) & 1) * 3 * ET;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) tma_store_3d(&outs->f[c], src + c * ET, k0, j0, i_end - 1);
+      }
+      bulk_commit();
+      bulk_wait_all();
+    }
+  } else if (tid == 0) {
+    // a staging wait ran out: flag it, let the copies in flight land and the
+    // issued stores finish before the CTA exits
+    atomicExch(err, 1);
+    for (int p = waited + 1; p <= staged; ++p) mbar_wait(bar + p % NS, phase(p));
+    bulk_wait_all();
+  }
+}
+
 // The one-sweep step kernel: one CTA per work item (x: k tile | kind << 16,
 // y: j tile, z: first plane, w: end plane); every kind runs its own
 // specialised body, so one launch covers the whole grid.  Kind bits: 1 x-slab
@@ -727,6 +939,10 @@ __device__ __forceinline__ void step_dispatch(const GridP<T>& s, const GridP<T>&
                                               const PsiH<T>& ps, const PsiH<T>& pd, const TfsfP& tf,
                                               const AdeP<T>& ad, int4 item, const T* lut8, const uint8_t* disp,
                                               int n_mat, const StageMaps* maps, const StoreMaps* outs, int* err) {
+  if (TMA && (item.x >> 16) == kLeanInterior) {
+    step_item_lean<T, R, NWM, NS_>(item, lut8, n_mat, maps, outs, err);
+    return;
+  }
 #define XFB_ITEM(q) step_item<T, R, NWM, NS_, kStepKinds[q], TMA>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat, maps, err)
   switch (item.x >> 16) {
     case 0: XFB_ITEM(0); break;
@@ -742,8 +958,9 @@ __device__ __forceinline__ void step_dispatch(const GridP<T>& s, const GridP<T>&
 }
 
 // The single-scene step stages with tiled bulk copies from the tensor maps of
-// its read set (`maps`, a grid constant); a staging wait that runs out sets
-// *err.
+// its read set (`maps`, a grid constant) and its lean interior items store
+// through the maps of the write set (`outs`); a staging wait that runs out
+// sets *err.
 template <typename T, int R, int NWM, int NS_>
 __global__ void __launch_bounds__(StepCfg<T, R, NWM, NS_>::NT, StepCfg<T, R, NWM, NS_>::min_blocks)
     k_step3(GridP<T> s, GridP<T> d, PmlP<T> pm, PsiH<T> ps, PsiH<T> pd, TfsfP tf_in, AdeP<T> ad, TimeP tp,

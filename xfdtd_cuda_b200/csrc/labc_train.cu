@@ -1,8 +1,10 @@
 // Training of the learned absorbing boundary's MLP on the device (see
 // labc.cuh for the network).  Hand-written kernels: a fused forward and
-// backward pass over chunks of samples (activations in shared memory, weight
-// gradients reduced per block and added to the global gradient), BF16
-// rounding of the FP32 master weights for the forward pass, and Adam.
+// backward pass over chunks of samples (activations in shared memory; every
+// block walks a fixed set of chunks and keeps its weight gradients in
+// registers), a reduction of the per-block gradients in block order (so a
+// training run is reproducible bit for bit), BF16 rounding of the FP32 master
+// weights for the forward pass, and Adam.
 // No counterpart in the reference.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -17,8 +19,17 @@
 namespace xfb {
 namespace {
 
-constexpr int kChunk = 32;     // samples per block
+constexpr int kChunk = 32;     // samples per chunk
 constexpr int kThreads = 256;
+constexpr int kGradBlocks = 4 * 148;  // blocks of the gradient pass (at most)
+constexpr int kPerThread = (kMlpParams + kThreads - 1) / kThreads;  // gradient slots per thread
+
+// Blocks of the gradient pass for n samples (a function of n only, so the
+// summation order is fixed).
+inline int grad_blocks(int n) {
+  const int chunks = (n + kChunk - 1) / kChunk;
+  return chunks < kGradBlocks ? chunks : kGradBlocks;
+}
 
 thread_local std::string g_mlp_err;
 
@@ -34,11 +45,12 @@ __global__ void k_round_bf16(const float* w, float* wq, int n) {
   if (q < n) wq[q] = __bfloat162float(__float2bfloat16_rn(w[q]));
 }
 
-// Loss (sum of squared errors / n) and gradient of one chunk of samples,
-// added into loss[0] and grad[] (gradients w.r.t. the rounded weights, used
-// for the master weights: straight-through rounding).
+// Loss (sum of squared errors / n) and gradient over the chunks blockIdx.x,
+// blockIdx.x + gridDim.x, ... of the samples: per block into lpart[block] and
+// gpart[block][kMlpParams] (gradients w.r.t. the rounded weights, used for
+// the master weights: straight-through rounding).
 __global__ void __launch_bounds__(kThreads) k_mlp_grad(const float* wq, const float* x, const float* y, int n,
-                                                       double* loss, float* grad) {
+                                                       double* lpart, float* gpart) {
   extern __shared__ float sm[];
   float* w = sm;                            // kMlpParams
   float* xs = w + kMlpParams;               // [kChunk][8]
@@ -48,80 +60,113 @@ __global__ void __launch_bounds__(kThreads) k_mlp_grad(const float* wq, const fl
   float* d1 = d2 + kChunk * kMlpHid;        // [kChunk][64] dL/dz1
   float* dy = d1 + kChunk * kMlpHid;        // [kChunk]
   const int tid = threadIdx.x;
-  const int s0 = blockIdx.x * kChunk;
-  const int ns = min(kChunk, n - s0);
+  const int chunks = (n + kChunk - 1) / kChunk;
   for (int q = tid; q < kMlpParams; q += kThreads) w[q] = wq[q];
-  for (int q = tid; q < kChunk * kMlpIn; q += kThreads) xs[q] = q / kMlpIn < ns ? x[static_cast<long long>(s0) * kMlpIn + q] : 0.f;
-  __syncthreads();
-  // layer 1
-  for (int q = tid; q < kChunk * kMlpHid; q += kThreads) {
-    const int sm_ = q / kMlpHid, j = q % kMlpHid;
-    float a = w[kMlpB1 + j];
+  float acc[kPerThread];
 #pragma unroll
-    for (int k = 0; k < kMlpIn; ++k) a = fmaf(w[kMlpW1 + j * kMlpIn + k], xs[sm_ * kMlpIn + k], a);
-    h1[q] = tanhf(a);
-  }
-  __syncthreads();
-  // layer 2
-  for (int q = tid; q < kChunk * kMlpHid; q += kThreads) {
-    const int sm_ = q / kMlpHid, j = q % kMlpHid;
-    float a = w[kMlpB2 + j];
-    for (int k = 0; k < kMlpHid; ++k) a = fmaf(w[kMlpW2 + j * kMlpHid + k], h1[sm_ * kMlpHid + k], a);
-    h2[q] = tanhf(a);
-  }
-  __syncthreads();
-  // output and loss; dL/dy = 2 (y - t) / n
-  if (tid < kChunk) {
-    float e = 0.f;
-    if (tid < ns) {
-      float o = w[kMlpB3];
-      for (int j = 0; j < kMlpHid; ++j) o = fmaf(w[kMlpW3 + j], h2[tid * kMlpHid + j], o);
-      e = o - y[s0 + tid];
+  for (int r = 0; r < kPerThread; ++r) acc[r] = 0.f;
+  double loss = 0.0;  // thread 0
+  for (int ch = blockIdx.x; ch < chunks; ch += gridDim.x) {
+    const int s0 = ch * kChunk;
+    const int ns = min(kChunk, n - s0);
+    __syncthreads();  // the previous chunk's last reads are done
+    for (int q = tid; q < kChunk * kMlpIn; q += kThreads)
+      xs[q] = q / kMlpIn < ns ? x[static_cast<long long>(s0) * kMlpIn + q] : 0.f;
+    __syncthreads();
+    // layer 1
+    for (int q = tid; q < kChunk * kMlpHid; q += kThreads) {
+      const int sm_ = q / kMlpHid, j = q % kMlpHid;
+      float a = w[kMlpB1 + j];
+#pragma unroll
+      for (int k = 0; k < kMlpIn; ++k) a = fmaf(w[kMlpW1 + j * kMlpIn + k], xs[sm_ * kMlpIn + k], a);
+      h1[q] = tanhf(a);
     }
-    dy[tid] = 2.f * e / static_cast<float>(n);
-    double se = static_cast<double>(e) * e;
-    for (int o = 16; o > 0; o >>= 1) se += __shfl_down_sync(0xffffffffu, se, o);
-    if (tid == 0) atomicAdd(loss, se / n);
+    __syncthreads();
+    // layer 2
+    for (int q = tid; q < kChunk * kMlpHid; q += kThreads) {
+      const int sm_ = q / kMlpHid, j = q % kMlpHid;
+      float a = w[kMlpB2 + j];
+      for (int k = 0; k < kMlpHid; ++k) a = fmaf(w[kMlpW2 + j * kMlpHid + k], h1[sm_ * kMlpHid + k], a);
+      h2[q] = tanhf(a);
+    }
+    __syncthreads();
+    // output and loss; dL/dy = 2 (y - t) / n
+    if (tid < kChunk) {
+      float e = 0.f;
+      if (tid < ns) {
+        float o = w[kMlpB3];
+        for (int j = 0; j < kMlpHid; ++j) o = fmaf(w[kMlpW3 + j], h2[tid * kMlpHid + j], o);
+        e = o - y[s0 + tid];
+      }
+      dy[tid] = 2.f * e / static_cast<float>(n);
+      double se = static_cast<double>(e) * e;
+      for (int o = 16; o > 0; o >>= 1) se += __shfl_down_sync(0xffffffffu, se, o);
+      if (tid == 0) loss += se / n;
+    }
+    __syncthreads();
+    // dL/dz2 = dy * w3 * (1 - h2^2)
+    for (int q = tid; q < kChunk * kMlpHid; q += kThreads) {
+      const int sm_ = q / kMlpHid, j = q % kMlpHid;
+      const float t = h2[q];
+      d2[q] = dy[sm_] * w[kMlpW3 + j] * (1.f - t * t);
+    }
+    __syncthreads();
+    // dL/dz1 = (W2^T d2) * (1 - h1^2)
+    for (int q = tid; q < kChunk * kMlpHid; q += kThreads) {
+      const int sm_ = q / kMlpHid, k = q % kMlpHid;
+      float a = 0.f;
+      for (int j = 0; j < kMlpHid; ++j) a = fmaf(w[kMlpW2 + j * kMlpHid + k], d2[sm_ * kMlpHid + j], a);
+      const float t = h1[q];
+      d1[q] = a * (1.f - t * t);
+    }
+    __syncthreads();
+    // weight gradients of this chunk, parameters tid, tid + kThreads, ...
+#pragma unroll
+    for (int r = 0; r < kPerThread; ++r) {
+      const int p = tid + r * kThreads;
+      if (p >= kMlpParams) break;
+      float g = 0.f;
+      if (p < kMlpB1) {                       // W1[j][k]
+        const int j = p / kMlpIn, k = p % kMlpIn;
+        for (int q = 0; q < ns; ++q) g = fmaf(d1[q * kMlpHid + j], xs[q * kMlpIn + k], g);
+      } else if (p < kMlpW2) {                // b1[j]
+        const int j = p - kMlpB1;
+        for (int q = 0; q < ns; ++q) g += d1[q * kMlpHid + j];
+      } else if (p < kMlpB2) {                // W2[j][k]
+        const int j = (p - kMlpW2) / kMlpHid, k = (p - kMlpW2) % kMlpHid;
+        for (int q = 0; q < ns; ++q) g = fmaf(d2[q * kMlpHid + j], h1[q * kMlpHid + k], g);
+      } else if (p < kMlpW3) {                // b2[j]
+        const int j = p - kMlpB2;
+        for (int q = 0; q < ns; ++q) g += d2[q * kMlpHid + j];
+      } else if (p < kMlpB3) {                // w3[j]
+        const int j = p - kMlpW3;
+        for (int q = 0; q < ns; ++q) g = fmaf(dy[q], h2[q * kMlpHid + j], g);
+      } else {                                // b3
+        for (int q = 0; q < ns; ++q) g += dy[q];
+      }
+      acc[r] += g;
+    }
   }
-  __syncthreads();
-  // dL/dz2 = dy * w3 * (1 - h2^2)
-  for (int q = tid; q < kChunk * kMlpHid; q += kThreads) {
-    const int sm_ = q / kMlpHid, j = q % kMlpHid;
-    const float t = h2[q];
-    d2[q] = dy[sm_] * w[kMlpW3 + j] * (1.f - t * t);
+#pragma unroll
+  for (int r = 0; r < kPerThread; ++r) {
+    const int p = tid + r * kThreads;
+    if (p < kMlpParams) gpart[static_cast<long long>(blockIdx.x) * kMlpParams + p] = acc[r];
   }
-  __syncthreads();
-  // dL/dz1 = (W2^T d2) * (1 - h1^2)
-  for (int q = tid; q < kChunk * kMlpHid; q += kThreads) {
-    const int sm_ = q / kMlpHid, k = q % kMlpHid;
-    float a = 0.f;
-    for (int j = 0; j < kMlpHid; ++j) a = fmaf(w[kMlpW2 + j * kMlpHid + k], d2[sm_ * kMlpHid + j], a);
-    const float t = h1[q];
-    d1[q] = a * (1.f - t * t);
-  }
-  __syncthreads();
-  // weight gradients of this chunk, one parameter per thread iteration
-  for (int p = tid; p < kMlpParams; p += kThreads) {
+  if (tid == 0) lpart[blockIdx.x] = loss;
+}
+
+// Sum of the per-block parts in block order: grad[p] and, for the thread
+// with p == kMlpParams, the loss.
+__global__ void k_mlp_reduce(const double* lpart, const float* gpart, int blocks, double* loss, float* grad) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < kMlpParams) {
     float g = 0.f;
-    if (p < kMlpB1) {                       // W1[j][k]
-      const int j = p / kMlpIn, k = p % kMlpIn;
-      for (int q = 0; q < ns; ++q) g = fmaf(d1[q * kMlpHid + j], xs[q * kMlpIn + k], g);
-    } else if (p < kMlpW2) {                // b1[j]
-      const int j = p - kMlpB1;
-      for (int q = 0; q < ns; ++q) g += d1[q * kMlpHid + j];
-    } else if (p < kMlpB2) {                // W2[j][k]
-      const int j = (p - kMlpW2) / kMlpHid, k = (p - kMlpW2) % kMlpHid;
-      for (int q = 0; q < ns; ++q) g = fmaf(d2[q * kMlpHid + j], h1[q * kMlpHid + k], g);
-    } else if (p < kMlpW3) {                // b2[j]
-      const int j = p - kMlpB2;
-      for (int q = 0; q < ns; ++q) g += d2[q * kMlpHid + j];
-    } else if (p < kMlpB3) {                // w3[j]
-      const int j = p - kMlpW3;
-      for (int q = 0; q < ns; ++q) g = fmaf(dy[q], h2[q * kMlpHid + j], g);
-    } else {                                // b3
-      for (int q = 0; q < ns; ++q) g += dy[q];
-    }
-    atomicAdd(&grad[p], g);
+    for (int b = 0; b < blocks; ++b) g += gpart[static_cast<long long>(b) * kMlpParams + p];
+    grad[p] = g;
+  } else if (p == kMlpParams) {
+    double l = 0.0;
+    for (int b = 0; b < blocks; ++b) l += lpart[b];
+    *loss = l;
   }
 }
 
@@ -159,15 +204,29 @@ int upload_samples(const float* x, const float* y, int n, DevBuf& dx, DevBuf& dy
   return XFB_OK;
 }
 
-int launch_grad(const float* wq, const float* x, const float* y, int n, double* loss, float* grad) {
+// Per-block partial sums of the gradient pass for n samples.
+struct GradParts {
+  DevBuf l, g;
+  int blocks = 0;
+};
+
+int alloc_parts(int n, GradParts& gp) {
+  gp.blocks = grad_blocks(n);
+  MLP_CUDA(cudaMalloc(&gp.l.p, static_cast<size_t>(gp.blocks) * sizeof(double)));
+  MLP_CUDA(cudaMalloc(&gp.g.p, static_cast<size_t>(gp.blocks) * kMlpParams * sizeof(float)));
+  return XFB_OK;
+}
+
+int launch_grad(const float* wq, const float* x, const float* y, int n, GradParts& gp, double* loss, float* grad) {
   static bool attr = false;
   if (!attr) {
     MLP_CUDA(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kGradSmem)));
     attr = true;
   }
-  MLP_CUDA(cudaMemset(loss, 0, sizeof(double)));
-  MLP_CUDA(cudaMemset(grad, 0, kMlpParams * sizeof(float)));
-  k_mlp_grad<<<(n + kChunk - 1) / kChunk, kThreads, kGradSmem>>>(wq, x, y, n, loss, grad);
+  double* lp = static_cast<double*>(gp.l.p);
+  float* gq = static_cast<float*>(gp.g.p);
+  k_mlp_grad<<<gp.blocks, kThreads, kGradSmem>>>(wq, x, y, n, lp, gq);
+  k_mlp_reduce<<<(kMlpParams + 1 + 255) / 256, 256>>>(lp, gq, gp.blocks, loss, grad);
   MLP_CUDA(cudaGetLastError());
   return XFB_OK;
 }
@@ -186,15 +245,17 @@ const char* xfb_mlp_last_error(void) { return g_mlp_err.c_str(); }
 int xfb_mlp_loss_grad(const float* x, const float* y, int n, const float* w, double* loss, float* grad) {
   if (!x || !y || !w || !loss || !grad || n <= 0) return mlp_fail(XFB_ERR_INVALID, "null argument or n <= 0");
   DevBuf dx, dy, dw, dwq, dl, dg;
+  GradParts gp;
   int rc;
   if ((rc = upload_samples(x, y, n, dx, dy))) return rc;
+  if ((rc = alloc_parts(n, gp))) return rc;
   MLP_CUDA(cudaMalloc(&dw.p, kMlpParams * sizeof(float)));
   MLP_CUDA(cudaMalloc(&dwq.p, kMlpParams * sizeof(float)));
   MLP_CUDA(cudaMalloc(&dl.p, sizeof(double)));
   MLP_CUDA(cudaMalloc(&dg.p, kMlpParams * sizeof(float)));
   MLP_CUDA(cudaMemcpy(dw.p, w, kMlpParams * sizeof(float), cudaMemcpyHostToDevice));
   k_round_bf16<<<(kMlpParams + 255) / 256, 256>>>(static_cast<float*>(dw.p), static_cast<float*>(dwq.p), kMlpParams);
-  if ((rc = launch_grad(static_cast<float*>(dwq.p), static_cast<float*>(dx.p), static_cast<float*>(dy.p), n,
+  if ((rc = launch_grad(static_cast<float*>(dwq.p), static_cast<float*>(dx.p), static_cast<float*>(dy.p), n, gp,
                         static_cast<double*>(dl.p), static_cast<float*>(dg.p))))
     return rc;
   MLP_CUDA(cudaMemcpy(loss, dl.p, sizeof(double), cudaMemcpyDeviceToHost));
@@ -206,8 +267,10 @@ int xfb_mlp_train(const float* x, const float* y, int n, int iters, float lr, co
                   double* loss_curve) {
   if (!x || !y || !w_init || !w_out || n <= 0 || iters < 0) return mlp_fail(XFB_ERR_INVALID, "null argument or bad size");
   DevBuf dx, dy, dw, dwq, dm, dv, dl, dg;
+  GradParts gp;
   int rc;
   if ((rc = upload_samples(x, y, n, dx, dy))) return rc;
+  if ((rc = alloc_parts(n, gp))) return rc;
   const size_t wb = kMlpParams * sizeof(float);
   MLP_CUDA(cudaMalloc(&dw.p, wb));
   MLP_CUDA(cudaMalloc(&dwq.p, wb));
@@ -223,7 +286,7 @@ int xfb_mlp_train(const float* x, const float* y, int n, int iters, float lr, co
   double c1 = 1, c2 = 1;
   for (int it = 0; it < iters; ++it) {
     k_round_bf16<<<(kMlpParams + 255) / 256, 256>>>(w, static_cast<float*>(dwq.p), kMlpParams);
-    if ((rc = launch_grad(static_cast<float*>(dwq.p), static_cast<float*>(dx.p), static_cast<float*>(dy.p), n,
+    if ((rc = launch_grad(static_cast<float*>(dwq.p), static_cast<float*>(dx.p), static_cast<float*>(dy.p), n, gp,
                           static_cast<double*>(dl.p), static_cast<float*>(dg.p))))
       return rc;
     c1 *= b1;
