@@ -929,7 +929,10 @@ __device__ __forceinline__ void step_item_lean(int4 item, const T* lut8, int n_m
 // specialised body, so one launch covers the whole grid.  Kind bits: 1 x-slab
 // planes, 2 y-slab columns, 8 z-slab columns, 4 ADE box, 16 TFSF corrections;
 // only the lean kind (0) leaves the TFSF code out, kind 16 is lean with it.
-constexpr int kStepKinds[8] = {0, 1 | 16, 4 | 16, 3 | 16, 9 | 16, 11 | 16, 15 | 16, 16};
+// Kind indices 0..6: lean, x planes, ADE box, y columns, z columns, y+z
+// corner columns, ADE next to a slab, all without TFSF code; 7: lean with
+// TFSF; 8: lean interior (step_item_lean); 9..14: kinds 1..6 with TFSF.
+constexpr int kStepKinds[15] = {0, 1, 4, 3, 9, 11, 15, 16, 0, 1 | 16, 4 | 16, 3 | 16, 9 | 16, 11 | 16, 15 | 16};
 
 // kind index of the lean interior items (step_item_lean, bulk-copy path only)
 constexpr int kLeanInterior = 8;
@@ -952,7 +955,13 @@ __device__ __forceinline__ void step_dispatch(const GridP<T>& s, const GridP<T>&
     case 4: XFB_ITEM(4); break;
     case 5: XFB_ITEM(5); break;
     case 6: XFB_ITEM(6); break;
-    default: XFB_ITEM(7); break;
+    case 7: XFB_ITEM(7); break;
+    case 9: XFB_ITEM(9); break;
+    case 10: XFB_ITEM(10); break;
+    case 11: XFB_ITEM(11); break;
+    case 12: XFB_ITEM(12); break;
+    case 13: XFB_ITEM(13); break;
+    default: XFB_ITEM(14); break;
   }
 #undef XFB_ITEM
 }
