@@ -305,9 +305,9 @@ constexpr StepTile kStepTiles[2] = {{2, 4}, {2, 8}};
 // z-slab columns, 4 ADE box, 16 TFSF): lean, x planes, ADE box, y columns,
 // z columns, y+z corner columns, anything with ADE next to a slab (all
 // without TFSF code), lean with TFSF corrections, lean interior (the
-// bulk-copy path of single scenes), and kinds 1..6 with TFSF corrections for
-// the items that meet the TFSF surface
-constexpr int kStepKindCount = 15;
+// bulk-copy path of single scenes), kinds 1..6 with TFSF corrections for the
+// items that meet the TFSF surface, lean interior with TFSF corrections
+constexpr int kStepKindCount = 16;
 
 // True when a work item over planes [p, q) of the tile at (j0, k0) may meet a
 // TFSF correction: the cells it updates (H at planes p-1 .. q-1, rows j0-1 ..
@@ -378,8 +378,9 @@ inline void build_step_items(const Compiled& c, int TJ, int NT, bool ade_deferre
         int kind = kind_of(bits);
         if (tfsf_touch(c, p, q, j0, TJ, k0)) kind = kind == 0 ? 7 : kind + 8;
         // lean and fully inside: the tile, its halo row and column, first plane >= 1
-        if (kind == 0 && lean_interior && p >= 1 && j0 >= 1 && k0 >= 1 && j0 + TJ <= ny && k0 + 32 <= nz)
-          kind = kLeanInterior;
+        if ((kind == 0 || kind == 7) && lean_interior && p >= 1 && j0 >= 1 && k0 >= 1 && j0 + TJ <= ny &&
+            k0 + 32 <= nz)
+          kind = kind == 0 ? kLeanInterior : kLeanInteriorTf;
         out[kind].push_back(make_int4(bx, by, p, q));
         p = q;
       }
@@ -478,7 +479,7 @@ inline int upload_step_items(xfb_handle* h) {
     std::vector<int4> all, rest;
     for (int q : costly)
       for (int4 v : items[q]) all.push_back(make_int4(v.x | (q << 16), v.y, v.z, v.w));
-    for (int q : {0, 1, 7, kLeanInterior, 9})
+    for (int q : {0, 1, 7, kLeanInterior, 9, kLeanInteriorTf})
       for (int4 v : items[q]) rest.push_back(make_int4(v.x | (q << 16), v.y, v.z, v.w));
     std::stable_sort(rest.begin(), rest.end(), [](const int4& a, const int4& b) {
       if (a.z != b.z) return a.z < b.z;

@@ -211,6 +211,68 @@ struct Cell {
   int tfl;     // bit 0: on a TFSF H correction line (j = js-1, je or k = ks-1, ke); bit 1: E line (js, je, ks, ke)
 };
 
+// TFSF H corrections of cell (i, jj, kk), in the reference's agency order
+// (TFSFCorrector3DAgency::correctH, src/waveform_source/tfsf/tfsf_corrector.cu:237-271).
+template <typename T>
+__device__ __forceinline__ void tfsf_h(const TfsfP& tf, int i, int jj, int kk, T& hxv, T& hyv, T& hzv) {
+  const bool iin = i >= tf.is && i <= tf.ie, jin = jj >= tf.js && jj <= tf.je, kin = kk >= tf.ks && kk <= tf.ke;
+  if (jin && jj < tf.je && kin) {
+    if (i == tf.is - 1) add_inc(hzv, ey_inc(tf, tf.is, jj, kk), tf.cb[0]);
+    if (i == tf.ie) add_inc(hzv, ey_inc(tf, tf.ie, jj, kk), -tf.cb[0]);
+  }
+  if (iin && i < tf.ie && kin) {
+    if (jj == tf.js - 1) add_inc(hzv, ex_inc(tf, i, tf.js, kk), -tf.cb[1]);
+    if (jj == tf.je) add_inc(hzv, ex_inc(tf, i, tf.je, kk), tf.cb[1]);
+  }
+  if (iin && jin && jj < tf.je) {
+    if (kk == tf.ks - 1) add_inc(hxv, ey_inc(tf, i, jj, tf.ks), -tf.cb[2]);
+    if (kk == tf.ke) add_inc(hxv, ey_inc(tf, i, jj, tf.ke), tf.cb[2]);
+  }
+  if (iin && kin && kk < tf.ke) {
+    if (jj == tf.js - 1) add_inc(hxv, ez_inc(tf, i, tf.js, kk), tf.cb[1]);
+    if (jj == tf.je) add_inc(hxv, ez_inc(tf, i, tf.je, kk), -tf.cb[1]);
+  }
+  if (iin && i < tf.ie && jin) {
+    if (kk == tf.ks - 1) add_inc(hyv, ex_inc(tf, i, jj, tf.ks), tf.cb[2]);
+    if (kk == tf.ke) add_inc(hyv, ex_inc(tf, i, jj, tf.ke), -tf.cb[2]);
+  }
+  if (jin && kin && kk < tf.ke) {
+    if (i == tf.is - 1) add_inc(hyv, ez_inc(tf, tf.is, jj, kk), -tf.cb[0]);
+    if (i == tf.ie) add_inc(hyv, ez_inc(tf, tf.ie, jj, kk), tf.cb[0]);
+  }
+}
+
+// TFSF E corrections of cell (i, j, k) (TFSFCorrector3DAgency::correctE,
+// src/waveform_source/tfsf/tfsf_corrector.cu:201-236).
+template <typename T>
+__device__ __forceinline__ void tfsf_e(const TfsfP& tf, int i, int j, int k, T& exv, T& eyv, T& ezv) {
+  const bool iin = i >= tf.is && i <= tf.ie, jin = j >= tf.js && j <= tf.je, kin = k >= tf.ks && k <= tf.ke;
+  if (jin && kin && k < tf.ke) {
+    if (i == tf.is) add_inc(ezv, hy_inc(tf, tf.is - 1, j, k), -tf.ca[0]);
+    if (i == tf.ie) add_inc(ezv, hy_inc(tf, tf.ie, j, k), tf.ca[0]);
+  }
+  if (iin && kin && k < tf.ke) {
+    if (j == tf.js) add_inc(ezv, hx_inc(tf, i, tf.js - 1, k), tf.ca[1]);
+    if (j == tf.je) add_inc(ezv, hx_inc(tf, i, tf.je, k), -tf.ca[1]);
+  }
+  if (iin && i < tf.ie && jin) {
+    if (k == tf.ks) add_inc(exv, hy_inc(tf, i, j, tf.ks - 1), tf.ca[2]);
+    if (k == tf.ke) add_inc(exv, hy_inc(tf, i, j, tf.ke), -tf.ca[2]);
+  }
+  if (iin && i < tf.ie && kin) {
+    if (j == tf.js) add_inc(exv, hz_inc(tf, i, tf.js - 1, k), -tf.ca[1]);
+    if (j == tf.je) add_inc(exv, hz_inc(tf, i, tf.je, k), tf.ca[1]);
+  }
+  if (iin && jin && j < tf.je) {
+    if (k == tf.ks) add_inc(eyv, hx_inc(tf, i, j, tf.ks - 1), -tf.ca[2]);
+    if (k == tf.ke) add_inc(eyv, hx_inc(tf, i, j, tf.ke), tf.ca[2]);
+  }
+  if (jin && j < tf.je && kin) {
+    if (i == tf.is) add_inc(eyv, hz_inc(tf, tf.is - 1, j, k), tf.ca[0]);
+    if (i == tf.ie) add_inc(eyv, hz_inc(tf, tf.ie, j, k), -tf.ca[0]);
+  }
+}
+
 // H^{n+1/2} of cell c at plane i: hNext from the staged E^n planes i and i+1
 // and H^{n-1/2}, then the TFSF and CPML corrections of H.  Stores the result
 // in the shared H plane; `own` also writes it (and the new H psi) to HBM
@@ -240,34 +302,7 @@ __device__ __forceinline__ void h_cell(const HCtx<T>& x, const T* Fc, const T* F
   hzv = cf.c * f[5 * PL] + cf.y * d_hz_a - cf.x * d_hz_b;
   const TfsfP& tf = x.tf;
   const int j = c.j, k = c.k;
-  if (((KIND & 16) != 0) && (tf_hplane || (c.tfl & 1))) {
-    const int jj = j, kk = k;
-    const bool iin = i >= tf.is && i <= tf.ie, jin = jj >= tf.js && jj <= tf.je, kin = kk >= tf.ks && kk <= tf.ke;
-    if (jin && jj < tf.je && kin) {
-      if (i == tf.is - 1) add_inc(hzv, ey_inc(tf, tf.is, jj, kk), tf.cb[0]);
-      if (i == tf.ie) add_inc(hzv, ey_inc(tf, tf.ie, jj, kk), -tf.cb[0]);
-    }
-    if (iin && i < tf.ie && kin) {
-      if (jj == tf.js - 1) add_inc(hzv, ex_inc(tf, i, tf.js, kk), -tf.cb[1]);
-      if (jj == tf.je) add_inc(hzv, ex_inc(tf, i, tf.je, kk), tf.cb[1]);
-    }
-    if (iin && jin && jj < tf.je) {
-      if (kk == tf.ks - 1) add_inc(hxv, ey_inc(tf, i, jj, tf.ks), -tf.cb[2]);
-      if (kk == tf.ke) add_inc(hxv, ey_inc(tf, i, jj, tf.ke), tf.cb[2]);
-    }
-    if (iin && kin && kk < tf.ke) {
-      if (jj == tf.js - 1) add_inc(hxv, ez_inc(tf, i, tf.js, kk), tf.cb[1]);
-      if (jj == tf.je) add_inc(hxv, ez_inc(tf, i, tf.je, kk), -tf.cb[1]);
-    }
-    if (iin && i < tf.ie && jin) {
-      if (kk == tf.ks - 1) add_inc(hyv, ex_inc(tf, i, jj, tf.ks), tf.cb[2]);
-      if (kk == tf.ke) add_inc(hyv, ex_inc(tf, i, jj, tf.ke), -tf.cb[2]);
-    }
-    if (jin && kin && kk < tf.ke) {
-      if (i == tf.is - 1) add_inc(hyv, ez_inc(tf, tf.is, jj, kk), -tf.cb[0]);
-      if (i == tf.ie) add_inc(hyv, ez_inc(tf, tf.ie, jj, kk), tf.cb[0]);
-    }
-  }
+  if (((KIND & 16) != 0) && (tf_hplane || (c.tfl & 1))) tfsf_h(tf, i, j, k, hxv, hyv, hzv);
   constexpr bool PX = (KIND & 1) != 0, PY = (KIND & 2) != 0, PZ = (KIND & 8) != 0;
   if (PX || PY || PZ) {
     const PmlP<T>& pm = x.pm;
@@ -618,34 +653,7 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
           if (upd_y) eyv = ade_e(ad, 1, abi, m, ey_o, eyv);
           if (upd_z) ezv = ade_e(ad, 2, abi, m, ez_o, ezv);
         }
-        if (TFC && (tf_eplane || (c.tfl & 2))) {
-          const int i = ie;
-          const bool iin = i >= tf.is && i <= tf.ie, jin = j >= tf.js && j <= tf.je, kin = k >= tf.ks && k <= tf.ke;
-          if (jin && kin && k < tf.ke) {
-            if (i == tf.is) add_inc(ezv, hy_inc(tf, tf.is - 1, j, k), -tf.ca[0]);
-            if (i == tf.ie) add_inc(ezv, hy_inc(tf, tf.ie, j, k), tf.ca[0]);
-          }
-          if (iin && kin && k < tf.ke) {
-            if (j == tf.js) add_inc(ezv, hx_inc(tf, i, tf.js - 1, k), tf.ca[1]);
-            if (j == tf.je) add_inc(ezv, hx_inc(tf, i, tf.je, k), -tf.ca[1]);
-          }
-          if (iin && i < tf.ie && jin) {
-            if (k == tf.ks) add_inc(exv, hy_inc(tf, i, j, tf.ks - 1), tf.ca[2]);
-            if (k == tf.ke) add_inc(exv, hy_inc(tf, i, j, tf.ke), -tf.ca[2]);
-          }
-          if (iin && i < tf.ie && kin) {
-            if (j == tf.js) add_inc(exv, hz_inc(tf, i, tf.js - 1, k), -tf.ca[1]);
-            if (j == tf.je) add_inc(exv, hz_inc(tf, i, tf.je, k), tf.ca[1]);
-          }
-          if (iin && jin && j < tf.je) {
-            if (k == tf.ks) add_inc(eyv, hx_inc(tf, i, j, tf.ks - 1), -tf.ca[2]);
-            if (k == tf.ke) add_inc(eyv, hx_inc(tf, i, j, tf.ke), tf.ca[2]);
-          }
-          if (jin && j < tf.je && kin) {
-            if (i == tf.is) add_inc(eyv, hz_inc(tf, tf.is - 1, j, k), tf.ca[0]);
-            if (i == tf.ie) add_inc(eyv, hz_inc(tf, tf.ie, j, k), -tf.ca[0]);
-          }
-        }
+        if (TFC && (tf_eplane || (c.tfl & 2))) tfsf_e(tf, ie, j, k, exv, eyv, ezv);
         if (PML) {
           const int sy_pml = c.py, sz_pml = c.pz;
           if (sxe >= 0 || sy_pml >= 0 || sz_pml >= 0) {
@@ -722,10 +730,11 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
 // At iteration i one thread issues the stores of H plane i-1 and E plane i-2
 // (both finished before the iteration's barrier) and waits, before the next
 // barrier, until they have read their tiles; so no thread computes a global
-// address or issues a global store.
-template <typename T, int R, int NWM, int NS_>
-__device__ __forceinline__ void step_item_lean(int4 item, const T* lut8, int n_mat, const StageMaps* maps,
-                                               const StoreMaps* outs, int* err) {
+// address or issues a global store.  TF: with the TFSF corrections of the
+// cells on the TFSF surface (tfsf_h / tfsf_e, as in step_item).
+template <typename T, int R, int NWM, int NS_, bool TF>
+__device__ __forceinline__ void step_item_lean(int4 item, const T* lut8, int n_mat, const TfsfP& tf,
+                                               const StageMaps* maps, const StoreMaps* outs, int* err) {
   using L = StepCfg<T, R, NWM, NS_>;
   constexpr int NS = L::NS, HP = L::HP, RW = L::RW, MW = L::MW, TJ = L::TJ, PL = L::PL, NT = L::NT, RH = L::RH;
   constexpr int CS = L::LCS, ET = TJ * 32;
@@ -771,9 +780,15 @@ __device__ __forceinline__ void step_item_lean(int4 item, const T* lut8, int n_m
   // the H tile, km: the k-1 neighbour's slot (row warps).
   const bool row_warp = warp < NWM;
   int wf[R], mo[R], hs[R], km[R];
+  int cj[R], ck[R], tfl[R];  // cell indices and TFSF line flags (TF only)
   bool act[R];
 #pragma unroll
   for (int u = 0; u < R; ++u) {
+    cj[u] = row_warp ? j0 + warp * R + u : (u == 0 ? j0 - 1 : j0 + lane);
+    ck[u] = row_warp ? k0 + lane : (u == 0 ? k0 + lane : k0 - 1);
+    tfl[u] = TF && tf.on ? ((cj[u] == tf.js - 1 || cj[u] == tf.je || ck[u] == tf.ks - 1 || ck[u] == tf.ke) ? 1 : 0) |
+                               ((cj[u] == tf.js || cj[u] == tf.je || ck[u] == tf.ks || ck[u] == tf.ke) ? 2 : 0)
+                         : 0;
     if (row_warp) {
       const int r = warp * R + u;
       wf[u] = (r + 1) * RW + HP + lane;
@@ -844,6 +859,7 @@ __device__ __forceinline__ void step_item_lean(int4 item, const T* lut8, int n_m
     T* Hc = sH + (i & 1) * 3 * CS;              // H plane i (written here)
     const T* Hq = sH + ((i + 1) & 1) * 3 * CS;  // H plane i-1
     // ---- H pass, plane i ------------------------------------------------------
+    const bool tf_hplane = TF && tf.on && (i == tf.is - 1 || i == tf.ie);
     if (do_h) {
 #pragma unroll
       for (int u = 0; u < R; ++u) {
@@ -858,9 +874,10 @@ __device__ __forceinline__ void step_item_lean(int4 item, const T* lut8, int n_m
         const T d_hy_b = f[1] - ex_c;
         const T d_hz_a = f[RW] - ex_c;
         const T d_hz_b = Fn[wf[u] + PL] - ey_c;
-        const T hxv = cf.c * f[3 * PL] + cf.z * d_hx_a - cf.y * d_hx_b;
-        const T hyv = cf.c * f[4 * PL] + cf.x * d_hy_a - cf.z * d_hy_b;
-        const T hzv = cf.c * f[5 * PL] + cf.y * d_hz_a - cf.x * d_hz_b;
+        T hxv = cf.c * f[3 * PL] + cf.z * d_hx_a - cf.y * d_hx_b;
+        T hyv = cf.c * f[4 * PL] + cf.x * d_hy_a - cf.z * d_hy_b;
+        T hzv = cf.c * f[5 * PL] + cf.y * d_hz_a - cf.x * d_hz_b;
+        if (TF && (tf_hplane || (tfl[u] & 1))) tfsf_h(tf, i, cj[u], ck[u], hxv, hyv, hzv);
         Hc[hs[u]] = hxv;
         Hc[CS + hs[u]] = hyv;
         Hc[2 * CS + hs[u]] = hzv;
@@ -870,6 +887,7 @@ __device__ __forceinline__ void step_item_lean(int4 item, const T* lut8, int n_m
       }
     }
     // ---- E pass, plane ie = i-1 ------------------------------------------------
+    const bool tf_eplane = TF && tf.on && (ie == tf.is || ie == tf.ie);
     if (row_warp && ie >= i_start) {
       T* Eo = sE + (ie & 1) * 3 * ET;
 #pragma unroll
@@ -887,9 +905,13 @@ __device__ __forceinline__ void step_item_lean(int4 item, const T* lut8, int n_m
         const T d_ez_a = hx_c - hx_jm;
         const T d_ez_b = hy_c - hy_p;
         const int o = (warp * R + u) * 32 + lane;
-        Eo[o] = cf.c * eox[u] - cf.z * d_ex_a + cf.y * d_ex_b;
-        Eo[ET + o] = cf.c * eoy[u] - cf.x * d_ey_a + cf.z * d_ey_b;
-        Eo[2 * ET + o] = cf.c * eoz[u] - cf.y * d_ez_a + cf.x * d_ez_b;
+        T exv = cf.c * eox[u] - cf.z * d_ex_a + cf.y * d_ex_b;
+        T eyv = cf.c * eoy[u] - cf.x * d_ey_a + cf.z * d_ey_b;
+        T ezv = cf.c * eoz[u] - cf.y * d_ez_a + cf.x * d_ez_b;
+        if (TF && (tf_eplane || (tfl[u] & 2))) tfsf_e(tf, ie, cj[u], ck[u], exv, eyv, ezv);
+        Eo[o] = exv;
+        Eo[ET + o] = eyv;
+        Eo[2 * ET + o] = ezv;
       }
     }
     if (row_warp && do_h) {
@@ -931,11 +953,13 @@ __device__ __forceinline__ void step_item_lean(int4 item, const T* lut8, int n_m
 // only the lean kind (0) leaves the TFSF code out, kind 16 is lean with it.
 // Kind indices 0..6: lean, x planes, ADE box, y columns, z columns, y+z
 // corner columns, ADE next to a slab, all without TFSF code; 7: lean with
-// TFSF; 8: lean interior (step_item_lean); 9..14: kinds 1..6 with TFSF.
-constexpr int kStepKinds[15] = {0, 1, 4, 3, 9, 11, 15, 16, 0, 1 | 16, 4 | 16, 3 | 16, 9 | 16, 11 | 16, 15 | 16};
+// TFSF; 8: lean interior (step_item_lean); 9..14: kinds 1..6 with TFSF;
+// 15: lean interior with TFSF.
+constexpr int kStepKinds[16] = {0, 1, 4, 3, 9, 11, 15, 16, 0, 1 | 16, 4 | 16, 3 | 16, 9 | 16, 11 | 16, 15 | 16, 16};
 
-// kind index of the lean interior items (step_item_lean, bulk-copy path only)
-constexpr int kLeanInterior = 8;
+// kind indices of the lean interior items (step_item_lean, bulk-copy path
+// only), without and with TFSF corrections
+constexpr int kLeanInterior = 8, kLeanInteriorTf = 15;
 
 template <typename T, int R, int NWM, int NS_, bool TMA>
 __device__ __forceinline__ void step_dispatch(const GridP<T>& s, const GridP<T>& d, const PmlP<T>& pm,
@@ -943,7 +967,11 @@ __device__ __forceinline__ void step_dispatch(const GridP<T>& s, const GridP<T>&
                                               const AdeP<T>& ad, int4 item, const T* lut8, const uint8_t* disp,
                                               int n_mat, const StageMaps* maps, const StoreMaps* outs, int* err) {
   if (TMA && (item.x >> 16) == kLeanInterior) {
-    step_item_lean<T, R, NWM, NS_>(item, lut8, n_mat, maps, outs, err);
+    step_item_lean<T, R, NWM, NS_, false>(item, lut8, n_mat, tf, maps, outs, err);
+    return;
+  }
+  if (TMA && (item.x >> 16) == kLeanInteriorTf) {
+    step_item_lean<T, R, NWM, NS_, true>(item, lut8, n_mat, tf, maps, outs, err);
     return;
   }
 #define XFB_ITEM(q) step_item<T, R, NWM, NS_, kStepKinds[q], TMA>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat, maps, err)
