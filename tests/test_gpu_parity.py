@@ -127,6 +127,25 @@ def test_fp64_no_tfsf_no_pml_initial_field(path):
     assert bit_equal(gf, of)
 
 
+def test_fp64_nf2ff_reads_between_steps():
+    # surface samples wait in a ring for several steps before they reach the
+    # NF2FF accumulators; reads in the middle of a run (which flush the ring)
+    # at step counts on and off the ring length change no bit of the result
+    sim = small_sphere()
+    n = 61
+    h = engine(sim, n, path=2)
+    for chunk in (5, 3, 8, 13, 1, 31):
+        h.step(chunk)
+        h.read_nf2ff(1, 3, 2)
+    h.sync()
+    o = oracle_of(sim, n)
+    o.run(n)
+    for f in range(2):
+        for face in range(6):
+            for w in range(4):
+                assert np.array_equal(h.read_nf2ff(f, face, w), o.nf2ff(f, face, w))
+
+
 def elongated_scene(precision="fp64"):
     # 36 x 56 x 104 inner cells of 3 mm + 6-cell CPML: the one-sweep tiles at
     # k0 = 32 and 64 away from the TFSF faces are lean interior work items
@@ -268,6 +287,9 @@ def test_checkpoint_resume_equivalence():
     b.sync()
     assert bit_equal(fields_of(b, 3), fields_of(a, 3))
     assert np.array_equal(a.read_probe(0), b.read_probe(0))
+    for face in range(6):  # NF2FF accumulators across a checkpoint taken off the sample-ring boundary
+        for w in range(4):
+            assert np.array_equal(a.read_nf2ff(0, face, w), b.read_nf2ff(0, face, w))
 
 
 def test_watchdog_and_errors():

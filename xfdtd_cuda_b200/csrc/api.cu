@@ -483,6 +483,30 @@ int xfb_nf2ff_face_shape(const xfb_handle* h, int face, int s[3]) {
   return XFB_OK;
 }
 
+// Accumulates the NF2FF surface samples still in the ring (k_nf2ff keeps the
+// samples of up to kNfRing steps before it adds them), so the accumulators
+// hold every step taken.  Enqueued on the stream that steps the handle (the
+// batch's stream while a batch steps it); launches kernels only.
+static int nf2ff_flush(xfb_handle* h) {
+  if (!h->c.nf_on || !h->nf_ring) return XFB_OK;
+  cudaStream_t s = h->batch ? h->batch->stream : h->stream;
+  const Compiled& c = h->c;
+  NfP nf{};
+  nf.nfreq = static_cast<int>(c.freqs.size());
+  for (int q = 0; q < 6; ++q) nf.box[q] = c.nf[q];
+  for (int q = 0; q < 7; ++q) nf.off[q] = h->nf_off[q];
+  nf.npts = h->nf_npts;
+  nf.acc = h->nf_acc; nf.te = h->te; nf.th = h->th;
+  nf.total_steps = c.total_steps;
+  nf.ring = h->nf_ring;
+  nf.done = h->nf_done;
+  k_nf2ff_flush<<<static_cast<unsigned>((h->nf_npts + 255) / 256), 256, 0, s>>>(nf, h->step);
+  k_nf2ff_done<<<1, 1, 0, s>>>(h->nf_done, h->step);
+  XFB_CUDA(h, cudaGetLastError());
+  if (s != h->stream) XFB_CUDA(h, cudaStreamSynchronize(s));
+  return XFB_OK;
+}
+
 int xfb_read_nf2ff(xfb_handle* h, int freq, int face, int which, double* dst, size_t len) {
   int rc = check_handle(h, true);
   if (rc) return rc;
@@ -492,6 +516,7 @@ int xfb_read_nf2ff(xfb_handle* h, int freq, int face, int which, double* dst, si
     return set_err(h, XFB_ERR_RANGE, "frequency or current index out of range");
   const size_t n = static_cast<size_t>(s[0]) * s[1] * s[2];
   if (len < 2 * n) return set_err(h, XFB_ERR_RANGE, "destination too small (complex interleaved)");
+  if ((rc = nf2ff_flush(h))) return rc;
   XFB_CUDA(h, cudaStreamSynchronize(h->stream));
   const double2* src = h->nf_acc + (static_cast<long long>(freq) * 4 + which) * h->nf_npts + h->nf_off[face];
   if ((rc = copy(h, dst, src, n * sizeof(double2), cudaMemcpyDeviceToHost))) return rc;
@@ -505,6 +530,7 @@ int xfb_far_field(xfb_handle* h, int freq, int n, const double* theta, const dou
   if (freq < 0 || freq >= static_cast<int>(h->c.freqs.size())) return set_err(h, XFB_ERR_RANGE, "frequency index out of range");
   if (n < 0 || (n > 0 && (!theta || !phi || !out))) return set_err(h, XFB_ERR_INVALID, "bad angle arrays");
   if (n == 0) return XFB_OK;
+  if ((rc = nf2ff_flush(h))) return rc;
   double *d_th = nullptr, *d_ph = nullptr, *d_out = nullptr;
   XFB_CUDA(h, cudaMalloc(&d_th, n * sizeof(double)));
   XFB_CUDA(h, cudaMalloc(&d_ph, n * sizeof(double)));
@@ -541,6 +567,7 @@ int xfb_far_field_static(xfb_handle* h, int freq, int n, const double* theta, co
                    "xfb_far_field_static takes at most " + std::to_string(kFarStaticMaxAngles) +
                        " angles per call (its scratch is a fixed device array); got " + std::to_string(n));
   if (n == 0) return XFB_OK;
+  if ((rc = nf2ff_flush(h))) return rc;
   double* scratch = nullptr;
   if ((rc = far_scratch_for(h, &scratch))) return rc;
   double* d_th = scratch;
@@ -582,6 +609,7 @@ int xfb_get_state(xfb_handle* h, void* dst, size_t len) {
   size_t need;
   if ((rc = xfb_state_size(h, &need))) return rc;
   if (!dst || len < need) return set_err(h, XFB_ERR_RANGE, "state buffer too small");
+  if ((rc = nf2ff_flush(h))) return rc;  // the state holds accumulators, not the sample ring
   XFB_CUDA(h, cudaStreamSynchronize(h->stream));
   char* o = static_cast<char*>(dst);
   std::memcpy(o, &h->step, sizeof(long long));

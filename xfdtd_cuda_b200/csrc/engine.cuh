@@ -153,6 +153,10 @@ int init_device(xfb_handle* h) {
     void* p;
     if ((rc = alloc(h, &p, nfq * 4 * h->nf_npts * sizeof(double2), true))) return rc;
     h->nf_acc = static_cast<double2*>(p);
+    if ((rc = alloc(h, &p, static_cast<size_t>(kNfRing) * 4 * h->nf_npts * sizeof(double), false))) return rc;
+    h->nf_ring = static_cast<double*>(p);
+    if ((rc = alloc(h, &p, sizeof(long long), true))) return rc;
+    h->nf_done = static_cast<long long*>(p);
     if ((rc = upload<double>(h, &p, c.te))) return rc;
     h->te = static_cast<double2*>(p);
     if ((rc = upload<double>(h, &p, c.th))) return rc;
@@ -636,6 +640,8 @@ void enqueue_records(xfb_handle* h, int parity, TimeP tp, cudaStream_t s, Prof* 
     nf.npts = h->nf_npts;
     nf.acc = h->nf_acc; nf.te = h->te; nf.th = h->th;
     nf.total_steps = c.total_steps;
+    nf.ring = h->nf_ring;
+    nf.done = h->nf_done;
     prof_begin(h, pf, XFB_K_NF2FF);
     k_nf2ff<T><<<static_cast<unsigned>((h->nf_npts + 255) / 256), 256, 0, s>>>(g, nf, tp);
     prof_end(h, pf);

@@ -64,6 +64,8 @@ struct xfb_handle {
   long long bsx = 0, bsy = 0, bn = 0;
   // NF2FF
   double2* nf_acc = nullptr;
+  double* nf_ring = nullptr;     // [kNfRing][4][npts] surface samples not yet accumulated
+  long long* nf_done = nullptr;  // steps accumulated by the last flush
   double2* te = nullptr;
   double2* th = nullptr;
   int nf_off[7] = {};

@@ -630,7 +630,16 @@ static __global__ void k_bump(long long* t, int n) { *t += n; }
 
 // ---------------------------------------------------------------------------
 // NF2FF frequency-domain accumulation: one thread per face point, all faces and
-// frequencies in one launch.
+// frequencies in one launch.  The four surface samples of a point (the
+// interpolated tangential H and E with the current signs) are kept for
+// kNfRing steps in a ring; every kNfRing-th step the point's accumulators are
+// read once, advanced over the buffered steps in step order, and written
+// back, so the running DFT costs one accumulator round trip per kNfRing steps
+// instead of one per step.  A host read first runs k_nf2ff_flush over the
+// steps still in the ring; `done` (steps already in the accumulators beyond
+// the last full ring) keeps a flushed step from being added twice.
+constexpr int kNfRing = 8;
+
 struct NfP {
   int nfreq;
   int box[6];                 // is ie js je ks ke
@@ -639,7 +648,66 @@ struct NfP {
   double2* acc;               // [nfreq][4][npts]  ja jb ma mb
   const double2* te; const double2* th;  // [nfreq][total_steps]
   long long total_steps;
+  double* ring;               // [kNfRing][4][npts] samples of the buffered steps
+  long long* done;            // steps accumulated by the last flush
 };
+
+// Advance the accumulators of point pt over steps lo .. hi-1 taken from the
+// ring, then (cur) over step hi with the samples s[4]; frequencies in groups
+// of four so the accumulators of a group stay in registers.  Every
+// accumulator sees its steps in increasing order, as in a per-step update.
+__device__ __forceinline__ void nf_advance(const NfP& nf, long long pt, long long lo, long long hi, bool cur,
+                                           const double s[4]) {
+  for (int f0 = 0; f0 < nf.nfreq; f0 += 4) {
+    const int nfg = min(4, nf.nfreq - f0);
+    double2 a[4][4];
+#pragma unroll
+    for (int g = 0; g < 4; ++g)
+      if (g < nfg)
+#pragma unroll
+        for (int w = 0; w < 4; ++w) a[g][w] = nf.acc[(static_cast<long long>(f0 + g) * 4 + w) * nf.npts + pt];
+    for (long long t = lo; t <= hi; ++t) {
+      if (t == hi && !cur) break;
+      double v[4];
+      if (t == hi) {
+#pragma unroll
+        for (int w = 0; w < 4; ++w) v[w] = s[w];
+      } else {
+        const double* r = nf.ring + static_cast<long long>(t % kNfRing) * 4 * nf.npts + pt;
+#pragma unroll
+        for (int w = 0; w < 4; ++w) v[w] = r[w * nf.npts];
+      }
+#pragma unroll
+      for (int g = 0; g < 4; ++g)
+        if (g < nfg) {
+          const double2 th = nf.th[(f0 + g) * nf.total_steps + t], te = nf.te[(f0 + g) * nf.total_steps + t];
+          a[g][0].x = a[g][0].x + v[0] * th.x; a[g][0].y = a[g][0].y + v[0] * th.y;
+          a[g][1].x = a[g][1].x + v[1] * th.x; a[g][1].y = a[g][1].y + v[1] * th.y;
+          a[g][2].x = a[g][2].x + v[2] * te.x; a[g][2].y = a[g][2].y + v[2] * te.y;
+          a[g][3].x = a[g][3].x + v[3] * te.x; a[g][3].y = a[g][3].y + v[3] * te.y;
+        }
+    }
+#pragma unroll
+    for (int g = 0; g < 4; ++g)
+      if (g < nfg)
+#pragma unroll
+        for (int w = 0; w < 4; ++w) nf.acc[(static_cast<long long>(f0 + g) * 4 + w) * nf.npts + pt] = a[g][w];
+  }
+}
+
+// Steps [max(t_end - t_end % kNfRing, *done), t_end) still in the ring into
+// the accumulators (t_end: steps taken).  *done is set afterwards by
+// k_nf2ff_done, so every thread reads the value of before the flush.
+static __global__ void k_nf2ff_flush(NfP nf, long long t_end) {
+  const long long pt = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (pt >= nf.npts) return;
+  const long long lo = max(t_end - t_end % kNfRing, *nf.done);
+  if (lo >= t_end) return;
+  const double none[4] = {0, 0, 0, 0};
+  nf_advance(nf, pt, lo, t_end, false, none);
+}
+
+static __global__ void k_nf2ff_done(long long* done, long long v) { *done = v; }
 
 template <typename T>
 __device__ __forceinline__ double ld(const T* p, long long i) { return static_cast<double>(p[i]); }
@@ -679,16 +747,15 @@ __global__ void k_nf2ff(GridP<T> g, NfP nf, TimeP tp) {
   }
   const double cja = pos ? -1.0 : 1.0, cjb = pos ? 1.0 : -1.0;
   const double cma = pos ? 1.0 : -1.0, cmb = pos ? -1.0 : 1.0;
-  const double sja = cja * hb, sjb = cjb * ha, sma = cma * eb, smb = cmb * ea;
-  for (int f = 0; f < nf.nfreq; ++f) {
-    const double2 th = nf.th[f * nf.total_steps + t], te = nf.te[f * nf.total_steps + t];
-    double2* a = nf.acc + static_cast<long long>(f) * 4 * nf.npts + pt;
-    double2 v;
-    v = a[0]; v.x = v.x + sja * th.x; v.y = v.y + sja * th.y; a[0] = v;
-    v = a[nf.npts]; v.x = v.x + sjb * th.x; v.y = v.y + sjb * th.y; a[nf.npts] = v;
-    v = a[2 * nf.npts]; v.x = v.x + sma * te.x; v.y = v.y + sma * te.y; a[2 * nf.npts] = v;
-    v = a[3 * nf.npts]; v.x = v.x + smb * te.x; v.y = v.y + smb * te.y; a[3 * nf.npts] = v;
+  const double smp[4] = {cja * hb, cjb * ha, cma * eb, cmb * ea};  // J_a, J_b, M_a, M_b samples
+  const int slot = static_cast<int>(t % kNfRing);
+  if (slot != kNfRing - 1) {
+    double* r = nf.ring + static_cast<long long>(slot) * 4 * nf.npts + pt;
+#pragma unroll
+    for (int w = 0; w < 4; ++w) r[w * nf.npts] = smp[w];
+    return;
   }
+  nf_advance(nf, pt, max(t - (kNfRing - 1), *nf.done), t, true, smp);
 }
 
 // ---------------------------------------------------------------------------
