@@ -132,6 +132,16 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def workload_label(scene, gi, cells):
+    dims = f"{gi.nx}x{gi.ny}x{gi.nz}"
+    if scene == "dispersive":
+        return (f"dispersive sphere {dims} ({cells}^3 + 12-cell CPML), Drude+Lorentz ADE, TFSF Gaussian, "
+                "NF2FF 1/3/5 GHz (FP64 accumulation)")
+    parts = {"vacuum": "PEC box only", "pml": "12-cell CPML", "tfsf": "12-cell CPML + TFSF Gaussian",
+             "nf2ff": "12-cell CPML + TFSF Gaussian + NF2FF 1/3/5 GHz"}[scene]
+    return f"diagnostic variant of the dispersive-sphere workload, {dims}: {parts}"
+
+
 def build_scene(cells, precision, scene="dispersive"):
     """The benchmark workload, or a reduced variant for kernel diagnostics
     (vacuum: PEC box only; pml: + CPML; tfsf: + CPML + TFSF; nf2ff: + NF2FF)."""
@@ -483,8 +493,7 @@ def main():
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic",
-               "config": {"workload": f"dispersive sphere {gi.nx}x{gi.ny}x{gi.nz} ({args.cells}^3 + 12-cell CPML), "
-                                      "Drude+Lorentz ADE, TFSF Gaussian, NF2FF 1/3/5 GHz (FP64 accumulation)",
+               "config": {"workload": workload_label(args.scene, gi, args.cells),
                           "cells_per_step": cells, "parallelism": f"scene-replica x{world}" if world > 1 else "1 GPU",
                           "l2": "resident state 3.3 GB >> 126 MB L2 (no flush needed)"},
                "e2e": e2e, "roofline": roofline, "step_roofline": step_roof, "cpu_baseline": cpu,
