@@ -310,8 +310,9 @@ constexpr StepTile kStepTiles[2] = {{2, 4}, {2, 8}};
 // z columns, y+z corner columns, anything with ADE next to a slab (all
 // without TFSF code), lean with TFSF corrections, lean interior (the
 // bulk-copy path of single scenes), kinds 1..6 with TFSF corrections for the
-// items that meet the TFSF surface, lean interior with TFSF corrections
-constexpr int kStepKindCount = 16;
+// items that meet the TFSF surface, lean interior with TFSF corrections, and
+// the y- and z-column kinds on the bulk-copy path
+constexpr int kStepKindCount = 18;
 
 // True when a work item over planes [p, q) of the tile at (j0, k0) may meet a
 // TFSF correction: the cells it updates (H at planes p-1 .. q-1, rows j0-1 ..
@@ -385,6 +386,7 @@ inline void build_step_items(const Compiled& c, int TJ, int NT, bool ade_deferre
         if ((kind == 0 || kind == 7) && lean_interior && p >= 1 && j0 >= 1 && k0 >= 1 && j0 + TJ <= ny &&
             k0 + 32 <= nz)
           kind = kind == 0 ? kLeanInterior : kLeanInteriorTf;
+        if (lean_interior && (kind == 3 || kind == 4)) kind = kind == 3 ? kFastY : kFastZ;
         out[kind].push_back(make_int4(bx, by, p, q));
         p = q;
       }
@@ -429,8 +431,9 @@ inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 // (nzp, ny+1, nx+1) over the padded layout, box = one plane's staged window
 // (RW x RH, resp. MW x RH), zero fill outside the extents.  Box origins are
 // k0 - HP (resp. k0 - 16) with k0 a multiple of 32: 16-byte aligned.  The
-// bulk-store maps of the lean interior items cover the same tensors with a
-// box of one tile (32 x TJ), stored at (k0, j0) >= 0 only.
+// bulk-store maps of step_item_fast cover the cells of the same arrays
+// (extents nz, ny, nx: an edge tile's cells outside the grid are clipped)
+// with a box of one tile (32 x TJ), stored at (k0, j0) >= 0 only.
 template <typename T>
 int encode_stage_maps(xfb_handle* h) {
   auto enc = tensor_map_encoder();
@@ -438,6 +441,9 @@ int encode_stage_maps(xfb_handle* h) {
   const Compiled& c = h->c;
   const cuuint64_t dims[3] = {static_cast<cuuint64_t>(h->nzp), static_cast<cuuint64_t>(c.ny + 1),
                               static_cast<cuuint64_t>(c.nx + 1)};
+  // bulk stores write cells only: extents (nz, ny, nx) clip an edge tile
+  const cuuint64_t sdims[3] = {static_cast<cuuint64_t>(c.nz), static_cast<cuuint64_t>(c.ny),
+                               static_cast<cuuint64_t>(c.nx)};
   const cuuint32_t estr[3] = {1, 1, 1};
   const CUtensorMapDataType ft = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
   for (int t = 0; t < 2; ++t) {
@@ -453,7 +459,7 @@ int encode_stage_maps(xfb_handle* h) {
         CUresult r = enc(&h->stage_maps[t][set][q], ft, 3, f[q], dims, fstr, fbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         if (r != CUDA_SUCCESS) return set_err(h, XFB_ERR_CUDA, "cuTensorMapEncodeTiled (field) failed: " + std::to_string(r));
-        r = enc(&h->store_maps[t][set][q], ft, 3, f[q], dims, fstr, sbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+        r = enc(&h->store_maps[t][set][q], ft, 3, f[q], sdims, fstr, sbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         if (r != CUDA_SUCCESS) return set_err(h, XFB_ERR_CUDA, "cuTensorMapEncodeTiled (store) failed: " + std::to_string(r));
       }
@@ -479,7 +485,7 @@ inline int upload_step_items(xfb_handle* h) {
     // and column tile, so CTAs resident together cover neighbouring tiles of
     // the same plane range and the halo rows and columns one CTA stages are
     // the ones its neighbours read moments before (L2 hits)
-    static const int costly[] = {14, 6, 13, 5, 12, 4, 11, 3, 10, 2};
+    static const int costly[] = {14, 6, 13, 5, 12, 4, kFastZ, 11, 3, kFastY, 10, 2};
     std::vector<int4> all, rest;
     for (int q : costly)
       for (int4 v : items[q]) all.push_back(make_int4(v.x | (q << 16), v.y, v.z, v.w));

@@ -720,24 +720,37 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
   }
 }
 
-// Lean interior work item: no CPML, TFSF or ADE cell and no PEC wall within
-// reach, the tile with its halo row and column inside the grid, first plane
-// >= 1.  The arithmetic is step_item's lean kind, term for term; what differs
-// is the data movement.  The H planes live in dense shared tiles (with the
-// halo row j0-1 and halo column k0-1 after them): the E update reads its j-1
-// and k-1 neighbours there at per-thread constant offsets, and the tiles are
-// also the sources of bulk tensor stores.  E^{n+1} goes to dense tiles too.
-// At iteration i one thread issues the stores of H plane i-1 and E plane i-2
-// (both finished before the iteration's barrier) and waits, before the next
-// barrier, until they have read their tiles; so no thread computes a global
-// address or issues a global store.  TF: with the TFSF corrections of the
-// cells on the TFSF surface (tfsf_h / tfsf_e, as in step_item).
-template <typename T, int R, int NWM, int NS_, bool TF>
-__device__ __forceinline__ void step_item_lean(int4 item, const T* lut8, int n_mat, const TfsfP& tf,
-                                               const StageMaps* maps, const StoreMaps* outs, int* err) {
+// Bulk-copy body of a work item: the lean interior items (PK = 0: no CPML or
+// ADE cell and no PEC wall within reach, the tile with its halo row and
+// column inside the grid, first plane >= 1) and the y- or z-slab CPML columns
+// (PK = 3 or 9: x+y or x+z slab kinds, at the grid's edges).  The arithmetic
+// is step_item's (hNext, TFSF, CPML x, y, z corrections; eNext, TFSF, CPML),
+// term for term and in the same order; what differs is the data movement.
+// The H planes live in dense shared tiles (with the halo row j0-1 and halo
+// column k0-1 after them): the E update reads its j-1 and k-1 neighbours
+// there at per-thread constant offsets, and the tiles are also the sources
+// of bulk tensor stores, whose tensor extents (nz, ny, nx) clip an edge
+// tile's cells outside the grid (the k extent only to 16-byte granules, so
+// those cells carry their old values into the tiles: a store that reaches the
+// wall column k = nz writes back what is there).  E^{n+1} goes to dense tiles
+// too, with the PEC walls' components keeping their old value.  At iteration i one
+// thread issues the stores of H plane i-1 and E plane i-2 (both finished
+// before the iteration's barrier) and waits, before the next barrier, until
+// they have read their tiles.  CPML: per-thread psi offsets and y/z profile
+// coefficients are computed once per item; the psi pair of the slab axis of
+// each cell (H of the next plane, E of the current one) is loaded a plane
+// ahead; x-slab psi (planes near the x faces) inline.  TF: with the TFSF
+// corrections of the cells on the TFSF surface.
+template <typename T, int R, int NWM, int NS_, bool TF, int PK>
+__device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>& pm, const PsiH<T>& ps,
+                                               const PsiH<T>& pd, int4 item, const T* lut8, int n_mat,
+                                               const TfsfP& tf, const StageMaps* maps, const StoreMaps* outs,
+                                               int* err) {
   using L = StepCfg<T, R, NWM, NS_>;
   constexpr int NS = L::NS, HP = L::HP, RW = L::RW, MW = L::MW, TJ = L::TJ, PL = L::PL, NT = L::NT, RH = L::RH;
   constexpr int CS = L::LCS, ET = TJ * 32;
+  constexpr bool PX = (PK & 1) != 0, PY = (PK & 2) != 0, PZ = (PK & 8) != 0, PML = PK != 0;
+  static_assert(!(PY && PZ), "one column slab axis per body");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* base = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
   T* sF = reinterpret_cast<T*>(base);                            // [NS][6][PL]
@@ -749,7 +762,7 @@ __device__ __forceinline__ void step_item_lean(int4 item, const T* lut8, int n_m
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int k0 = (item.x & 0xffff) * 32, j0 = item.y * TJ;
-  const int i_start = item.z, i_end = item.w, i_first = i_start - 1;
+  const int i_start = item.z, i_end = item.w, i_first = i_start > 0 ? i_start - 1 : 0;
   const bool lut_shared = n_mat <= L::LUTM;
   if (lut_shared)
     for (int q = tid; q < n_mat * 8; q += NT) sL[q] = lut8[q];
@@ -780,7 +793,7 @@ __device__ __forceinline__ void step_item_lean(int4 item, const T* lut8, int n_m
   // the H tile, km: the k-1 neighbour's slot (row warps).
   const bool row_warp = warp < NWM;
   int wf[R], mo[R], hs[R], km[R];
-  int cj[R], ck[R], tfl[R];  // cell indices and TFSF line flags (TF only)
+  int cj[R], ck[R], tfl[R];  // cell indices, TFSF line flags (TF only)
   bool act[R];
 #pragma unroll
   for (int u = 0; u < R; ++u) {
@@ -812,14 +825,61 @@ __device__ __forceinline__ void step_item_lean(int4 item, const T* lut8, int n_m
   }
   const int jm0 = warp * R > 0 ? (warp * R - 1) * 32 + lane : TJ * 32 + lane;  // j-1 of row u = 0
 
+  // CPML: per cell the slab index of the column axis (-1: outside the slab or
+  // outside the grid), its psi offset inside a plane and its profile
+  // coefficients; the x-slab offset inside a plane; the PEC wall flags
+  int sp[R], so[R], go[R];
+  T cah[R], cbh[R], cae[R], cbe[R];
+  bool in_grid[R];
+#pragma unroll
+  for (int u = 0; u < R; ++u) {
+    const int j = cj[u], k = ck[u];
+    in_grid[u] = act[u] && j >= 0 && k >= 0 && j < s.ny && k < s.nz;
+    go[u] = j * static_cast<int>(s.sy) + k;
+    sp[u] = -1;
+    so[u] = 0;
+    cah[u] = cbh[u] = cae[u] = cbe[u] = T(0);
+    if (PY && in_grid[u]) {
+      sp[u] = slab(j, s.ny, pm.L[2], pm.L[3]);
+      if (sp[u] >= 0) {
+        so[u] = sp[u] * static_cast<int>(s.sy) + k;
+        cah[u] = pm.ah[1][j]; cbh[u] = pm.bh[1][j]; cae[u] = pm.ae[1][j]; cbe[u] = pm.be[1][j];
+      }
+    }
+    if (PZ && in_grid[u]) {
+      sp[u] = slab(k, s.nz, pm.L[4], pm.L[5]);
+      if (sp[u] >= 0) {
+        so[u] = j * static_cast<int>(pm.zsy) + sp[u];
+        cah[u] = pm.ah[2][k]; cbh[u] = pm.bh[2][k]; cae[u] = pm.ae[2][k]; cbe[u] = pm.be[2][k];
+      }
+    }
+  }
+  const long long psx = PY ? pm.ysx : pm.zsx;  // psi plane stride of the column axis
+  // psi arrays of the column axis, in the order the updates read them
+  // (H: y: hz, hx; z: hx, hy; E: y: ez, ex; z: ex, ey)
+  const T* hr0 = PY ? ps.hz_y : ps.hx_z;
+  const T* hr1 = PY ? ps.hx_y : ps.hy_z;
+  T* hw0 = PY ? pd.hz_y : pd.hx_z;
+  T* hw1 = PY ? pd.hx_y : pd.hy_z;
+  T* er0 = PY ? pm.ez_y : pm.ex_z;
+  T* er1 = PY ? pm.ex_y : pm.ey_z;
+
   T hnx[R], hny[R], hnz[R], hpx[R], hpy[R], hpz[R], hqy[R], hqz[R];
   T eox[R], eoy[R], eoz[R], enx[R], eny[R], enz[R];
+  T ph0[R], ph1[R], pe0[R], pe1[R];  // column-axis psi pairs loaded a plane ahead
   int em[R], enm[R];
 #pragma unroll
   for (int u = 0; u < R; ++u) {
     hnx[u] = hny[u] = hnz[u] = hpx[u] = hpy[u] = hpz[u] = hqy[u] = hqz[u] = T(0);
     eox[u] = eoy[u] = eoz[u] = enx[u] = eny[u] = enz[u] = T(0);
+    ph0[u] = ph1[u] = pe0[u] = pe1[u] = T(0);
     em[u] = enm[u] = 0;
+  }
+  if (PML && (PY || PZ)) {
+    const long long pb = static_cast<long long>(i_first) * psx;
+#pragma unroll
+    for (int u = 0; u < R; ++u)
+      if (sp[u] >= 0) { ph0[u] = hr0[pb + so[u]]; ph1[u] = hr1[pb + so[u]]; }
   }
   int slot = i_first % NS;
   int waited = i_first - 1;
@@ -860,7 +920,10 @@ __device__ __forceinline__ void step_item_lean(int4 item, const T* lut8, int n_m
     const T* Hq = sH + ((i + 1) & 1) * 3 * CS;  // H plane i-1
     // ---- H pass, plane i ------------------------------------------------------
     const bool tf_hplane = TF && tf.on && (i == tf.is - 1 || i == tf.ie);
+    const int sxp = PX ? slab(i, s.nx, pm.L[0], pm.L[1]) : -1;
+    const bool own_h = row_warp && i >= i_start;
     if (do_h) {
+      const long long pbh = static_cast<long long>(i) * psx;
 #pragma unroll
       for (int u = 0; u < R; ++u) {
         if (!act[u]) continue;
@@ -878,6 +941,32 @@ __device__ __forceinline__ void step_item_lean(int4 item, const T* lut8, int n_m
         T hyv = cf.c * f[4 * PL] + cf.x * d_hy_a - cf.z * d_hy_b;
         T hzv = cf.c * f[5 * PL] + cf.y * d_hz_a - cf.x * d_hz_b;
         if (TF && (tf_hplane || (tfl[u] & 1))) tfsf_h(tf, i, cj[u], ck[u], hxv, hyv, hzv);
+        if (PX && sxp >= 0 && in_grid[u]) {
+          const long long p = static_cast<long long>(sxp) * s.sx + go[u];
+          const T a = pm.ah[0][i], b = pm.bh[0][i];
+          const T qy = b * ps.hy_x[p] + a * d_hy_a;
+          hyv = hyv + cf.x * qy;   // chyez
+          const T qz = b * ps.hz_x[p] + a * d_hz_b;
+          hzv = hzv - cf.x * qz;   // chzey
+          if (own_h) { pd.hy_x[p] = qy; pd.hz_x[p] = qz; }
+        }
+        if (PY && sp[u] >= 0) {
+          const T qz = cbh[u] * ph0[u] + cah[u] * d_hz_a;
+          hzv = hzv + cf.y * qz;   // chzex
+          const T qx = cbh[u] * ph1[u] + cah[u] * d_hx_b;
+          hxv = hxv - cf.y * qx;   // chxez
+          if (own_h) { hw0[pbh + so[u]] = qz; hw1[pbh + so[u]] = qx; }
+        }
+        if (PZ && sp[u] >= 0) {
+          const T qx = cbh[u] * ph0[u] + cah[u] * d_hx_a;
+          hxv = hxv + cf.z * qx;   // chxey
+          const T qy = cbh[u] * ph1[u] + cah[u] * d_hy_b;
+          hyv = hyv - cf.z * qy;   // chyex
+          if (own_h) { hw0[pbh + so[u]] = qx; hw1[pbh + so[u]] = qy; }
+        }
+        if (PML && !in_grid[u]) {  // outside the grid: the bulk store writes back the old value
+          hxv = f[3 * PL]; hyv = f[4 * PL]; hzv = f[5 * PL];
+        }
         Hc[hs[u]] = hxv;
         Hc[CS + hs[u]] = hyv;
         Hc[2 * CS + hs[u]] = hzv;
@@ -890,6 +979,9 @@ __device__ __forceinline__ void step_item_lean(int4 item, const T* lut8, int n_m
     const bool tf_eplane = TF && tf.on && (ie == tf.is || ie == tf.ie);
     if (row_warp && ie >= i_start) {
       T* Eo = sE + (ie & 1) * 3 * ET;
+      const int sxe = PX ? slab(ie, s.nx, pm.L[0], pm.L[1]) : -1;
+      const long long pbe = static_cast<long long>(ie) * psx;
+      const bool ipos = ie > 0;
 #pragma unroll
       for (int u = 0; u < R; ++u) {
         const C4<T> cf = ld_c4(lut + 8 * em[u]);  // ce, cb/dx, cb/dy, cb/dz
@@ -909,6 +1001,30 @@ __device__ __forceinline__ void step_item_lean(int4 item, const T* lut8, int n_m
         T eyv = cf.c * eoy[u] - cf.x * d_ey_a + cf.z * d_ey_b;
         T ezv = cf.c * eoz[u] - cf.y * d_ez_a + cf.x * d_ez_b;
         if (TF && (tf_eplane || (tfl[u] & 2))) tfsf_e(tf, ie, cj[u], ck[u], exv, eyv, ezv);
+        if (PML) {
+          const bool jpos = cj[u] > 0, kpos = ck[u] > 0;
+          const bool upd_x = jpos && kpos, upd_y = ipos && kpos, upd_z = ipos && jpos;
+          if (PX && sxe >= 0 && in_grid[u]) {
+            const long long p = static_cast<long long>(sxe) * s.sx + go[u];
+            const T a = pm.ae[0][ie], b = pm.be[0][ie];
+            if (upd_y) { T q = b * pm.ey_x[p] + a * d_ey_a; pm.ey_x[p] = q; eyv = eyv - cf.x * q; }  // ceyhz
+            if (upd_z) { T q = b * pm.ez_x[p] + a * d_ez_b; pm.ez_x[p] = q; ezv = ezv + cf.x * q; }  // cezhy
+          }
+          if (PY && sp[u] >= 0) {
+            if (upd_z) { T q = cbe[u] * pe0[u] + cae[u] * d_ez_a; er0[pbe + so[u]] = q; ezv = ezv - cf.y * q; }  // cezhx
+            if (upd_x) { T q = cbe[u] * pe1[u] + cae[u] * d_ex_b; er1[pbe + so[u]] = q; exv = exv + cf.y * q; }  // cexhz
+          }
+          if (PZ && sp[u] >= 0) {
+            if (upd_x) { T q = cbe[u] * pe0[u] + cae[u] * d_ex_a; er0[pbe + so[u]] = q; exv = exv - cf.z * q; }  // cexhy
+            if (upd_y) { T q = cbe[u] * pe1[u] + cae[u] * d_ey_b; er1[pbe + so[u]] = q; eyv = eyv + cf.z * q; }  // ceyhx
+          }
+          // E components on PEC walls keep their value, and so do the cells
+          // of an edge tile outside the grid (a bulk store clips the k extent
+          // only to 16-byte granules, so it may write the wall column k = nz)
+          if (!upd_x || !in_grid[u]) exv = eox[u];
+          if (!upd_y || !in_grid[u]) eyv = eoy[u];
+          if (!upd_z || !in_grid[u]) ezv = eoz[u];
+        }
         Eo[o] = exv;
         Eo[ET + o] = eyv;
         Eo[2 * ET + o] = ezv;
@@ -922,6 +1038,16 @@ __device__ __forceinline__ void step_item_lean(int4 item, const T* lut8, int n_m
         em[u] = enm[u];
         eox[u] = enx[u]; eoy[u] = eny[u]; eoz[u] = enz[u];
       }
+    }
+    // column-axis psi of the next iteration: H of plane i+1, E of plane i
+    if (PML && (PY || PZ)) {
+      const long long pbh = static_cast<long long>(i + 1) * psx, pbe = static_cast<long long>(i) * psx;
+#pragma unroll
+      for (int u = 0; u < R; ++u)
+        if (sp[u] >= 0) {
+          if (i + 1 < i_end) { ph0[u] = hr0[pbh + so[u]]; ph1[u] = hr1[pbh + so[u]]; }
+          if (row_warp && do_h && i >= i_start) { pe0[u] = er0[pbe + so[u]]; pe1[u] = er1[pbe + so[u]]; }
+        }
     }
     fence_proxy_async();             // this thread's tile writes before the next iteration's bulk stores
     if (tid == 0) bulk_wait_read();  // this iteration's stores have read their tiles
@@ -960,19 +1086,23 @@ constexpr int kStepKinds[16] = {0, 1, 4, 3, 9, 11, 15, 16, 0, 1 | 16, 4 | 16, 3 
 // kind indices of the lean interior items (step_item_lean, bulk-copy path
 // only), without and with TFSF corrections
 constexpr int kLeanInterior = 8, kLeanInteriorTf = 15;
+// kind indices of the y- and z-slab CPML columns run by step_item_fast (the
+// bulk-copy path only; without TFSF cells)
+constexpr int kFastY = 16, kFastZ = 17;
 
 template <typename T, int R, int NWM, int NS_, bool TMA>
 __device__ __forceinline__ void step_dispatch(const GridP<T>& s, const GridP<T>& d, const PmlP<T>& pm,
                                               const PsiH<T>& ps, const PsiH<T>& pd, const TfsfP& tf,
                                               const AdeP<T>& ad, int4 item, const T* lut8, const uint8_t* disp,
                                               int n_mat, const StageMaps* maps, const StoreMaps* outs, int* err) {
-  if (TMA && (item.x >> 16) == kLeanInterior) {
-    step_item_lean<T, R, NWM, NS_, false>(item, lut8, n_mat, tf, maps, outs, err);
-    return;
-  }
-  if (TMA && (item.x >> 16) == kLeanInteriorTf) {
-    step_item_lean<T, R, NWM, NS_, true>(item, lut8, n_mat, tf, maps, outs, err);
-    return;
+  if (TMA) {
+    switch (item.x >> 16) {
+      case kLeanInterior: step_item_fast<T, R, NWM, NS_, false, 0>(s, pm, ps, pd, item, lut8, n_mat, tf, maps, outs, err); return;
+      case kLeanInteriorTf: step_item_fast<T, R, NWM, NS_, true, 0>(s, pm, ps, pd, item, lut8, n_mat, tf, maps, outs, err); return;
+      case kFastY: step_item_fast<T, R, NWM, NS_, false, 3>(s, pm, ps, pd, item, lut8, n_mat, tf, maps, outs, err); return;
+      case kFastZ: step_item_fast<T, R, NWM, NS_, false, 9>(s, pm, ps, pd, item, lut8, n_mat, tf, maps, outs, err); return;
+      default: break;
+    }
   }
 #define XFB_ITEM(q) step_item<T, R, NWM, NS_, kStepKinds[q], TMA>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat, maps, err)
   switch (item.x >> 16) {
