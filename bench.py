@@ -132,6 +132,25 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def max_over_ranks(x, dist):
+    """Max of x over all ranks (a time: the job's is the slowest rank's).
+    dist = (torch, torch.distributed) or None; NCCL reduces on the device,
+    gloo on the host."""
+    if not dist:
+        return x
+    torch, tdist = dist
+    dev = "cuda" if tdist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(cells, steps, world, ms):
+    """Whole-job Mcell-updates/s: every rank steps its own copy of `cells`
+    cells `steps` times in `ms` (the slowest rank's time)."""
+    return cells * steps * world / (ms / 1e3) / 1e6
+
+
 def workload_label(scene, gi, cells):
     dims = f"{gi.nx}x{gi.ny}x{gi.nz}"
     if scene == "dispersive":
@@ -357,6 +376,10 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        # host-side CPU run: rank 0 alone works and prints, the others exit at
+        # once; no rank takes a collective step, so no process group is needed
+        return run_reference(args, rank, world)
     dist = None
     if world > 1:
         import datetime
@@ -365,12 +388,6 @@ def main():
         torch.cuda.set_device(local)
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = (torch, tdist)
-
-    if args.impl == "reference":
-        rc = run_reference(args, rank, world)
-        if dist:
-            dist[1].destroy_process_group()
-        return rc
 
     import xfdtd_cuda_b200 as X
     from xfdtd_cuda_b200 import _lib as L
@@ -399,11 +416,8 @@ def main():
     with ClockSampler(local) as clk:
         ms = h.timed_step(args.steps)
     barrier()
-    if dist:
-        t = dist[0].tensor([ms], dtype=dist[0].float64, device="cuda")
-        dist[1].all_reduce(t, op=dist[1].ReduceOp.MAX)
-        ms = float(t.item())
-    value = cells * args.steps * world / (ms / 1e3) / 1e6
+    ms = max_over_ranks(ms, dist)
+    value = job_rate(cells, args.steps, world, ms)
 
     # per-kernel device time (launches bracketed by events, no graph)
     kms, kcnt = h.profile_kernels(args.profile_steps)
@@ -453,11 +467,8 @@ def main():
                     d2h += h2.read_nf2ff(f, face, w).size * 16
         wall = time.perf_counter() - t0
         h2d = cells * 1 + 64 * 1024  # material ids + coefficient/profile tables
-        if dist:
-            t = dist[0].tensor([wall], dtype=dist[0].float64, device="cuda")
-            dist[1].all_reduce(t, op=dist[1].ReduceOp.MAX)
-            wall = float(t.item())
-        e2e = {"value": cells * args.steps * world / wall / 1e6, "unit": UNIT,
+        wall = max_over_ranks(wall, dist)
+        e2e = {"value": job_rate(cells, args.steps, world, wall * 1e3), "unit": UNIT,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                "path": "Handle(scene) + init + step + read-back (SimulationHD.run flow), wall clock"}
         h2.close()

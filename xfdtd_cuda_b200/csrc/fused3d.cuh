@@ -876,10 +876,11 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
     em[u] = enm[u] = 0;
   }
   if (PML && (PY || PZ)) {
-    const long long pb = static_cast<long long>(i_first) * psx;
+    const T* a0 = hr0 + static_cast<long long>(i_first) * psx;
+    const T* a1 = hr1 + static_cast<long long>(i_first) * psx;
 #pragma unroll
     for (int u = 0; u < R; ++u)
-      if (sp[u] >= 0) { ph0[u] = hr0[pb + so[u]]; ph1[u] = hr1[pb + so[u]]; }
+      if (sp[u] >= 0) { ph0[u] = a0[so[u]]; ph1[u] = a1[so[u]]; }
   }
   int slot = i_first % NS;
   int waited = i_first - 1;
@@ -923,7 +924,9 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
     const int sxp = PX ? slab(i, s.nx, pm.L[0], pm.L[1]) : -1;
     const bool own_h = row_warp && i >= i_start;
     if (do_h) {
-      const long long pbh = static_cast<long long>(i) * psx;
+      // psi planes of the column axis at plane i (H written to the other set)
+      T* w0 = hw0 + static_cast<long long>(i) * psx;
+      T* w1 = hw1 + static_cast<long long>(i) * psx;
 #pragma unroll
       for (int u = 0; u < R; ++u) {
         if (!act[u]) continue;
@@ -955,14 +958,14 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
           hzv = hzv + cf.y * qz;   // chzex
           const T qx = cbh[u] * ph1[u] + cah[u] * d_hx_b;
           hxv = hxv - cf.y * qx;   // chxez
-          if (own_h) { hw0[pbh + so[u]] = qz; hw1[pbh + so[u]] = qx; }
+          if (own_h) { w0[so[u]] = qz; w1[so[u]] = qx; }
         }
         if (PZ && sp[u] >= 0) {
           const T qx = cbh[u] * ph0[u] + cah[u] * d_hx_a;
           hxv = hxv + cf.z * qx;   // chxey
           const T qy = cbh[u] * ph1[u] + cah[u] * d_hy_b;
           hyv = hyv - cf.z * qy;   // chyex
-          if (own_h) { hw0[pbh + so[u]] = qx; hw1[pbh + so[u]] = qy; }
+          if (own_h) { w0[so[u]] = qx; w1[so[u]] = qy; }
         }
         if (PML && !in_grid[u]) {  // outside the grid: the bulk store writes back the old value
           hxv = f[3 * PL]; hyv = f[4 * PL]; hzv = f[5 * PL];
@@ -980,7 +983,8 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
     if (row_warp && ie >= i_start) {
       T* Eo = sE + (ie & 1) * 3 * ET;
       const int sxe = PX ? slab(ie, s.nx, pm.L[0], pm.L[1]) : -1;
-      const long long pbe = static_cast<long long>(ie) * psx;
+      T* e0p = er0 + static_cast<long long>(ie) * psx;
+      T* e1p = er1 + static_cast<long long>(ie) * psx;
       const bool ipos = ie > 0;
 #pragma unroll
       for (int u = 0; u < R; ++u) {
@@ -1011,12 +1015,12 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
             if (upd_z) { T q = b * pm.ez_x[p] + a * d_ez_b; pm.ez_x[p] = q; ezv = ezv + cf.x * q; }  // cezhy
           }
           if (PY && sp[u] >= 0) {
-            if (upd_z) { T q = cbe[u] * pe0[u] + cae[u] * d_ez_a; er0[pbe + so[u]] = q; ezv = ezv - cf.y * q; }  // cezhx
-            if (upd_x) { T q = cbe[u] * pe1[u] + cae[u] * d_ex_b; er1[pbe + so[u]] = q; exv = exv + cf.y * q; }  // cexhz
+            if (upd_z) { T q = cbe[u] * pe0[u] + cae[u] * d_ez_a; e0p[so[u]] = q; ezv = ezv - cf.y * q; }  // cezhx
+            if (upd_x) { T q = cbe[u] * pe1[u] + cae[u] * d_ex_b; e1p[so[u]] = q; exv = exv + cf.y * q; }  // cexhz
           }
           if (PZ && sp[u] >= 0) {
-            if (upd_x) { T q = cbe[u] * pe0[u] + cae[u] * d_ex_a; er0[pbe + so[u]] = q; exv = exv - cf.z * q; }  // cexhy
-            if (upd_y) { T q = cbe[u] * pe1[u] + cae[u] * d_ey_b; er1[pbe + so[u]] = q; eyv = eyv + cf.z * q; }  // ceyhx
+            if (upd_x) { T q = cbe[u] * pe0[u] + cae[u] * d_ex_a; e0p[so[u]] = q; exv = exv - cf.z * q; }  // cexhy
+            if (upd_y) { T q = cbe[u] * pe1[u] + cae[u] * d_ey_b; e1p[so[u]] = q; eyv = eyv + cf.z * q; }  // ceyhx
           }
           // E components on PEC walls keep their value, and so do the cells
           // of an edge tile outside the grid (a bulk store clips the k extent
@@ -1041,12 +1045,16 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
     }
     // column-axis psi of the next iteration: H of plane i+1, E of plane i
     if (PML && (PY || PZ)) {
-      const long long pbh = static_cast<long long>(i + 1) * psx, pbe = static_cast<long long>(i) * psx;
+      const T* a0 = hr0 + static_cast<long long>(i + 1) * psx;
+      const T* a1 = hr1 + static_cast<long long>(i + 1) * psx;
+      const T* b0 = er0 + static_cast<long long>(i) * psx;
+      const T* b1 = er1 + static_cast<long long>(i) * psx;
+      const bool nh = i + 1 < i_end, ne = row_warp && do_h && i >= i_start;
 #pragma unroll
       for (int u = 0; u < R; ++u)
         if (sp[u] >= 0) {
-          if (i + 1 < i_end) { ph0[u] = hr0[pbh + so[u]]; ph1[u] = hr1[pbh + so[u]]; }
-          if (row_warp && do_h && i >= i_start) { pe0[u] = er0[pbe + so[u]]; pe1[u] = er1[pbe + so[u]]; }
+          if (nh) { ph0[u] = a0[so[u]]; ph1[u] = a1[so[u]]; }
+          if (ne) { pe0[u] = b0[so[u]]; pe1[u] = b1[so[u]]; }
         }
     }
     fence_proxy_async();             // this thread's tile writes before the next iteration's bulk stores
