@@ -75,7 +75,7 @@ enum xfb_ade_kind { XFB_ADE_NONE = 0, XFB_ADE_DEBYE = 1, XFB_ADE_DRUDE = 2, XFB_
  * separate launches per face (src/include/updator/update_scheme.cuh:132-197,
  * src/boundary/pml_corrector.cu:9-291,
  * src/waveform_source/tfsf/tfsf_corrector.cu:155-271); 3-D scenes without
- * dispersive media only.  AUTO: FUSED in 3-D, SPLIT in 2-D. */
+ * dispersive media only.  AUTO: FUSED (3-D and 2-D TMz). */
 enum xfb_kernel_path { XFB_PATH_AUTO = 0, XFB_PATH_SPLIT = 1, XFB_PATH_FUSED = 2, XFB_PATH_PLAIN = 3 };
 
 #define XFB_MAX_POLES 4

@@ -96,11 +96,13 @@ def test_fp64_ade_bitexact(kind, path, radius):
     check_all(h, o, 3, 2, 0, nf=True)
 
 
-def test_fp64_cylinder_2d_bitexact():
+@pytest.mark.parametrize("path", PATHS)
+def test_fp64_cylinder_2d_bitexact(path):
+    # 2-D TMz: H and E half-step kernels, and the one-sweep 2-D step
     sim = configs.cylinder_2d(cells=96, dl=1e-3, pml=8, precision="fp64", radius=0.012, tfsf_inset=6, n_probes=5)
     sim.addMonitor(X.MovieMonitor(X.FieldMonitor(X.Cube(X.Vector(-0.04, -0.04, -math.inf), X.Vector(0.08, 0.08, math.inf)),
                                                  X.EMF.Field.EZ), 9))
-    h, o = run_pair(sim, 150)
+    h, o = run_pair(sim, 150, path)
     check_all(h, o, 2, 5, 1, nf=False)
 
 

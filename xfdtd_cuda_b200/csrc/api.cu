@@ -114,14 +114,14 @@ int launches_per_step(const xfb_handle* h) {
   if (plain(h)) {
     int faces = 0;
     for (int f = 0; f < 6; ++f) faces += c.pml[f] > 0;
-    return 6 + 2 * faces + (c.tfsf_on ? 1 + 24 : 0) + (c.nf_on ? 1 : 0) + (c.probes.empty() ? 0 : 1) +
+    return 6 + 2 * faces + (c.tfsf_on ? 24 : 0) + (c.nf_on ? 1 : 0) + (c.probes.empty() ? 0 : 1) +
            static_cast<int>(c.movies.size());
   }
   int bulk = 2;
   if (fused(h)) {
-    bulk = (h->n_step_items[step_tile_index(h->tj)] > 0 ? 1 : 0) + (h->ade_deferred ? 1 : 0);
+    bulk = c.dim == 2 ? 1 : (h->n_step_items[step_tile_index(h->tj)] > 0 ? 1 : 0) + (h->ade_deferred ? 1 : 0);
   }
-  return bulk + (c.tfsf_on ? 1 : 0) + (c.nf_on ? 1 : 0) + (c.probes.empty() ? 0 : 1) +
+  return bulk + (c.nf_on ? 1 : 0) + (c.probes.empty() ? 0 : 1) +
          static_cast<int>(c.movies.size());
 }
 
@@ -134,11 +134,11 @@ int batch_err(xfb_batch* b, int code, const std::string& m) {
 void batch_free(xfb_batch* b) {
   for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
   b->graphs.clear();
-  void* ps[5] = {b->scenes, b->aux, b->items[0], b->items[1], b->t_dev};
+  void* ps[4] = {b->scenes, b->items[0], b->items[1], b->t_dev};
   for (void* p : ps) cudaFree(p);
-  b->scenes = b->aux = b->items[0] = b->items[1] = nullptr;
+  b->scenes = b->items[0] = b->items[1] = nullptr;
   b->t_dev = nullptr;
-  b->n_items[0] = b->n_items[1] = b->n_aux = 0;
+  b->n_items[0] = b->n_items[1] = 0;
   b->inited = false;
 }
 
@@ -316,8 +316,7 @@ int xfb_init(xfb_handle* h, long long total_steps) {
   size_tables(h->c, total_steps);
   if (h->path == XFB_PATH_PLAIN && (h->c.dim != 3 || h->c.ade_kind != XFB_ADE_NONE))
     return set_err(h, XFB_ERR_INVALID, "the plain path handles 3-D scenes without dispersive media only");
-  if (h->path == XFB_PATH_AUTO || (h->c.dim == 2 && h->path != XFB_PATH_PLAIN))
-    h->path = h->c.dim == 3 ? XFB_PATH_FUSED : XFB_PATH_SPLIT;
+  if (h->path == XFB_PATH_AUTO) h->path = XFB_PATH_FUSED;
   int rc;
   try {
     rc = h->c.prec == XFB_FP64 ? init_device<double>(h) : init_device<float>(h);

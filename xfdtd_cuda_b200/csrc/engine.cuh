@@ -61,7 +61,7 @@ int init_device(xfb_handle* h) {
   }
   if ((rc = upload<T>(h, &h->lut, c.coeff))) return rc;
   if ((rc = upload<T>(h, &h->lut8, c.coeff8))) return rc;
-  if (fused(h) && (rc = upload_step_items(h))) return rc;
+  if (fused(h) && c.dim == 3 && (rc = upload_step_items(h))) return rc;
   if (fused(h) && c.dim == 3) {
     if ((rc = encode_stage_maps<T>(h))) return rc;
     void* p;
@@ -110,6 +110,10 @@ int init_device(xfb_handle* h) {
     if ((rc = alloc(h, &h->psi[2], by, true))) return rc;   // ez_y
     if ((rc = alloc(h, &h->psi[6], bx, true))) return rc;   // hy_x
     if ((rc = alloc(h, &h->psi[9], by, true))) return rc;   // hx_y
+    if (fused(h)) {  // H-side psi of field set 1 (one-sweep path)
+      if ((rc = alloc(h, &h->psi_h1[0], bx, true))) return rc;
+      if ((rc = alloc(h, &h->psi_h1[3], by, true))) return rc;
+    }
   }
   // TFSF
   if (c.tfsf_on) {
@@ -120,13 +124,18 @@ int init_device(xfb_handle* h) {
       if ((rc = upload<double>(h, &p, c.proj_half[a]))) return rc;
       h->proj[3 + a] = static_cast<double*>(p);
     }
+    // incident-field tables of every step of the run (k_aux_table)
     void* p;
-    if ((rc = alloc(h, &p, 2 * (c.aux_nl + 1) * sizeof(double), true))) return rc;
+    const size_t steps = static_cast<size_t>(c.total_steps);
+    if ((rc = alloc(h, &p, (steps + 1) * (c.aux_nl + 1) * sizeof(double), false))) return rc;
     h->e_aux = static_cast<double*>(p);
-    if ((rc = alloc(h, &p, c.aux_nl * sizeof(double), true))) return rc;
+    if ((rc = alloc(h, &p, std::max<size_t>(1, steps) * c.aux_nl * sizeof(double), false))) return rc;
     h->h_aux = static_cast<double*>(p);
     if ((rc = upload<double>(h, &p, c.aux_source))) return rc;
     h->src = static_cast<double*>(p);
+    k_aux_table<<<1, 1024, 0, h->stream>>>(h->e_aux, h->h_aux, c.aux_nl, c.aux_ceih, c.aux_chie, c.aux_abc, h->src,
+                                            c.total_steps);
+    XFB_CUDA(h, cudaGetLastError());
   }
   // ADE
   if (c.ade_kind != XFB_ADE_NONE) {
@@ -236,7 +245,7 @@ inline TfsfP tfsf_params(xfb_handle* h) {
   t.pi0 = h->proj[0]; t.pi1 = h->proj[1]; t.pi2 = h->proj[2];
   t.ph0 = h->proj[3]; t.ph1 = h->proj[4]; t.ph2 = h->proj[5];
   for (int a = 0; a < 3; ++a) { t.tre[a] = c.tr_e[a]; t.trh[a] = c.tr_h[a]; t.ca[a] = c.ca[a]; t.cb[a] = c.cb[a]; }
-  t.e_aux0 = h->e_aux; t.e_aux1 = h->e_aux + (c.aux_nl + 1); t.h_aux = h->h_aux; t.e_aux = nullptr;
+  t.e_tab = h->e_aux; t.h_tab = h->h_aux; t.nl = c.aux_nl; t.e_aux = nullptr; t.h_aux = nullptr;
   return t;
 }
 
@@ -688,11 +697,6 @@ void enqueue_step(xfb_handle* h, int off, Prof* pf = nullptr) {
     if (c.tfsf_on) plain_tfsf<T>(h, g, tp, 1);
     plain_pml<T, false>(h, g);
     prof_end(h, pf);
-    if (c.tfsf_on) {
-      prof_begin(h, pf, XFB_K_AUX);
-      k_aux<<<1, 1024, 0, s>>>(h->e_aux, h->e_aux + (c.aux_nl + 1), h->h_aux, c.aux_nl, c.aux_ceih, c.aux_chie, c.aux_abc, h->src, tp);
-      prof_end(h, pf);
-    }
     prof_begin(h, pf, XFB_K_UPDATE_E);
     plain_update<T, true>(h, g);
     prof_end(h, pf);
@@ -701,14 +705,18 @@ void enqueue_step(xfb_handle* h, int off, Prof* pf = nullptr) {
     plain_pml<T, true>(h, g);
     prof_end(h, pf);
   } else if (fused(h)) {
-    if (c.tfsf_on) {
-      prof_begin(h, pf, XFB_K_AUX);
-      k_aux<<<1, 1024, 0, s>>>(h->e_aux, h->e_aux + (c.aux_nl + 1), h->h_aux, c.aux_nl, c.aux_ceih, c.aux_chie,
-                               c.aux_abc, h->src, tp);
-      prof_end(h, pf);
-    }
     prof_begin(h, pf, XFB_K_STEP);
-    launch_fused<T>(h, parity, tp, s);
+    if (c.dim == 2) {
+      // one-sweep 2-D step: 128-column blocks over plane chunks
+      const int gx = (c.ny + 127) / 128;
+      const int nch = chunks_for(gx, c.nx, 160);
+      const int ich = (c.nx + nch - 1) / nch;
+      k_step2<T><<<dim3(gx, (c.nx + ich - 1) / ich), 160, 0, s>>>(
+          grid_params<T>(h, parity), grid_params<T>(h, 1 - parity), pml_params<T>(h), psi_h_set<T>(h, parity),
+          psi_h_set<T>(h, 1 - parity), tfsf_params(h), tp, ich);
+    } else {
+      launch_fused<T>(h, parity, tp, s);
+    }
     if (h->ade_deferred) {
       const int* b = c.ade_box;
       dim3 grd((b[5] - b[4] + 127) / 128, b[3] - b[2], b[1] - b[0]);
@@ -731,11 +739,6 @@ void enqueue_step(xfb_handle* h, int off, Prof* pf = nullptr) {
     prof_begin(h, pf, XFB_K_UPDATE_H);
     k_h3<T><<<grd, blk, 0, s>>>(g, pm, tf, tp, ich);
     prof_end(h, pf);
-    if (c.tfsf_on) {
-      prof_begin(h, pf, XFB_K_AUX);
-      k_aux<<<1, 1024, 0, s>>>(h->e_aux, h->e_aux + (c.aux_nl + 1), h->h_aux, c.aux_nl, c.aux_ceih, c.aux_chie, c.aux_abc, h->src, tp);
-      prof_end(h, pf);
-    }
     prof_begin(h, pf, XFB_K_UPDATE_E);
     k_e3<T><<<grd, blk, 0, s>>>(g, pm, tf, ade_params<T>(h), tp, ich);
     prof_end(h, pf);
@@ -748,11 +751,6 @@ void enqueue_step(xfb_handle* h, int off, Prof* pf = nullptr) {
     prof_begin(h, pf, XFB_K_UPDATE_H);
     k_h2<T><<<grd, bx, 0, s>>>(g, pm, tf, tp, ich);
     prof_end(h, pf);
-    if (c.tfsf_on) {
-      prof_begin(h, pf, XFB_K_AUX);
-      k_aux<<<1, 1024, 0, s>>>(h->e_aux, h->e_aux + (c.aux_nl + 1), h->h_aux, c.aux_nl, c.aux_ceih, c.aux_chie, c.aux_abc, h->src, tp);
-      prof_end(h, pf);
-    }
     prof_begin(h, pf, XFB_K_UPDATE_E);
     k_e2<T><<<grd, bx, 0, s>>>(g, pm, tf, tp, ich);
     prof_end(h, pf);
@@ -897,18 +895,9 @@ inline int batch_upload(xfb_batch* b, void** dst, const void* src, size_t bytes)
 template <typename T>
 int batch_init(xfb_batch* b) {
   std::vector<BatchScene<T>> sc;
-  std::vector<AuxScene> aux;
-  for (xfb_handle* h : b->hs) {
-    sc.push_back(batch_scene<T>(h));
-    const Compiled& c = h->c;
-    if (c.tfsf_on)
-      aux.push_back(AuxScene{h->e_aux, h->e_aux + (c.aux_nl + 1), h->h_aux, h->src, c.aux_ceih, c.aux_chie, c.aux_abc,
-                             c.aux_nl});
-  }
+  for (xfb_handle* h : b->hs) sc.push_back(batch_scene<T>(h));
   int rc;
   if ((rc = batch_upload(b, &b->scenes, sc.data(), sc.size() * sizeof(BatchScene<T>)))) return rc;
-  b->n_aux = static_cast<int>(aux.size());
-  if (b->n_aux && (rc = batch_upload(b, &b->aux, aux.data(), aux.size() * sizeof(AuxScene)))) return rc;
   for (int t = 0; t < 2; ++t) {
     const int TJ = kStepTiles[t].r * kStepTiles[t].nwm, NT = (kStepTiles[t].nwm + 1) * 32;
     long long columns = 0;
@@ -953,13 +942,13 @@ void batch_step3(xfb_batch* b, int t, TimeP tp, int parity) {
       static_cast<const BatchScene<T>*>(b->scenes), static_cast<const int4*>(b->items[t]), tp, parity);
 }
 
-// One step of every scene: TFSF auxiliary grids, the one-sweep kernel over
-// all work items, deferred ADE passes, monitors.
+// One step of every scene: the one-sweep kernel over all work items,
+// deferred ADE passes, monitors (the TFSF incident tables were computed when
+// each handle was initialised).
 template <typename T>
 void batch_enqueue_step(xfb_batch* b, int off, int t) {
   TimeP tp{b->t_dev, off};
   const int parity = static_cast<int>((b->step + off) & 1);
-  if (b->n_aux) k_aux_batch<<<b->n_aux, 1024, 0, b->stream>>>(static_cast<const AuxScene*>(b->aux), tp);
   if (b->n_items[t]) {
     if (t == 0) batch_step3<T, kStepTiles[0].r, kStepTiles[0].nwm>(b, 0, tp, parity);
     else batch_step3<T, kStepTiles[1].r, kStepTiles[1].nwm>(b, 1, tp, parity);

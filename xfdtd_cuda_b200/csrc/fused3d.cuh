@@ -121,6 +121,114 @@ struct PsiH {  // H-side CPML psi of one buffer set
   T* hy_x; T* hz_x; T* hz_y; T* hx_y; T* hx_z; T* hy_z;
 };
 
+// One-sweep 2-D TMz step: the H and E half-steps of a Yee step in one
+// launch (the TFSF incident fields come from the precomputed tables).  A block owns 128
+// columns j0 .. j0+127 over a chunk of planes [i0, i1) and marches along i;
+// thread t holds column j0 - 1 + t, thread 0 the halo column whose Hx the
+// first column's Ez update needs, so no block reads what another writes in
+// the same launch: fields and H-side psi are ping-pong buffered (read s / ps,
+// write d / pd; the E-side psi has one owner per cell).  At plane i a thread
+// computes H of plane i (Hx from Ez(i, j+1) - Ez(i, j), Hy from Ez(i+1, j) -
+// Ez(i, j), both from the read set) and then Ez of plane i from Hy(i) -
+// Hy(i-1) (its own registers) and Hx(i, j) - Hx(i, j-1) (its left
+// neighbour's, through shared memory): one barrier per plane.  The march
+// starts a plane early (i0 - 1) for Hy(i0 - 1).  PEC wall entries (i = 0 or
+// j = 0 for Ez) are never written, so both sets keep their value.  The
+// arithmetic and its order are those of k_h2 and k_e2.
+template <typename T>
+__global__ void __launch_bounds__(160) k_step2(GridP<T> s, GridP<T> d, PmlP<T> pm, PsiH<T> ps, PsiH<T> pd,
+                                               TfsfP tf_in, TimeP tp, int i_chunk) {
+  const TfsfP tf = tfsf_at_step(tf_in, cur_step(tp));
+  __shared__ T hxs[2][160];
+  const int t = threadIdx.x;
+  const int j = blockIdx.x * 128 + t - 1;
+  const int i0 = blockIdx.y * i_chunk;
+  const int i1 = min(s.nx, i0 + i_chunk);
+  if (i0 >= i1) return;  // the whole block
+  const bool hcol = t <= 128 && j >= 0 && j < s.ny;  // H of this column is computed
+  const bool own = hcol && t >= 1;                    // and written, with its Ez
+  const long long sx = s.sx;
+  const int sy_pml = hcol ? slab(j, s.ny, pm.L[2], pm.L[3]) : -1;
+  T hy_prev = T(0);
+  for (int i = i0 > 0 ? i0 - 1 : 0; i < i1; ++i) {
+    const long long idx = static_cast<long long>(i) * sx + j;
+    const bool in_range = i >= i0;
+    T hxv = T(0), hyv = T(0);
+    const T* c = nullptr;
+    if (hcol) {
+      const T ez_c = s.ez[idx];
+      const T ez_n = s.ez[idx + sx];
+      const T ez_j1 = s.ez[idx + 1];
+      c = s.lut + 18 * static_cast<int>(s.mid[idx]);
+      const T d_hx_b = ez_j1 - ez_c;  // Hx from Ez along y
+      const T d_hy_a = ez_n - ez_c;   // Hy from Ez along x
+      hxv = c[9] * s.hx[idx] + c[11] * d_hx_b;
+      hyv = c[12] * s.hy[idx] + c[13] * d_hy_a;
+      if (tf.on) {
+        if (j >= tf.js && j <= tf.je) {
+          if (i == tf.is - 1) add_inc(hyv, ez_inc(tf, tf.is, j, 0), -tf.cb[0]);
+          if (i == tf.ie) add_inc(hyv, ez_inc(tf, tf.ie, j, 0), tf.cb[0]);
+        }
+        if (i >= tf.is && i <= tf.ie) {
+          if (j == tf.js - 1) add_inc(hxv, ez_inc(tf, i, tf.js, 0), tf.cb[1]);
+          if (j == tf.je) add_inc(hxv, ez_inc(tf, i, tf.je, 0), -tf.cb[1]);
+        }
+      }
+      const int sx_pml = slab(i, s.nx, pm.L[0], pm.L[1]);
+      if (sx_pml >= 0) {
+        const long long p = sx_pml * sx + j;
+        T py = pm.bh[0][i] * ps.hy_x[p] + pm.ah[0][i] * d_hy_a;
+        if (own && in_range) pd.hy_x[p] = py;
+        hyv = hyv + c[13] * py;
+      }
+      if (sy_pml >= 0) {
+        const long long p = static_cast<long long>(i) * pm.ysx + sy_pml;
+        T px = pm.bh[1][j] * ps.hx_y[p] + pm.ah[1][j] * d_hx_b;
+        if (own && in_range) pd.hx_y[p] = px;
+        hxv = hxv + c[11] * px;
+      }
+      if (own && in_range) {
+        d.hx[idx] = hxv;
+        d.hy[idx] = hyv;
+      }
+    }
+    hxs[i & 1][t] = hxv;
+    __syncthreads();
+    if (own && in_range && i > 0 && j > 0) {
+      const T hx_c = hxv, hx_jm = hxs[i & 1][t - 1];
+      const T hy_c = hyv, hy_p = hy_prev;
+      const T d_ez_a = hx_c - hx_jm;
+      const T d_ez_b = hy_c - hy_p;
+      T ezv = c[6] * s.ez[idx] + c[7] * d_ez_a + c[8] * d_ez_b;
+      if (tf.on) {
+        if (j >= tf.js && j <= tf.je) {
+          if (i == tf.is) add_inc(ezv, hy_inc(tf, tf.is - 1, j, 0), -tf.ca[0]);
+          if (i == tf.ie) add_inc(ezv, hy_inc(tf, tf.ie, j, 0), tf.ca[0]);
+        }
+        if (i >= tf.is && i <= tf.ie) {
+          if (j == tf.js) add_inc(ezv, hx_inc(tf, i, tf.js - 1, 0), tf.ca[1]);
+          if (j == tf.je) add_inc(ezv, hx_inc(tf, i, tf.je, 0), -tf.ca[1]);
+        }
+      }
+      const int sx_pml = slab(i, s.nx, pm.L[0], pm.L[1]);
+      if (sx_pml >= 0) {
+        const long long p = sx_pml * sx + j;
+        T q = pm.be[0][i] * pm.ez_x[p] + pm.ae[0][i] * d_ez_b;
+        pm.ez_x[p] = q;
+        ezv = ezv + c[8] * q;
+      }
+      if (sy_pml >= 0) {
+        const long long p = static_cast<long long>(i) * pm.ysx + sy_pml;
+        T q = pm.be[1][j] * pm.ez_y[p] + pm.ae[1][j] * d_ez_a;
+        pm.ez_y[p] = q;
+        ezv = ezv + c[7] * q;
+      }
+      d.ez[idx] = ezv;
+    }
+    hy_prev = hyv;
+  }
+}
+
 // Four coefficients of one half of the compact LUT (E: ce, cb/dx, cb/dy, cb/dz;
 // H: ch, db/dx, db/dy, db/dz), read from shared memory with vector loads.
 template <typename T>
@@ -1177,7 +1285,7 @@ __global__ void __launch_bounds__(StepCfg<T, R, NWM, NS_>::NT, StepCfg<T, R, NWM
     for (int q = threadIdx.x; q < static_cast<int>(sizeof(BatchScene<T>) / 4); q += blockDim.x) dst[q] = src[q];
   }
   __syncthreads();
-  if (threadIdx.x == 0) sp.tf.e_aux = (cur_step(tp) & 1) ? sp.tf.e_aux1 : sp.tf.e_aux0;  // E_inc of this step
+  if (threadIdx.x == 0) sp.tf = tfsf_at_step(sp.tf, cur_step(tp));  // incident-table rows of this step
   __syncthreads();
   const int4 item = make_int4((it.x & 0xfff) | (((it.x >> 12) & 0xf) << 16), it.y, it.z, it.w);
   step_dispatch<T, R, NWM, NS_, false>(sp.g[parity], sp.g[1 - parity], sp.pm, sp.psh[parity], sp.psh[1 - parity],

@@ -52,8 +52,8 @@ struct xfb_handle {
   long long ysx = 0, zsx = 0, zsy = 0;
   // TFSF
   double* proj[6] = {};
-  double* e_aux = nullptr;   // [2][nl+1] by step parity
-  double* h_aux = nullptr;
+  double* e_aux = nullptr;   // [total_steps + 1][nl + 1] incident E of every step
+  double* h_aux = nullptr;   // [total_steps][nl] incident H of every half step
   double* src = nullptr;
   // ADE
   void* ade_mat = nullptr;
@@ -117,8 +117,6 @@ struct xfb_batch {
   int tile = -1;      // tile configuration in use (-1 until chosen)
   int graph_steps = 64;
   void* scenes = nullptr;   // BatchScene<T>[n]
-  void* aux = nullptr;      // AuxScene[n_aux]
-  int n_aux = 0;
   void* items[2] = {};      // per tile configuration
   int n_items[2] = {};
   long long* t_dev = nullptr;

@@ -6,8 +6,9 @@
 //          basic_updator.cuh:16-32; TFSFCorrector3DAgency::correctH,
 //          src/waveform_source/tfsf/tfsf_corrector.cu:237-271; PMLCorrector<xyz>::
 //          correctH, src/boundary/pml_corrector.cu:180-270)
-//   k_aux  TFSF 1-D auxiliary grid, one step, FP64 (the reference precomputes it on
-//          the host inside XFDTD_CORE)
+//   (TFSF 1-D auxiliary grid: k_aux_table computes the incident E/H of every
+//          step once at set-up, in FP64, as the reference's host set-up inside
+//          XFDTD_CORE precomputes its incident tables)
 //   k_e3   E half-step: Yee / ADE update + TFSF E correction + CPML psi
 //          (BasicUpdator3D::updateE, src/updator/basic_updator/basic_updator_3d.cu:10-34;
 //          TemplateADEUpdateScheme::updateE, src/include/updator/ade_updator/
@@ -55,15 +56,17 @@ struct TfsfP {
   const double* pi0; const double* pi1; const double* pi2;  // projections at nodes
   const double* ph0; const double* ph1; const double* ph2;  // projections at half nodes
   double tre[3], trh[3], ca[3], cb[3];
-  double* e_aux0;  // [nl+1] E incident at t*dt for even t (double buffer by step parity)
-  double* e_aux1;  // [nl+1] ... for odd t
-  double* h_aux;   // [nl]   H incident at (t+1/2)*dt (valid after k_aux of step t)
-  const double* e_aux;  // resolved by tfsf_at_step: E buffer of the current step
+  const double* e_tab;  // [total_steps + 1][nl + 1]: row t = E incident at t*dt
+  const double* h_tab;  // [total_steps][nl]: row t = H incident at (t+1/2)*dt
+  int nl;
+  const double* e_aux;  // resolved by tfsf_at_step: the rows of the current step
+  const double* h_aux;
 };
 
-// Resolve the auxiliary E buffer that holds E_inc at time t*dt.
+// Resolve the rows of the auxiliary-grid tables of step t.
 __device__ __forceinline__ TfsfP tfsf_at_step(TfsfP s, long long t) {
-  s.e_aux = (t & 1) ? s.e_aux1 : s.e_aux0;
+  s.e_aux = s.e_tab + t * (s.nl + 1);
+  s.h_aux = s.h_tab + t * s.nl;
   return s;
 }
 
@@ -362,7 +365,8 @@ __global__ void k_ade_box(GridP<T> s, GridP<T> d, AdeP<T> ad, const uint8_t* dis
 // E half-step, 3-D.  Same tiling as k_h3; H values of plane i are carried to
 // plane i+1 as its i-1 neighbours.
 template <typename T>
-__global__ void k_e3(GridP<T> g, PmlP<T> pm, TfsfP tf, AdeP<T> ad, TimeP tp, int i_chunk) {
+__global__ void k_e3(GridP<T> g, PmlP<T> pm, TfsfP tf_in, AdeP<T> ad, TimeP tp, int i_chunk) {
+  const TfsfP tf = tfsf_at_step(tf_in, cur_step(tp));
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (k >= g.nz || j >= g.ny) return;
@@ -543,7 +547,8 @@ __global__ void k_h2(GridP<T> g, PmlP<T> pm, TfsfP tf_in, TimeP tp, int i_chunk)
 }
 
 template <typename T>
-__global__ void k_e2(GridP<T> g, PmlP<T> pm, TfsfP tf, TimeP tp, int i_chunk) {
+__global__ void k_e2(GridP<T> g, PmlP<T> pm, TfsfP tf_in, TimeP tp, int i_chunk) {
+  const TfsfP tf = tfsf_at_step(tf_in, cur_step(tp));
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= g.ny) return;
   const int i0 = blockIdx.y * i_chunk;
@@ -591,39 +596,27 @@ __global__ void k_e2(GridP<T> g, PmlP<T> pm, TfsfP tf, TimeP tp, int i_chunk) {
 }
 
 // ---------------------------------------------------------------------------
-// TFSF 1-D auxiliary grid, one time step (single block).  Before: e = E^t,
-// h = H^{t-1/2}; after: h = H^{t+1/2}, e = E^{t+1} with the source at node 0
-// and a first-order Mur boundary at node nl.
-// E^t lives in e_buf[t & 1]; E^{t+1} is written to the other buffer so the
-// bulk kernels of step t can still read E^t after this kernel ran.
-__device__ __forceinline__ void aux_step(double* e0, double* e1, double* h, int nl, double ceih, double chie,
-                                         double abc, const double* src, long long t) {
-  const double* e = (t & 1) ? e1 : e0;
-  double* en = (t & 1) ? e0 : e1;
-  for (int l = threadIdx.x; l < nl; l += blockDim.x) h[l] = h[l] + chie * (e[l + 1] - e[l]);
-  __syncthreads();
-  for (int l = threadIdx.x + 1; l < nl; l += blockDim.x) en[l] = e[l] + ceih * (h[l] - h[l - 1]);
-  if (threadIdx.x == 0) en[0] = src[t + 1];
-  __syncthreads();
-  if (threadIdx.x == 0) en[nl] = e[nl - 1] + abc * (en[nl - 1] - e[nl]);
-}
-
-static __global__ void k_aux(double* e0, double* e1, double* h, int nl, double ceih, double chie, double abc,
-                             const double* src, TimeP tp) {
-  aux_step(e0, e1, h, nl, ceih, chie, abc, src, cur_step(tp));
-}
-
-// TFSF auxiliary grids of a batch of scenes, one CTA per scene.
-struct AuxScene {
-  double* e0; double* e1; double* h;
-  const double* src;
-  double ceih, chie, abc;
-  int nl;
-};
-
-static __global__ void k_aux_batch(const AuxScene* a, TimeP tp) {
-  const AuxScene& s = a[blockIdx.x];
-  aux_step(s.e0, s.e1, s.h, s.nl, s.ceih, s.chie, s.abc, s.src, cur_step(tp));
+// TFSF 1-D auxiliary grid: its whole history, computed once when the run is
+// set up (the grid depends on the source only, not on the 3-D fields), so no
+// time step waits on it.  Row t of e_tab holds E^t, row t of h_tab H^{t+1/2};
+// step t: h = h_prev + chie (e[l+1] - e[l]), then E^{t+1} with the source at
+// node 0 and a first-order Mur boundary at node nl.  One block walks the
+// steps (one barrier per half-step); e_tab row 0 is zero.
+static __global__ void k_aux_table(double* e_tab, double* h_tab, int nl, double ceih, double chie, double abc,
+                                   const double* src, long long steps) {
+  for (long long t = 0; t < steps; ++t) {
+    const double* e = e_tab + t * (nl + 1);
+    const double* hp = t > 0 ? h_tab + (t - 1) * nl : nullptr;
+    double* h = h_tab + t * nl;
+    double* en = e_tab + (t + 1) * (nl + 1);
+    for (int l = threadIdx.x; l < nl; l += blockDim.x) h[l] = (hp ? hp[l] : 0.0) + chie * (e[l + 1] - e[l]);
+    __syncthreads();
+    for (int l = threadIdx.x + 1; l < nl; l += blockDim.x) en[l] = e[l] + ceih * (h[l] - h[l - 1]);
+    if (threadIdx.x == 0) en[0] = src[t + 1];
+    __syncthreads();
+    if (threadIdx.x == 0) en[nl] = e[nl - 1] + abc * (en[nl - 1] - e[nl]);
+    __syncthreads();
+  }
 }
 
 static __global__ void k_bump(long long* t, int n) { *t += n; }
