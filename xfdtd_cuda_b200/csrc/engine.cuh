@@ -711,9 +711,9 @@ void enqueue_step(xfb_handle* h, int off, Prof* pf = nullptr) {
       const int gx = (c.ny + 127) / 128;
       const int nch = chunks_for(gx, c.nx, 160);
       const int ich = (c.nx + nch - 1) / nch;
-      k_step2<T><<<dim3(gx, (c.nx + ich - 1) / ich), 160, 0, s>>>(
+      k_step2<T><<<dim3(gx, (c.nx + ich - 1) / ich), 160, static_cast<size_t>(c.n_mat) * 18 * sizeof(T), s>>>(
           grid_params<T>(h, parity), grid_params<T>(h, 1 - parity), pml_params<T>(h), psi_h_set<T>(h, parity),
-          psi_h_set<T>(h, 1 - parity), tfsf_params(h), tp, ich);
+          psi_h_set<T>(h, 1 - parity), tfsf_params(h), tp, ich, h->c.n_mat);
     } else {
       launch_fused<T>(h, parity, tp, s);
     }

@@ -137,80 +137,104 @@ struct PsiH {  // H-side CPML psi of one buffer set
 // arithmetic and its order are those of k_h2 and k_e2.
 template <typename T>
 __global__ void __launch_bounds__(160) k_step2(GridP<T> s, GridP<T> d, PmlP<T> pm, PsiH<T> ps, PsiH<T> pd,
-                                               TfsfP tf_in, TimeP tp, int i_chunk) {
+                                               TfsfP tf_in, TimeP tp, int i_chunk, int n_mat) {
   const TfsfP tf = tfsf_at_step(tf_in, cur_step(tp));
   __shared__ T hxs[2][160];
+  extern __shared__ __align__(16) unsigned char k2_smem[];
+  T* lut = reinterpret_cast<T*>(k2_smem);  // [n_mat][18] coefficients
   const int t = threadIdx.x;
   const int j = blockIdx.x * 128 + t - 1;
   const int i0 = blockIdx.y * i_chunk;
   const int i1 = min(s.nx, i0 + i_chunk);
   if (i0 >= i1) return;  // the whole block
+  for (int q = t; q < n_mat * 18; q += blockDim.x) lut[q] = s.lut[q];
   const bool hcol = t <= 128 && j >= 0 && j < s.ny;  // H of this column is computed
   const bool own = hcol && t >= 1;                    // and written, with its Ez
   const long long sx = s.sx;
   const int sy_pml = hcol ? slab(j, s.ny, pm.L[2], pm.L[3]) : -1;
+  // TFSF lines through this column (the plane tests are made once per plane)
+  const bool tf_jin = tf.on && j >= tf.js && j <= tf.je;
+  const bool tf_hline = tf.on && (j == tf.js - 1 || j == tf.je);  // Hx corrections
+  const bool tf_eline = tf.on && (j == tf.js || j == tf.je);      // Ez corrections
+  const int ib = i0 > 0 ? i0 - 1 : 0;
+  // plane i's inputs, loaded one iteration ahead: Ez(i, j), Ez(i+1, j),
+  // Ez(i, j+1), Hx(i, j), Hy(i, j), material id
+  T ez_c = T(0), ez_n = T(0), ez_j1 = T(0), hx_o = T(0), hy_o = T(0);
+  int m = 0;
+  if (hcol) {
+    const long long x0 = static_cast<long long>(ib) * sx + j;
+    ez_c = s.ez[x0]; ez_n = s.ez[x0 + sx]; ez_j1 = s.ez[x0 + 1]; hx_o = s.hx[x0]; hy_o = s.hy[x0];
+    m = s.mid[x0];
+  }
+  __syncthreads();  // shared LUT ready
   T hy_prev = T(0);
-  for (int i = i0 > 0 ? i0 - 1 : 0; i < i1; ++i) {
+  for (int i = ib; i < i1; ++i) {
     const long long idx = static_cast<long long>(i) * sx + j;
     const bool in_range = i >= i0;
+    const bool wr = own && in_range;
+    T nez_n = T(0), nez_j1 = T(0), nhx = T(0), nhy = T(0);
+    int nm = 0;
+    if (hcol && i + 1 < i1) {  // plane i+1
+      const long long x1 = idx + sx;
+      nez_n = s.ez[x1 + sx]; nez_j1 = s.ez[x1 + 1]; nhx = s.hx[x1]; nhy = s.hy[x1];
+      nm = s.mid[x1];
+    }
+    const int sx_pml = slab(i, s.nx, pm.L[0], pm.L[1]);  // plane-uniform
+    const bool tf_iin = tf.on && i >= tf.is && i <= tf.ie;
+    const bool tf_hplane = tf.on && (i == tf.is - 1 || i == tf.ie);
+    const bool tf_eplane = tf.on && (i == tf.is || i == tf.ie);
     T hxv = T(0), hyv = T(0);
-    const T* c = nullptr;
+    const T* c = lut + 18 * m;
     if (hcol) {
-      const T ez_c = s.ez[idx];
-      const T ez_n = s.ez[idx + sx];
-      const T ez_j1 = s.ez[idx + 1];
-      c = s.lut + 18 * static_cast<int>(s.mid[idx]);
       const T d_hx_b = ez_j1 - ez_c;  // Hx from Ez along y
       const T d_hy_a = ez_n - ez_c;   // Hy from Ez along x
-      hxv = c[9] * s.hx[idx] + c[11] * d_hx_b;
-      hyv = c[12] * s.hy[idx] + c[13] * d_hy_a;
-      if (tf.on) {
-        if (j >= tf.js && j <= tf.je) {
+      hxv = c[9] * hx_o + c[11] * d_hx_b;
+      hyv = c[12] * hy_o + c[13] * d_hy_a;
+      if ((tf_hplane && tf_jin) || (tf_hline && tf_iin)) {
+        if (tf_jin) {
           if (i == tf.is - 1) add_inc(hyv, ez_inc(tf, tf.is, j, 0), -tf.cb[0]);
           if (i == tf.ie) add_inc(hyv, ez_inc(tf, tf.ie, j, 0), tf.cb[0]);
         }
-        if (i >= tf.is && i <= tf.ie) {
+        if (tf_iin) {
           if (j == tf.js - 1) add_inc(hxv, ez_inc(tf, i, tf.js, 0), tf.cb[1]);
           if (j == tf.je) add_inc(hxv, ez_inc(tf, i, tf.je, 0), -tf.cb[1]);
         }
       }
-      const int sx_pml = slab(i, s.nx, pm.L[0], pm.L[1]);
       if (sx_pml >= 0) {
         const long long p = sx_pml * sx + j;
         T py = pm.bh[0][i] * ps.hy_x[p] + pm.ah[0][i] * d_hy_a;
-        if (own && in_range) pd.hy_x[p] = py;
+        if (wr) pd.hy_x[p] = py;
         hyv = hyv + c[13] * py;
       }
       if (sy_pml >= 0) {
         const long long p = static_cast<long long>(i) * pm.ysx + sy_pml;
         T px = pm.bh[1][j] * ps.hx_y[p] + pm.ah[1][j] * d_hx_b;
-        if (own && in_range) pd.hx_y[p] = px;
+        if (wr) pd.hx_y[p] = px;
         hxv = hxv + c[11] * px;
       }
-      if (own && in_range) {
+      if (wr) {
         d.hx[idx] = hxv;
         d.hy[idx] = hyv;
       }
     }
     hxs[i & 1][t] = hxv;
     __syncthreads();
-    if (own && in_range && i > 0 && j > 0) {
+    if (wr && i > 0 && j > 0) {
       const T hx_c = hxv, hx_jm = hxs[i & 1][t - 1];
       const T hy_c = hyv, hy_p = hy_prev;
       const T d_ez_a = hx_c - hx_jm;
       const T d_ez_b = hy_c - hy_p;
-      T ezv = c[6] * s.ez[idx] + c[7] * d_ez_a + c[8] * d_ez_b;
-      if (tf.on) {
-        if (j >= tf.js && j <= tf.je) {
+      T ezv = c[6] * ez_c + c[7] * d_ez_a + c[8] * d_ez_b;
+      if ((tf_eplane && tf_jin) || (tf_eline && tf_iin)) {
+        if (tf_jin) {
           if (i == tf.is) add_inc(ezv, hy_inc(tf, tf.is - 1, j, 0), -tf.ca[0]);
           if (i == tf.ie) add_inc(ezv, hy_inc(tf, tf.ie, j, 0), tf.ca[0]);
         }
-        if (i >= tf.is && i <= tf.ie) {
+        if (tf_iin) {
           if (j == tf.js) add_inc(ezv, hx_inc(tf, i, tf.js - 1, 0), tf.ca[1]);
           if (j == tf.je) add_inc(ezv, hx_inc(tf, i, tf.je, 0), -tf.ca[1]);
         }
       }
-      const int sx_pml = slab(i, s.nx, pm.L[0], pm.L[1]);
       if (sx_pml >= 0) {
         const long long p = sx_pml * sx + j;
         T q = pm.be[0][i] * pm.ez_x[p] + pm.ae[0][i] * d_ez_b;
@@ -226,6 +250,7 @@ __global__ void __launch_bounds__(160) k_step2(GridP<T> s, GridP<T> d, PmlP<T> p
       d.ez[idx] = ezv;
     }
     hy_prev = hyv;
+    ez_c = ez_n; ez_n = nez_n; ez_j1 = nez_j1; hx_o = nhx; hy_o = nhy; m = nm;
   }
 }
 
