@@ -2,9 +2,10 @@
 same state as the same scene stepped alone, with CPML, TFSF, ADE (deferred
 box pass), probes and NF2FF — bit for bit in FP64 (both follow the
 reference's operation order with no contraction); in FP32 within 1e-5
-relative, since a single scene runs the bulk-copy bodies of the step kernel
-and a batch the general one, which the compiler contracts into FMAs
-differently; and an FP64 batch agrees with the CPU restatement bit for bit."""
+relative, since a batch cuts its scenes into different work items (whole
+tile columns) than a single scene does, so some cells run another body of the
+step kernel, which the compiler contracts into FMAs differently; and an FP64
+batch agrees with the CPU restatement bit for bit."""
 import numpy as np
 import pytest
 

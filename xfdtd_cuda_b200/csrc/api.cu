@@ -134,10 +134,11 @@ int batch_err(xfb_batch* b, int code, const std::string& m) {
 void batch_free(xfb_batch* b) {
   for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
   b->graphs.clear();
-  void* ps[4] = {b->scenes, b->items[0], b->items[1], b->t_dev};
+  void* ps[6] = {b->scenes, b->maps, b->items[0], b->items[1], b->t_dev, b->err_dev};
   for (void* p : ps) cudaFree(p);
-  b->scenes = b->items[0] = b->items[1] = nullptr;
+  b->scenes = b->maps = b->items[0] = b->items[1] = nullptr;
   b->t_dev = nullptr;
+  b->err_dev = nullptr;
   b->n_items[0] = b->n_items[1] = 0;
   b->inited = false;
 }
@@ -827,6 +828,12 @@ int xfb_batch_sync(xfb_batch* b) {
   cudaError_t e = cudaStreamSynchronize(b->stream);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) return batch_err(b, XFB_ERR_CUDA, cudaGetErrorString(e));
+  if (b->err_dev) {
+    int flag = 0;
+    e = cudaMemcpy(&flag, b->err_dev, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return batch_err(b, XFB_ERR_CUDA, cudaGetErrorString(e));
+    if (flag) return batch_err(b, XFB_ERR_CUDA, "batch step: a staging copy did not complete (wait limit reached)");
+  }
   return XFB_OK;
 }
 

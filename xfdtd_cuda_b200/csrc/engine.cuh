@@ -888,16 +888,34 @@ inline int batch_upload(xfb_batch* b, void** dst, const void* src, size_t bytes)
   return XFB_OK;
 }
 
-// Device tables of an initialised batch: scene parameters, TFSF auxiliary
-// grids, and for both tile configurations one work list over all scenes
+// Device tables of an initialised batch: scene parameters, the scenes'
+// tensor maps, and for both tile configurations one work list over all scenes
 // (costliest region kinds first; whole columns per item when the batch has
 // enough columns to fill the GPU several times over).
 template <typename T>
 int batch_init(xfb_batch* b) {
+  for (xfb_handle* h : b->hs)  // work items pack the k tile into 11 bits
+    if ((h->c.nz + 31) / 32 > 2048) return batch_err(b, XFB_ERR_INVALID, "a batched scene has more than 65536 cells along z");
   std::vector<BatchScene<T>> sc;
-  for (xfb_handle* h : b->hs) sc.push_back(batch_scene<T>(h));
+  std::vector<BatchMaps> mp(b->hs.size());
+  for (size_t q = 0; q < b->hs.size(); ++q) {
+    xfb_handle* h = b->hs[q];
+    sc.push_back(batch_scene<T>(h));
+    for (int t = 0; t < 2; ++t)
+      for (int set = 0; set < 2; ++set) {
+        std::memcpy(mp[q].stage[t][set].f, h->stage_maps[t][set], sizeof(mp[q].stage[t][set].f));
+        mp[q].stage[t][set].mid = h->stage_maps[t][set][6];
+        std::memcpy(mp[q].store[t][set].f, h->store_maps[t][set], sizeof(mp[q].store[t][set].f));
+      }
+  }
   int rc;
   if ((rc = batch_upload(b, &b->scenes, sc.data(), sc.size() * sizeof(BatchScene<T>)))) return rc;
+  if ((rc = batch_upload(b, &b->maps, mp.data(), mp.size() * sizeof(BatchMaps)))) return rc;
+  {
+    cudaError_t e = cudaMalloc(&b->err_dev, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->err_dev, 0, sizeof(int), b->stream);
+    if (e != cudaSuccess) return batch_err(b, XFB_ERR_CUDA, cudaGetErrorString(e));
+  }
   for (int t = 0; t < 2; ++t) {
     const int TJ = kStepTiles[t].r * kStepTiles[t].nwm, NT = (kStepTiles[t].nwm + 1) * 32;
     long long columns = 0;
@@ -907,9 +925,9 @@ int batch_init(xfb_batch* b) {
     for (size_t q = 0; q < b->hs.size(); ++q) {
       const xfb_handle* h = b->hs[q];
       std::vector<int4> items[kStepKindCount];
-      build_step_items(h->c, TJ, NT, h->ade_deferred, items, whole ? h->c.nx : 0);
+      build_step_items(h->c, TJ, NT, h->ade_deferred, items, whole ? h->c.nx : 0, true);
       for (int k = 0; k < kStepKindCount; ++k)
-        for (int4 v : items[k]) per_kind[k].push_back(make_int4(v.x | (k << 12) | (static_cast<int>(q) << 16), v.y, v.z, v.w));
+        for (int4 v : items[k]) per_kind[k].push_back(make_int4(v.x | (k << 11) | (static_cast<int>(q) << 16), v.y, v.z, v.w));
     }
     std::vector<int4> all;
     for (int k = kStepKindCount - 1; k >= 0; --k) {
@@ -939,7 +957,8 @@ void batch_step3(xfb_batch* b, int t, TimeP tp, int parity) {
     attr_set[b->device & 63] = true;
   }
   k_step3_batch<T, R, NWM, NS><<<b->n_items[t], S::NT, S::bytes, b->stream>>>(
-      static_cast<const BatchScene<T>*>(b->scenes), static_cast<const int4*>(b->items[t]), tp, parity);
+      static_cast<const BatchScene<T>*>(b->scenes), static_cast<const BatchMaps*>(b->maps),
+      static_cast<const int4*>(b->items[t]), tp, parity, t, b->err_dev);
 }
 
 // One step of every scene: the one-sweep kernel over all work items,

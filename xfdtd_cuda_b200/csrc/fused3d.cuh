@@ -1294,27 +1294,40 @@ struct BatchScene {
   int pad;
 };
 
+// Tensor maps of one scene of a batch, in global memory: staging maps per tile
+// configuration and read set, bulk-store maps per tile configuration and
+// write set.
+struct BatchMaps {
+  StageMaps stage[2][2];
+  StoreMaps store[2][2];
+};
+
 // The one-sweep step of a batch of scenes in one launch: one CTA per work
-// item (x: k tile | kind << 12 | scene << 16, y: j tile, z/w: plane range).
+// item (x: k tile | kind << 11 | scene << 16, y: j tile, z/w: plane range).
 // The CTA copies its scene's parameters into shared memory and runs the same
-// region-specialised body as k_step3, so every scene's result is identical
-// to stepping it alone.
+// region-specialised bodies as k_step3 (bulk copies through the scene's
+// tensor maps in `maps`, tile configuration `tile`); a staging wait that runs
+// out sets *err.
 template <typename T, int R, int NWM, int NS_>
 __global__ void __launch_bounds__(StepCfg<T, R, NWM, NS_>::NT, StepCfg<T, R, NWM, NS_>::min_blocks)
-    k_step3_batch(const BatchScene<T>* scenes, const int4* items, TimeP tp, int parity) {
+    k_step3_batch(const BatchScene<T>* scenes, const BatchMaps* maps, const int4* items, TimeP tp, int parity,
+                  int tile, int* err) {
   __shared__ BatchScene<T> sp;
   const int4 it = items[blockIdx.x];
+  const int scene = static_cast<int>(static_cast<unsigned>(it.x) >> 16);
   {
-    const int* src = reinterpret_cast<const int*>(scenes + (it.x >> 16));
+    const int* src = reinterpret_cast<const int*>(scenes + scene);
     int* dst = reinterpret_cast<int*>(&sp);
     for (int q = threadIdx.x; q < static_cast<int>(sizeof(BatchScene<T>) / 4); q += blockDim.x) dst[q] = src[q];
   }
   __syncthreads();
   if (threadIdx.x == 0) sp.tf = tfsf_at_step(sp.tf, cur_step(tp));  // incident-table rows of this step
   __syncthreads();
-  const int4 item = make_int4((it.x & 0xfff) | (((it.x >> 12) & 0xf) << 16), it.y, it.z, it.w);
-  step_dispatch<T, R, NWM, NS_, false>(sp.g[parity], sp.g[1 - parity], sp.pm, sp.psh[parity], sp.psh[1 - parity],
-                                       sp.tf, sp.ad, item, sp.lut8, sp.disp, sp.n_mat, nullptr, nullptr, nullptr);
+  const int4 item = make_int4((it.x & 0x7ff) | (((it.x >> 11) & 0x1f) << 16), it.y, it.z, it.w);
+  const BatchMaps& bm = maps[scene];
+  step_dispatch<T, R, NWM, NS_, true>(sp.g[parity], sp.g[1 - parity], sp.pm, sp.psh[parity], sp.psh[1 - parity],
+                                      sp.tf, sp.ad, item, sp.lut8, sp.disp, sp.n_mat, &bm.stage[tile][parity],
+                                      &bm.store[tile][1 - parity], err);
 }
 
 }  // namespace xfb

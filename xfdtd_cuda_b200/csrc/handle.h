@@ -117,6 +117,8 @@ struct xfb_batch {
   int tile = -1;      // tile configuration in use (-1 until chosen)
   int graph_steps = 64;
   void* scenes = nullptr;   // BatchScene<T>[n]
+  void* maps = nullptr;     // BatchMaps[n]: tensor maps of every scene
+  int* err_dev = nullptr;   // 1: a staging wait of the step kernel ran out
   void* items[2] = {};      // per tile configuration
   int n_items[2] = {};
   long long* t_dev = nullptr;
