@@ -308,7 +308,13 @@ struct StepCfg {
   static constexpr size_t off_h = (off_b + 8 * NS + 127) / 128 * 128;
   static constexpr size_t off_e = off_h + (hr_bytes + 127) / 128 * 128;
   static constexpr size_t off_l = off_e + le_bytes, off_d = off_l + l_bytes;
-  static constexpr size_t bytes = off_d + d_bytes + 128;  // + alignment slack of the base
+  // CPML profile coefficients (ah, bh, ae, be) of the tile's rows or columns
+  // with their halo, for the CPML column bodies of step_item_fast
+  static constexpr int NC = 40;
+  static constexpr size_t off_c = (off_d + d_bytes + 15) / 16 * 16;
+  static constexpr size_t c_bytes = 4 * NC * sizeof(T);
+  static constexpr size_t bytes = off_c + c_bytes + 128;  // + alignment slack of the base
+  static_assert(NC >= RH && NC >= TK + 1, "coefficient table covers the tile with its halo");
   // bytes one staged plane brings (six field boxes and the material box)
   static constexpr unsigned tx_bytes = static_cast<unsigned>(6 * RH * RW * sizeof(T) + RH * MW);
   static_assert((RH * MW) % 128 == 0, "material planes stay 128-byte aligned");
@@ -892,6 +898,7 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
   T* sH = reinterpret_cast<T*>(base + L::off_h);                 // [2][3][CS]
   T* sE = reinterpret_cast<T*>(base + L::off_e);                 // [2][3][TJ * 32]
   T* sL = reinterpret_cast<T*>(base + L::off_l);                 // [LUTM][8]
+  T* sC = reinterpret_cast<T*>(base + L::off_c);                 // [4][NC] CPML coefficients
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int k0 = (item.x & 0xffff) * 32, j0 = item.y * TJ;
@@ -900,6 +907,15 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
   if (lut_shared)
     for (int q = tid; q < n_mat * 8; q += NT) sL[q] = lut8[q];
   const T* lut = lut_shared ? sL : lut8;
+  if ((PY || PZ) && tid < L::NC) {  // profile coefficients of the tile's rows / columns
+    const int q = PY ? j0 - 1 + tid : k0 - 1 + tid;
+    const int n = PY ? s.ny : s.nz, ax = PY ? 1 : 2;
+    const bool in = q >= 0 && q < n && slab(q, n, pm.L[2 * ax], pm.L[2 * ax + 1]) >= 0;
+    sC[tid] = in ? pm.ah[ax][q] : T(0);
+    sC[L::NC + tid] = in ? pm.bh[ax][q] : T(0);
+    sC[2 * L::NC + tid] = in ? pm.ae[ax][q] : T(0);
+    sC[3 * L::NC + tid] = in ? pm.be[ax][q] : T(0);
+  }
   if (tid == 0) {
     for (int q = 0; q < NS; ++q) mbar_init(bar + q, 1);
     fence_mbar_init();
@@ -962,7 +978,9 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
   // outside the grid), its psi offset inside a plane and its profile
   // coefficients; the x-slab offset inside a plane; the PEC wall flags
   int sp[R], so[R], go[R];
-  T cah[R], cbh[R], cae[R], cbe[R];
+  // (the coefficients themselves sit in the shared table sC at index ci,
+  // filled before the first barrier of the item)
+  int ci[R];
   bool in_grid[R];
 #pragma unroll
   for (int u = 0; u < R; ++u) {
@@ -971,22 +989,20 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
     go[u] = j * static_cast<int>(s.sy) + k;
     sp[u] = -1;
     so[u] = 0;
-    cah[u] = cbh[u] = cae[u] = cbe[u] = T(0);
+    ci[u] = PY ? j - j0 + 1 : k - k0 + 1;
     if (PY && in_grid[u]) {
       sp[u] = slab(j, s.ny, pm.L[2], pm.L[3]);
-      if (sp[u] >= 0) {
-        so[u] = sp[u] * static_cast<int>(s.sy) + k;
-        cah[u] = pm.ah[1][j]; cbh[u] = pm.bh[1][j]; cae[u] = pm.ae[1][j]; cbe[u] = pm.be[1][j];
-      }
+      if (sp[u] >= 0) so[u] = sp[u] * static_cast<int>(s.sy) + k;
     }
     if (PZ && in_grid[u]) {
       sp[u] = slab(k, s.nz, pm.L[4], pm.L[5]);
-      if (sp[u] >= 0) {
-        so[u] = j * static_cast<int>(pm.zsy) + sp[u];
-        cah[u] = pm.ah[2][k]; cbh[u] = pm.bh[2][k]; cae[u] = pm.ae[2][k]; cbe[u] = pm.be[2][k];
-      }
+      if (sp[u] >= 0) so[u] = j * static_cast<int>(pm.zsy) + sp[u];
     }
   }
+  const T* cah = sC;
+  const T* cbh = sC + L::NC;
+  const T* cae = sC + 2 * L::NC;
+  const T* cbe = sC + 3 * L::NC;
   const long long psx = PY ? pm.ysx : pm.zsx;  // psi plane stride of the column axis
   // psi arrays of the column axis, in the order the updates read them
   // (H: y: hz, hx; z: hx, hy; E: y: ez, ex; z: ex, ey)
@@ -1087,16 +1103,16 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
           if (own_h) { pd.hy_x[p] = qy; pd.hz_x[p] = qz; }
         }
         if (PY && sp[u] >= 0) {
-          const T qz = cbh[u] * ph0[u] + cah[u] * d_hz_a;
+          const T qz = cbh[ci[u]] * ph0[u] + cah[ci[u]] * d_hz_a;
           hzv = hzv + cf.y * qz;   // chzex
-          const T qx = cbh[u] * ph1[u] + cah[u] * d_hx_b;
+          const T qx = cbh[ci[u]] * ph1[u] + cah[ci[u]] * d_hx_b;
           hxv = hxv - cf.y * qx;   // chxez
           if (own_h) { w0[so[u]] = qz; w1[so[u]] = qx; }
         }
         if (PZ && sp[u] >= 0) {
-          const T qx = cbh[u] * ph0[u] + cah[u] * d_hx_a;
+          const T qx = cbh[ci[u]] * ph0[u] + cah[ci[u]] * d_hx_a;
           hxv = hxv + cf.z * qx;   // chxey
-          const T qy = cbh[u] * ph1[u] + cah[u] * d_hy_b;
+          const T qy = cbh[ci[u]] * ph1[u] + cah[ci[u]] * d_hy_b;
           hyv = hyv - cf.z * qy;   // chyex
           if (own_h) { w0[so[u]] = qx; w1[so[u]] = qy; }
         }
@@ -1148,12 +1164,12 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
             if (upd_z) { T q = b * pm.ez_x[p] + a * d_ez_b; pm.ez_x[p] = q; ezv = ezv + cf.x * q; }  // cezhy
           }
           if (PY && sp[u] >= 0) {
-            if (upd_z) { T q = cbe[u] * pe0[u] + cae[u] * d_ez_a; e0p[so[u]] = q; ezv = ezv - cf.y * q; }  // cezhx
-            if (upd_x) { T q = cbe[u] * pe1[u] + cae[u] * d_ex_b; e1p[so[u]] = q; exv = exv + cf.y * q; }  // cexhz
+            if (upd_z) { T q = cbe[ci[u]] * pe0[u] + cae[ci[u]] * d_ez_a; e0p[so[u]] = q; ezv = ezv - cf.y * q; }  // cezhx
+            if (upd_x) { T q = cbe[ci[u]] * pe1[u] + cae[ci[u]] * d_ex_b; e1p[so[u]] = q; exv = exv + cf.y * q; }  // cexhz
           }
           if (PZ && sp[u] >= 0) {
-            if (upd_x) { T q = cbe[u] * pe0[u] + cae[u] * d_ex_a; e0p[so[u]] = q; exv = exv - cf.z * q; }  // cexhy
-            if (upd_y) { T q = cbe[u] * pe1[u] + cae[u] * d_ey_b; e1p[so[u]] = q; eyv = eyv + cf.z * q; }  // ceyhx
+            if (upd_x) { T q = cbe[ci[u]] * pe0[u] + cae[ci[u]] * d_ex_a; e0p[so[u]] = q; exv = exv - cf.z * q; }  // cexhy
+            if (upd_y) { T q = cbe[ci[u]] * pe1[u] + cae[ci[u]] * d_ey_b; e1p[so[u]] = q; eyv = eyv + cf.z * q; }  // ceyhx
           }
           // E components on PEC walls keep their value, and so do the cells
           // of an edge tile outside the grid (a bulk store clips the k extent
