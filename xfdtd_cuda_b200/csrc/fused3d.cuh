@@ -312,7 +312,7 @@ struct StepCfg {
   // with their halo, for the CPML column bodies of step_item_fast
   static constexpr int NC = 40;
   static constexpr size_t off_c = (off_d + d_bytes + 15) / 16 * 16;
-  static constexpr size_t c_bytes = 4 * NC * sizeof(T);
+  static constexpr size_t c_bytes = 8 * NC * sizeof(T);  // column axis, and z of a corner tile
   static constexpr size_t bytes = off_c + c_bytes + 128;  // + alignment slack of the base
   static_assert(NC >= RH && NC >= TK + 1, "coefficient table covers the tile with its halo");
   // bytes one staged plane brings (six field boxes and the material box)
@@ -889,7 +889,9 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
   constexpr int NS = L::NS, HP = L::HP, RW = L::RW, MW = L::MW, TJ = L::TJ, PL = L::PL, NT = L::NT, RH = L::RH;
   constexpr int CS = L::LCS, ET = TJ * 32;
   constexpr bool PX = (PK & 1) != 0, PY = (PK & 2) != 0, PZ = (PK & 8) != 0, PML = PK != 0;
-  static_assert(!(PY && PZ), "one column slab axis per body");
+  // column axis whose psi pair is loaded a plane ahead (y when both are
+  // present), and z as a second column axis (corner columns, loaded inline)
+  constexpr bool CY = PY, CZ = PZ && !PY, Z2 = PY && PZ;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* base = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
   T* sF = reinterpret_cast<T*>(base);                            // [NS][6][PL]
@@ -898,7 +900,7 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
   T* sH = reinterpret_cast<T*>(base + L::off_h);                 // [2][3][CS]
   T* sE = reinterpret_cast<T*>(base + L::off_e);                 // [2][3][TJ * 32]
   T* sL = reinterpret_cast<T*>(base + L::off_l);                 // [LUTM][8]
-  T* sC = reinterpret_cast<T*>(base + L::off_c);                 // [4][NC] CPML coefficients
+  T* sC = reinterpret_cast<T*>(base + L::off_c);                 // [2][4][NC] CPML coefficients
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int k0 = (item.x & 0xffff) * 32, j0 = item.y * TJ;
@@ -915,6 +917,15 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
     sC[L::NC + tid] = in ? pm.bh[ax][q] : T(0);
     sC[2 * L::NC + tid] = in ? pm.ae[ax][q] : T(0);
     sC[3 * L::NC + tid] = in ? pm.be[ax][q] : T(0);
+    if (Z2) {  // the z columns of a corner tile
+      const int qk = k0 - 1 + tid;
+      const bool inz = qk >= 0 && qk < s.nz && slab(qk, s.nz, pm.L[4], pm.L[5]) >= 0;
+      T* z = sC + 4 * L::NC;
+      z[tid] = inz ? pm.ah[2][qk] : T(0);
+      z[L::NC + tid] = inz ? pm.bh[2][qk] : T(0);
+      z[2 * L::NC + tid] = inz ? pm.ae[2][qk] : T(0);
+      z[3 * L::NC + tid] = inz ? pm.be[2][qk] : T(0);
+    }
   }
   if (tid == 0) {
     for (int q = 0; q < NS; ++q) mbar_init(bar + q, 1);
@@ -981,6 +992,7 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
   // (the coefficients themselves sit in the shared table sC at index ci,
   // filled before the first barrier of the item)
   int ci[R];
+  int spz[R], soz[R], ciz[R];  // second column axis (z of a corner tile)
   bool in_grid[R];
 #pragma unroll
   for (int u = 0; u < R; ++u) {
@@ -990,19 +1002,30 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
     sp[u] = -1;
     so[u] = 0;
     ci[u] = PY ? j - j0 + 1 : k - k0 + 1;
+    spz[u] = -1;
+    soz[u] = 0;
+    ciz[u] = k - k0 + 1;
     if (PY && in_grid[u]) {
       sp[u] = slab(j, s.ny, pm.L[2], pm.L[3]);
       if (sp[u] >= 0) so[u] = sp[u] * static_cast<int>(s.sy) + k;
     }
-    if (PZ && in_grid[u]) {
+    if (CZ && in_grid[u]) {
       sp[u] = slab(k, s.nz, pm.L[4], pm.L[5]);
       if (sp[u] >= 0) so[u] = j * static_cast<int>(pm.zsy) + sp[u];
+    }
+    if (Z2 && in_grid[u]) {
+      spz[u] = slab(k, s.nz, pm.L[4], pm.L[5]);
+      if (spz[u] >= 0) soz[u] = j * static_cast<int>(pm.zsy) + spz[u];
     }
   }
   const T* cah = sC;
   const T* cbh = sC + L::NC;
   const T* cae = sC + 2 * L::NC;
   const T* cbe = sC + 3 * L::NC;
+  const T* zah = sC + 4 * L::NC;  // z coefficients of a corner tile
+  const T* zbh = sC + 5 * L::NC;
+  const T* zae = sC + 6 * L::NC;
+  const T* zbe = sC + 7 * L::NC;
   const long long psx = PY ? pm.ysx : pm.zsx;  // psi plane stride of the column axis
   // psi arrays of the column axis, in the order the updates read them
   // (H: y: hz, hx; z: hx, hy; E: y: ez, ex; z: ex, ey)
@@ -1109,12 +1132,20 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
           hxv = hxv - cf.y * qx;   // chxez
           if (own_h) { w0[so[u]] = qz; w1[so[u]] = qx; }
         }
-        if (PZ && sp[u] >= 0) {
+        if (CZ && sp[u] >= 0) {
           const T qx = cbh[ci[u]] * ph0[u] + cah[ci[u]] * d_hx_a;
           hxv = hxv + cf.z * qx;   // chxey
           const T qy = cbh[ci[u]] * ph1[u] + cah[ci[u]] * d_hy_b;
           hyv = hyv - cf.z * qy;   // chyex
           if (own_h) { w0[so[u]] = qx; w1[so[u]] = qy; }
+        }
+        if (Z2 && spz[u] >= 0) {
+          const long long p = static_cast<long long>(i) * pm.zsx + soz[u];
+          const T qx = zbh[ciz[u]] * ps.hx_z[p] + zah[ciz[u]] * d_hx_a;
+          hxv = hxv + cf.z * qx;   // chxey
+          const T qy = zbh[ciz[u]] * ps.hy_z[p] + zah[ciz[u]] * d_hy_b;
+          hyv = hyv - cf.z * qy;   // chyex
+          if (own_h) { pd.hx_z[p] = qx; pd.hy_z[p] = qy; }
         }
         if (PML && !in_grid[u]) {  // outside the grid: the bulk store writes back the old value
           hxv = f[3 * PL]; hyv = f[4 * PL]; hzv = f[5 * PL];
@@ -1167,9 +1198,14 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
             if (upd_z) { T q = cbe[ci[u]] * pe0[u] + cae[ci[u]] * d_ez_a; e0p[so[u]] = q; ezv = ezv - cf.y * q; }  // cezhx
             if (upd_x) { T q = cbe[ci[u]] * pe1[u] + cae[ci[u]] * d_ex_b; e1p[so[u]] = q; exv = exv + cf.y * q; }  // cexhz
           }
-          if (PZ && sp[u] >= 0) {
+          if (CZ && sp[u] >= 0) {
             if (upd_x) { T q = cbe[ci[u]] * pe0[u] + cae[ci[u]] * d_ex_a; e0p[so[u]] = q; exv = exv - cf.z * q; }  // cexhy
             if (upd_y) { T q = cbe[ci[u]] * pe1[u] + cae[ci[u]] * d_ey_b; e1p[so[u]] = q; eyv = eyv + cf.z * q; }  // ceyhx
+          }
+          if (Z2 && spz[u] >= 0) {
+            const long long p = static_cast<long long>(ie) * pm.zsx + soz[u];
+            if (upd_x) { T q = zbe[ciz[u]] * pm.ex_z[p] + zae[ciz[u]] * d_ex_a; pm.ex_z[p] = q; exv = exv - cf.z * q; }  // cexhy
+            if (upd_y) { T q = zbe[ciz[u]] * pm.ey_z[p] + zae[ciz[u]] * d_ey_b; pm.ey_z[p] = q; eyv = eyv + cf.z * q; }  // ceyhx
           }
           // E components on PEC walls keep their value, and so do the cells
           // of an edge tile outside the grid (a bulk store clips the k extent
@@ -1246,6 +1282,8 @@ constexpr int kLeanInterior = 8, kLeanInteriorTf = 15;
 // kind indices of the y- and z-slab CPML columns run by step_item_fast (the
 // bulk-copy path only; without TFSF cells)
 constexpr int kFastY = 16, kFastZ = 17;
+// ... and of the y+z corner columns
+constexpr int kFastYZ = 18;
 
 template <typename T, int R, int NWM, int NS_, bool TMA>
 __device__ __forceinline__ void step_dispatch(const GridP<T>& s, const GridP<T>& d, const PmlP<T>& pm,
@@ -1258,6 +1296,7 @@ __device__ __forceinline__ void step_dispatch(const GridP<T>& s, const GridP<T>&
       case kLeanInteriorTf: step_item_fast<T, R, NWM, NS_, true, 0>(s, pm, ps, pd, item, lut8, n_mat, tf, maps, outs, err); return;
       case kFastY: step_item_fast<T, R, NWM, NS_, false, 3>(s, pm, ps, pd, item, lut8, n_mat, tf, maps, outs, err); return;
       case kFastZ: step_item_fast<T, R, NWM, NS_, false, 9>(s, pm, ps, pd, item, lut8, n_mat, tf, maps, outs, err); return;
+      case kFastYZ: step_item_fast<T, R, NWM, NS_, false, 11>(s, pm, ps, pd, item, lut8, n_mat, tf, maps, outs, err); return;
       default: break;
     }
   }
