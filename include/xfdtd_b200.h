@@ -329,7 +329,7 @@ int xfb_labc_wall_cells(const xfb_handle* h, long long* cells);
 typedef struct xfb_batch xfb_batch;
 /* Group n created handles (same precision, 3-D, one device). */
 int xfb_batch_create(xfb_handle* const* handles, int n, xfb_batch** out);
-/* Tile rows of the one-sweep kernel: 0 = autotune on the first steps (default), 8 or 16. */
+/* Tile rows of the one-sweep kernel: 0 = autotune on the first steps (default), 8, 14 or 16. */
 int xfb_batch_set_tile(xfb_batch* b, int rows);
 /* xfb_init every scene for total_steps steps (one-sweep path) and build the batch's work list. */
 int xfb_batch_init(xfb_batch* b, long long total_steps);

@@ -38,7 +38,7 @@ def _handle(sim, n, path=2):
 
 
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])
-@pytest.mark.parametrize("tile", [0, 8, 16])
+@pytest.mark.parametrize("tile", [0, 8, 14, 16])
 def test_batch_matches_scenes_stepped_alone(precision, tile):
     n = 45
     sims = _scenes(precision)
@@ -55,7 +55,7 @@ def test_batch_matches_scenes_stepped_alone(precision, tile):
     b.step(n - 7)
     b.sync()
     info = b.info()
-    assert info["tile_rows"] in (8, 16) and info["work_items"] > 0
+    assert info["tile_rows"] in (8, 14, 16) and info["work_items"] > 0
     for h, a in zip(hs, alone):
         if precision == "fp64":
             assert bit_equal(fields_of(h, 3), fields_of(a, 3))

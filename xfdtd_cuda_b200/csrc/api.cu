@@ -134,12 +134,15 @@ int batch_err(xfb_batch* b, int code, const std::string& m) {
 void batch_free(xfb_batch* b) {
   for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
   b->graphs.clear();
-  void* ps[6] = {b->scenes, b->maps, b->items[0], b->items[1], b->t_dev, b->err_dev};
+  void* ps[7] = {b->scenes, b->maps, b->items[0], b->items[1], b->items[2], b->t_dev, b->err_dev};
   for (void* p : ps) cudaFree(p);
-  b->scenes = b->maps = b->items[0] = b->items[1] = nullptr;
+  b->scenes = b->maps = nullptr;
+  for (int t = 0; t < kStepTileCount; ++t) {
+    b->items[t] = nullptr;
+    b->n_items[t] = 0;
+  }
   b->t_dev = nullptr;
   b->err_dev = nullptr;
-  b->n_items[0] = b->n_items[1] = 0;
   b->inited = false;
 }
 
@@ -761,7 +764,8 @@ int xfb_batch_create(xfb_handle* const* handles, int n, xfb_batch** out) {
 
 int xfb_batch_set_tile(xfb_batch* b, int rows) {
   if (!b) return set_err(nullptr, XFB_ERR_INVALID, "null batch");
-  if (rows != 0 && rows != 8 && rows != 16) return batch_err(b, XFB_ERR_INVALID, "tile rows must be 0 (autotune), 8 or 16");
+  if (rows != 0 && rows != 8 && rows != 14 && rows != 16)
+    return batch_err(b, XFB_ERR_INVALID, "tile rows must be 0 (autotune), 8, 14 or 16");
   b->tile_req = rows;
   b->tile = -1;
   return XFB_OK;

@@ -311,9 +311,11 @@ PsiH<T> psi_h_set(xfb_handle* h, int set) {
 }
 
 // Tile configurations of the one-sweep kernel: rows per thread R, row warps
-// NWM (tile rows TJ = R * NWM), picked by the launch hint's row count.
+// NWM (tile rows TJ = R * NWM).  A single scene picks 8 or 16 rows by the
+// launch hint's row count; a batch also tries 14 rows (an 8-warp CTA, whose
+// register budget at two CTAs per SM is 128 instead of 96).
 struct StepTile { int r, nwm; };
-constexpr StepTile kStepTiles[2] = {{2, 4}, {2, 8}};
+constexpr StepTile kStepTiles[kStepTileCount] = {{2, 4}, {2, 8}, {2, 7}};
 // region kinds (kStepKinds, bits: 1 x-slab planes, 2 y-slab columns, 8
 // z-slab columns, 4 ADE box, 16 TFSF): lean, x planes, ADE box, y columns,
 // z columns, y+z corner columns, anything with ADE next to a slab (all
@@ -455,7 +457,7 @@ int encode_stage_maps(xfb_handle* h) {
                                static_cast<cuuint64_t>(c.nx)};
   const cuuint32_t estr[3] = {1, 1, 1};
   const CUtensorMapDataType ft = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-  for (int t = 0; t < 2; ++t) {
+  for (int t = 0; t < kStepTileCount; ++t) {
     const int TJ = kStepTiles[t].r * kStepTiles[t].nwm;
     const cuuint32_t rh = static_cast<cuuint32_t>(TJ + 2);
     const cuuint32_t fbox[3] = {static_cast<cuuint32_t>(32 + 2 * (16 / sizeof(T))), rh, 1};
@@ -901,7 +903,7 @@ int batch_init(xfb_batch* b) {
   for (size_t q = 0; q < b->hs.size(); ++q) {
     xfb_handle* h = b->hs[q];
     sc.push_back(batch_scene<T>(h));
-    for (int t = 0; t < 2; ++t)
+    for (int t = 0; t < kStepTileCount; ++t)
       for (int set = 0; set < 2; ++set) {
         std::memcpy(mp[q].stage[t][set].f, h->stage_maps[t][set], sizeof(mp[q].stage[t][set].f));
         mp[q].stage[t][set].mid = h->stage_maps[t][set][6];
@@ -916,7 +918,7 @@ int batch_init(xfb_batch* b) {
     if (e == cudaSuccess) e = cudaMemsetAsync(b->err_dev, 0, sizeof(int), b->stream);
     if (e != cudaSuccess) return batch_err(b, XFB_ERR_CUDA, cudaGetErrorString(e));
   }
-  for (int t = 0; t < 2; ++t) {
+  for (int t = 0; t < kStepTileCount; ++t) {
     const int TJ = kStepTiles[t].r * kStepTiles[t].nwm, NT = (kStepTiles[t].nwm + 1) * 32;
     long long columns = 0;
     for (xfb_handle* h : b->hs) columns += static_cast<long long>((h->c.nz + 31) / 32) * ((h->c.ny + TJ - 1) / TJ);
@@ -970,7 +972,8 @@ void batch_enqueue_step(xfb_batch* b, int off, int t) {
   const int parity = static_cast<int>((b->step + off) & 1);
   if (b->n_items[t]) {
     if (t == 0) batch_step3<T, kStepTiles[0].r, kStepTiles[0].nwm>(b, 0, tp, parity);
-    else batch_step3<T, kStepTiles[1].r, kStepTiles[1].nwm>(b, 1, tp, parity);
+    else if (t == 1) batch_step3<T, kStepTiles[1].r, kStepTiles[1].nwm>(b, 1, tp, parity);
+    else batch_step3<T, kStepTiles[2].r, kStepTiles[2].nwm>(b, 2, tp, parity);
   }
   for (xfb_handle* h : b->hs) {
     const Compiled& c = h->c;
@@ -992,7 +995,7 @@ int batch_chunk(xfb_batch* b, int n, int t, bool graph) {
   };
   cudaError_t e = cudaSuccess;
   if (graph) {
-    const int key = (n * 2 + static_cast<int>(b->step & 1)) * 2 + t;
+    const int key = (n * 2 + static_cast<int>(b->step & 1)) * kStepTileCount + t;
     auto it = b->graphs.find(key);
     if (it == b->graphs.end()) {
       cudaGraph_t g;
@@ -1019,32 +1022,42 @@ int batch_chunk(xfb_batch* b, int n, int t, bool graph) {
 }
 
 // Advance every scene n steps.  With tile autotuning on, the first call
-// times one chunk with each tile configuration (results do not depend on the
-// tile) and keeps the faster for the rest of the run.
+// steps once with each tile configuration (untimed: the first launch of a
+// kernel loads its module), then times a few steps with each (results do
+// not depend on the tile) and keeps the fastest for the rest of the run.
 template <typename T>
 int batch_run(xfb_batch* b, long long n) {
   int rc;
   if (b->tile < 0) {
-    if (b->tile_req == 8 || b->tile_req == 16 || n < 2) {
-      b->tile = b->tile_req == 8 ? 0 : 1;
+    if (b->tile_req != 0 || n < 2 * kStepTileCount) {
+      b->tile = 1;
+      for (int t = 0; t < kStepTileCount; ++t)
+        if (kStepTileRows[t] == b->tile_req) b->tile = t;
     } else {
-      const int probe = static_cast<int>(std::min<long long>(4, n / 2));
-      float ms[2] = {0, 0};
-      cudaEvent_t e0, e1;
-      cudaEventCreate(&e0);
-      cudaEventCreate(&e1);
-      for (int t = 0; t < 2; ++t) {
-        cudaEventRecord(e0, b->stream);
-        if ((rc = batch_chunk<T>(b, probe, t, false))) return rc;
-        cudaEventRecord(e1, b->stream);
-        cudaError_t e = cudaEventSynchronize(e1);
-        if (e != cudaSuccess) return batch_err(b, XFB_ERR_CUDA, cudaGetErrorString(e));
-        cudaEventElapsedTime(&ms[t], e0, e1);
+      for (int t = 0; t < kStepTileCount; ++t)
+        if ((rc = batch_chunk<T>(b, 1, t, false))) return rc;
+      n -= kStepTileCount;
+      const int probe = static_cast<int>(std::min<long long>(4, n / kStepTileCount));
+      float ms[kStepTileCount] = {};
+      cudaEvent_t ev[2];
+      cudaEventCreate(&ev[0]);
+      cudaEventCreate(&ev[1]);
+      rc = XFB_OK;
+      for (int t = 0; t < kStepTileCount && !rc; ++t) {
+        cudaEventRecord(ev[0], b->stream);
+        if ((rc = batch_chunk<T>(b, probe, t, false))) break;
+        cudaEventRecord(ev[1], b->stream);
+        cudaError_t e = cudaEventSynchronize(ev[1]);
+        if (e != cudaSuccess) rc = batch_err(b, XFB_ERR_CUDA, cudaGetErrorString(e));
+        else cudaEventElapsedTime(&ms[t], ev[0], ev[1]);
       }
-      cudaEventDestroy(e0);
-      cudaEventDestroy(e1);
-      b->tile = ms[0] <= ms[1] ? 0 : 1;
-      n -= 2 * probe;
+      cudaEventDestroy(ev[0]);
+      cudaEventDestroy(ev[1]);
+      if (rc) return rc;
+      b->tile = 0;
+      for (int t = 1; t < kStepTileCount; ++t)
+        if (ms[t] < ms[b->tile]) b->tile = t;
+      n -= kStepTileCount * probe;
     }
   }
   while (n > 0) {

@@ -1353,8 +1353,8 @@ struct BatchScene {
 // configuration and read set, bulk-store maps per tile configuration and
 // write set.
 struct BatchMaps {
-  StageMaps stage[2][2];
-  StoreMaps store[2][2];
+  StageMaps stage[3][2];
+  StoreMaps store[3][2];
 };
 
 // The one-sweep step of a batch of scenes in one launch: one CTA per work

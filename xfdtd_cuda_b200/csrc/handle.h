@@ -87,8 +87,8 @@ struct xfb_handle {
   // read set (six field components, then the material ids), the bulk-store
   // maps of its lean interior items per tile configuration and write set
   // (Ex Ey Ez Hx Hy Hz), and its error flag (1: a staging wait ran out)
-  CUtensorMap stage_maps[2][2][7];
-  CUtensorMap store_maps[2][2][6];
+  CUtensorMap stage_maps[3][2][7];
+  CUtensorMap store_maps[3][2][6];
   int* step_err = nullptr;
   // ADE applied by k_ade_box after the one-sweep step (no dispersive cell
   // takes a TFSF or CPML correction)
@@ -113,14 +113,14 @@ struct xfb_batch {
   cudaStream_t stream = nullptr;
   bool inited = false;
   long long step = 0, total = 0, cells = 0;
-  int tile_req = 0;   // 0: autotune, 8 or 16 rows
+  int tile_req = 0;   // 0: autotune, else 8, 14 or 16 rows
   int tile = -1;      // tile configuration in use (-1 until chosen)
   int graph_steps = 64;
   void* scenes = nullptr;   // BatchScene<T>[n]
   void* maps = nullptr;     // BatchMaps[n]: tensor maps of every scene
   int* err_dev = nullptr;   // 1: a staging wait of the step kernel ran out
-  void* items[2] = {};      // per tile configuration
-  int n_items[2] = {};
+  void* items[3] = {};      // per tile configuration
+  int n_items[3] = {};
   long long* t_dev = nullptr;
   std::map<int, cudaGraphExec_t> graphs;
 };
@@ -162,7 +162,10 @@ long long roundup(long long v, long long m);
 bool fused(const xfb_handle* h);
 // tile configuration of the one-sweep kernel picked by the launch hint's rows
 inline int step_tile_index(int tj) { return tj <= 8 ? 0 : 1; }
-constexpr int kStepTileRows[2] = {8, 16};
+// tile rows of the one-sweep kernel's configurations; single scenes use the
+// first two, a batch autotunes over all three
+constexpr int kStepTileCount = 3;
+constexpr int kStepTileRows[kStepTileCount] = {8, 16, 14};
 bool plain(const xfb_handle* h);
 int cur_set(const xfb_handle* h);
 void* field_ptr(const xfb_handle* h, int set, int q);
