@@ -321,9 +321,10 @@ constexpr StepTile kStepTiles[kStepTileCount] = {{2, 4}, {2, 8}, {2, 7}};
 // z columns, y+z corner columns, anything with ADE next to a slab (all
 // without TFSF code), lean with TFSF corrections, lean interior (the
 // bulk-copy path of single scenes), kinds 1..6 with TFSF corrections for the
-// items that meet the TFSF surface, lean interior with TFSF corrections, and
-// the y- and z-column kinds on the bulk-copy path
-constexpr int kStepKindCount = 19;
+// items that meet the TFSF surface, lean interior with TFSF corrections, the
+// y-, z- and corner-column kinds on the bulk-copy path, and those three with
+// TFSF corrections
+constexpr int kStepKindCount = 22;
 
 // True when a work item over planes [p, q) of the tile at (j0, k0) may meet a
 // TFSF correction: the cells it updates (H at planes p-1 .. q-1, rows j0-1 ..
@@ -398,6 +399,8 @@ inline void build_step_items(const Compiled& c, int TJ, int NT, bool ade_deferre
             k0 + 32 <= nz)
           kind = kind == 0 ? kLeanInterior : kLeanInteriorTf;
         if (lean_interior && (kind == 3 || kind == 4 || kind == 5)) kind = kind == 3 ? kFastY : kind == 4 ? kFastZ : kFastYZ;
+        if (lean_interior && (kind == 11 || kind == 12 || kind == 13))
+          kind = kind == 11 ? kFastYTf : kind == 12 ? kFastZTf : kFastYZTf;
         out[kind].push_back(make_int4(bx, by, p, q));
         p = q;
       }
@@ -496,7 +499,7 @@ inline int upload_step_items(xfb_handle* h) {
     // and column tile, so CTAs resident together cover neighbouring tiles of
     // the same plane range and the halo rows and columns one CTA stages are
     // the ones its neighbours read moments before (L2 hits)
-    static const int costly[] = {14, 6, 13, 5, kFastYZ, 12, 4, kFastZ, 11, 3, kFastY, 10, 2};
+    static const int costly[] = {14, 6, 13, 5, kFastYZTf, kFastYZ, 12, 4, kFastZTf, kFastZ, 11, 3, kFastYTf, kFastY, 10, 2};
     std::vector<int4> all, rest;
     for (int q : costly)
       for (int4 v : items[q]) all.push_back(make_int4(v.x | (q << 16), v.y, v.z, v.w));

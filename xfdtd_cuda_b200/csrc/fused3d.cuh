@@ -1284,6 +1284,9 @@ constexpr int kLeanInterior = 8, kLeanInteriorTf = 15;
 constexpr int kFastY = 16, kFastZ = 17;
 // ... and of the y+z corner columns
 constexpr int kFastYZ = 18;
+// ... and of the same three column kinds with TFSF corrections (a tile
+// column whose 32 columns or TJ rows hold both CPML cells and a TFSF face)
+constexpr int kFastYTf = 19, kFastZTf = 20, kFastYZTf = 21;
 
 template <typename T, int R, int NWM, int NS_, bool TMA>
 __device__ __forceinline__ void step_dispatch(const GridP<T>& s, const GridP<T>& d, const PmlP<T>& pm,
@@ -1297,6 +1300,9 @@ __device__ __forceinline__ void step_dispatch(const GridP<T>& s, const GridP<T>&
       case kFastY: step_item_fast<T, R, NWM, NS_, false, 3>(s, pm, ps, pd, item, lut8, n_mat, tf, maps, outs, err); return;
       case kFastZ: step_item_fast<T, R, NWM, NS_, false, 9>(s, pm, ps, pd, item, lut8, n_mat, tf, maps, outs, err); return;
       case kFastYZ: step_item_fast<T, R, NWM, NS_, false, 11>(s, pm, ps, pd, item, lut8, n_mat, tf, maps, outs, err); return;
+      case kFastYTf: step_item_fast<T, R, NWM, NS_, true, 3>(s, pm, ps, pd, item, lut8, n_mat, tf, maps, outs, err); return;
+      case kFastZTf: step_item_fast<T, R, NWM, NS_, true, 9>(s, pm, ps, pd, item, lut8, n_mat, tf, maps, outs, err); return;
+      case kFastYZTf: step_item_fast<T, R, NWM, NS_, true, 11>(s, pm, ps, pd, item, lut8, n_mat, tf, maps, outs, err); return;
       default: break;
     }
   }
