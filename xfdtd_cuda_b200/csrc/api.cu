@@ -57,6 +57,8 @@ void free_device(xfb_handle* h) {
   h->labc_w = nullptr;
   h->labc_hist = nullptr;
   h->step_err = nullptr;
+  h->ade_runs = nullptr;
+  h->n_ade_runs = -1;
   h->inited = false;
 }
 

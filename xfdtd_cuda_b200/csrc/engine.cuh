@@ -18,6 +18,7 @@
 namespace xfb {
 
 inline int upload_step_items(xfb_handle* h);
+inline int upload_ade_runs(xfb_handle* h);
 template <typename T>
 int encode_stage_maps(xfb_handle* h);
 
@@ -62,6 +63,7 @@ int init_device(xfb_handle* h) {
   if ((rc = upload<T>(h, &h->lut, c.coeff))) return rc;
   if ((rc = upload<T>(h, &h->lut8, c.coeff8))) return rc;
   if (fused(h) && c.dim == 3 && (rc = upload_step_items(h))) return rc;
+  if (fused(h) && c.dim == 3 && h->ade_deferred && (rc = upload_ade_runs(h))) return rc;
   if (fused(h) && c.dim == 3) {
     if ((rc = encode_stage_maps<T>(h))) return rc;
     void* p;
@@ -520,6 +522,52 @@ inline int upload_step_items(xfb_handle* h) {
   return XFB_OK;
 }
 
+// Work list of the deferred ADE pass: the dispersive cells of the ADE box as
+// runs along k, cut at multiples of 32 (k_ade_runs).  Grids with a side of
+// 2^16 cells or more keep k_ade_box.
+inline int upload_ade_runs(xfb_handle* h) {
+  const Compiled& c = h->c;
+  const int* b = c.ade_box;
+  if (c.nx >= 65536 || c.ny >= 65536 || c.nz >= 65536) return XFB_OK;
+  std::vector<int2> runs;
+  for (int i = b[0]; i < b[1]; ++i)
+    for (int j = b[2]; j < b[3]; ++j) {
+      const uint8_t* row = c.mat_id.data() + (static_cast<size_t>(i) * c.ny + j) * c.nz;
+      int k = b[4];
+      while (k < b[5]) {
+        if (!c.mat_disp[row[k]]) { ++k; continue; }
+        const int kb = k & ~31;
+        int e = k;
+        while (e < b[5] && e < kb + 32 && c.mat_disp[row[e]]) ++e;
+        runs.push_back(make_int2(static_cast<int>(static_cast<unsigned>(i) | (static_cast<unsigned>(j) << 16)),
+                                 kb | ((k - kb) << 16) | ((e - kb) << 24)));
+        k = e;
+      }
+    }
+  h->n_ade_runs = static_cast<int>(runs.size());
+  if (runs.empty()) return XFB_OK;
+  int rc = alloc(h, &h->ade_runs, runs.size() * sizeof(int2), false);
+  if (rc) return rc;
+  return copy(h, h->ade_runs, runs.data(), runs.size() * sizeof(int2), cudaMemcpyHostToDevice);
+}
+
+// The deferred ADE pass of one step (E^n in field set `parity`, the plain
+// eNext values in the other).
+template <typename T>
+void launch_ade(xfb_handle* h, int parity, cudaStream_t st) {
+  if (h->n_ade_runs >= 0) {
+    if (h->n_ade_runs > 0)
+      k_ade_runs<T><<<(h->n_ade_runs + 3) / 4, 128, 0, st>>>(grid_params<T>(h, parity), grid_params<T>(h, 1 - parity),
+                                                             ade_params<T>(h), static_cast<const int2*>(h->ade_runs),
+                                                             h->n_ade_runs);
+    return;
+  }
+  const int* b = h->c.ade_box;
+  dim3 grd((b[5] - b[4] + 127) / 128, b[3] - b[2], b[1] - b[0]);
+  k_ade_box<T><<<grd, 128, 0, st>>>(grid_params<T>(h, parity), grid_params<T>(h, 1 - parity), ade_params<T>(h),
+                                    h->mat_disp);
+}
+
 template <typename T, int R, int NWM>
 void launch_step3(xfb_handle* h, int t, int parity, TimeP tp, cudaStream_t st) {
   constexpr int NS = 4;
@@ -722,12 +770,7 @@ void enqueue_step(xfb_handle* h, int off, Prof* pf = nullptr) {
     } else {
       launch_fused<T>(h, parity, tp, s);
     }
-    if (h->ade_deferred) {
-      const int* b = c.ade_box;
-      dim3 grd((b[5] - b[4] + 127) / 128, b[3] - b[2], b[1] - b[0]);
-      k_ade_box<T><<<grd, 128, 0, s>>>(grid_params<T>(h, parity), grid_params<T>(h, 1 - parity), ade_params<T>(h),
-                                       h->mat_disp);
-    }
+    if (h->ade_deferred) launch_ade<T>(h, parity, s);
     if (h->labc_on) {
       const LabcP lp = labc_params(h);
       k_labc_apply<T><<<static_cast<unsigned>((lp.off[12] + 127) / 128), 128, 0, s>>>(
@@ -980,12 +1023,7 @@ void batch_enqueue_step(xfb_batch* b, int off, int t) {
   }
   for (xfb_handle* h : b->hs) {
     const Compiled& c = h->c;
-    if (h->ade_deferred) {
-      const int* bx = c.ade_box;
-      dim3 grd((bx[5] - bx[4] + 127) / 128, bx[3] - bx[2], bx[1] - bx[0]);
-      k_ade_box<T><<<grd, 128, 0, b->stream>>>(grid_params<T>(h, parity), grid_params<T>(h, 1 - parity),
-                                               ade_params<T>(h), h->mat_disp);
-    }
+    if (h->ade_deferred) launch_ade<T>(h, parity, b->stream);
     if (c.nf_on || !c.probes.empty() || !c.movies.empty()) enqueue_records<T>(h, parity, tp, b->stream, nullptr);
   }
 }

@@ -93,6 +93,9 @@ struct xfb_handle {
   // ADE applied by k_ade_box after the one-sweep step (no dispersive cell
   // takes a TFSF or CPML correction)
   bool ade_deferred = false;
+  // its work list: runs of dispersive cells (k_ade_runs); -1: no list (k_ade_box)
+  void* ade_runs = nullptr;
+  int n_ade_runs = -1;
   // set while a batch steps this handle (xfb_batch_*)
   xfb_batch* batch = nullptr;
   // learned absorbing boundary (xfb_set_learned_abc): BF16 weights and the

@@ -286,23 +286,19 @@ __device__ __forceinline__ T ade_e(const AdeP<T>& a, int comp, long long bi, int
   return e_new;
 }
 
-// Deferred ADE update of the dispersive box after a one-sweep step.  The step
-// kernel stored the plain eNext value of every cell in `d`; this applies the
-// TemplateADEUpdateScheme::updateE recursion with E^n from `s`, one thread per
-// box cell, k fastest.  All inputs of a cell (E^n, plain values, J, J_prev,
+// Deferred ADE update of one dispersive cell of the box after a one-sweep
+// step.  The step kernel stored the plain eNext value of every cell in `d`;
+// this applies the TemplateADEUpdateScheme::updateE recursion with E^n from
+// `s` (k_ade_box: one thread per box cell, k fastest; k_ade_runs: one thread
+// per dispersive cell).  All inputs of a cell (E^n, plain values, J, J_prev,
 // E_prev of the three components) are loaded before any update, so the loads
 // overlap; the arithmetic and its order are those of ade_e.  Valid only when
 // no dispersive cell also takes a TFSF or CPML correction, which the
 // reference applies after the ADE update.
 template <typename T>
-__global__ void k_ade_box(GridP<T> s, GridP<T> d, AdeP<T> ad, const uint8_t* disp) {
+__device__ __forceinline__ void ade_box_cell(const GridP<T>& s, const GridP<T>& d, const AdeP<T>& ad, int i, int j,
+                                             int k, long long idx, int m) {
   constexpr int MP = 4;  // XFB_MAX_POLES
-  const int k = ad.b4 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= ad.b5) return;
-  const int j = ad.b2 + blockIdx.y, i = ad.b0 + blockIdx.z;
-  const long long idx = static_cast<long long>(i) * s.sx + static_cast<long long>(j) * s.sy + k;
-  const int m = s.mid[idx];
-  if (!disp[m]) return;
   const long long bi = static_cast<long long>(i - ad.b0) * ad.bsx + static_cast<long long>(j - ad.b2) * ad.bsy + (k - ad.b4);
   const bool upd[3] = {j > 0 && k > 0, i > 0 && k > 0, i > 0 && j > 0};
   T* dd[3] = {d.ex, d.ey, d.ez};
@@ -360,6 +356,34 @@ __global__ void k_ade_box(GridP<T> s, GridP<T> d, AdeP<T> ad, const uint8_t* dis
     }
     dd[c][idx] = e_new;
   }
+}
+
+template <typename T>
+__global__ void k_ade_box(GridP<T> s, GridP<T> d, AdeP<T> ad, const uint8_t* disp) {
+  const int k = ad.b4 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ad.b5) return;
+  const int j = ad.b2 + blockIdx.y, i = ad.b0 + blockIdx.z;
+  const long long idx = static_cast<long long>(i) * s.sx + static_cast<long long>(j) * s.sy + k;
+  const int m = s.mid[idx];
+  if (!disp[m]) return;
+  ade_box_cell(s, d, ad, i, j, k, idx, m);
+}
+
+// The same update over a list of runs of dispersive cells (one warp per run
+// of at most 32 cells inside one 32-aligned k segment, so each warp's field
+// accesses stay inside one 128-byte line per array): run q = {i | j << 16,
+// kb | lo << 16 | hi << 24}, cells k = kb + lane for lo <= lane < hi.
+template <typename T>
+__global__ void k_ade_runs(GridP<T> s, GridP<T> d, AdeP<T> ad, const int2* runs, int n_runs) {
+  const int q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (q >= n_runs) return;
+  const int lane = threadIdx.x & 31;
+  const int2 r = runs[q];
+  const int lo = (r.y >> 16) & 0xff, hi = static_cast<int>(static_cast<unsigned>(r.y) >> 24);
+  if (lane < lo || lane >= hi) return;
+  const int i = r.x & 0xffff, j = static_cast<int>(static_cast<unsigned>(r.x) >> 16), k = (r.y & 0xffff) + lane;
+  const long long idx = static_cast<long long>(i) * s.sx + static_cast<long long>(j) * s.sy + k;
+  ade_box_cell(s, d, ad, i, j, k, idx, s.mid[idx]);
 }
 
 // E half-step, 3-D.  Same tiling as k_h3; H values of plane i are carried to
