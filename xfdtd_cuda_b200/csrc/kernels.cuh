@@ -372,9 +372,11 @@ __global__ void k_ade_box(GridP<T> s, GridP<T> d, AdeP<T> ad, const uint8_t* dis
 // The same update over a list of runs of dispersive cells (one warp per run
 // of at most 32 cells inside one 32-aligned k segment, so each warp's field
 // accesses stay inside one 128-byte line per array): run q = {i | j << 16,
-// kb | lo << 16 | hi << 24}, cells k = kb + lane for lo <= lane < hi.
+// kb | lo << 16 | hi << 24}, cells k = kb + lane for lo <= lane < hi.  FP32:
+// 64 registers, so 8 CTAs (32 warps) fit an SM (the pass is load-latency
+// bound); FP64 keeps its own register count (it would spill at 64).
 template <typename T>
-__global__ void k_ade_runs(GridP<T> s, GridP<T> d, AdeP<T> ad, const int2* runs, int n_runs) {
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 8 : 1) k_ade_runs(GridP<T> s, GridP<T> d, AdeP<T> ad, const int2* runs, int n_runs) {
   const int q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (q >= n_runs) return;
   const int lane = threadIdx.x & 31;
