@@ -523,13 +523,12 @@ inline int upload_step_items(xfb_handle* h) {
 }
 
 // Work list of the deferred ADE pass: the dispersive cells of the ADE box as
-// runs along k, cut at multiples of 32 (k_ade_runs).  Grids with a side of
-// 2^16 cells or more keep k_ade_box.
-inline int upload_ade_runs(xfb_handle* h) {
-  const Compiled& c = h->c;
+// runs along k, cut at multiples of 32 (k_ade_runs), in (i, j, k) order.
+// False (no list: k_ade_box) for grids with a side of 2^16 cells or more.
+inline bool build_ade_runs(const Compiled& c, std::vector<int2>& runs) {
   const int* b = c.ade_box;
-  if (c.nx >= 65536 || c.ny >= 65536 || c.nz >= 65536) return XFB_OK;
-  std::vector<int2> runs;
+  runs.clear();
+  if (c.nx >= 65536 || c.ny >= 65536 || c.nz >= 65536) return false;
   for (int i = b[0]; i < b[1]; ++i)
     for (int j = b[2]; j < b[3]; ++j) {
       const uint8_t* row = c.mat_id.data() + (static_cast<size_t>(i) * c.ny + j) * c.nz;
@@ -544,6 +543,12 @@ inline int upload_ade_runs(xfb_handle* h) {
         k = e;
       }
     }
+  return true;
+}
+
+inline int upload_ade_runs(xfb_handle* h) {
+  std::vector<int2> runs;
+  if (!build_ade_runs(h->c, runs)) return XFB_OK;
   h->n_ade_runs = static_cast<int>(runs.size());
   if (runs.empty()) return XFB_OK;
   int rc = alloc(h, &h->ade_runs, runs.size() * sizeof(int2), false);
