@@ -1267,16 +1267,16 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
 
 // The one-sweep step kernel: one CTA per work item (x: k tile | kind << 16,
 // y: j tile, z: first plane, w: end plane); every kind runs its own
-// specialised body, so one launch covers the whole grid.  Kind bits: 1 x-slab
-// planes, 2 y-slab columns, 8 z-slab columns, 4 ADE box, 16 TFSF corrections;
-// only the lean kind (0) leaves the TFSF code out, kind 16 is lean with it.
-// Kind indices 0..6: lean, x planes, ADE box, y columns, z columns, y+z
-// corner columns, ADE next to a slab, all without TFSF code; 7: lean with
-// TFSF; 8: lean interior (step_item_lean); 9..14: kinds 1..6 with TFSF;
-// 15: lean interior with TFSF.
+// specialised body, so one launch covers the whole grid.  Region bits of a
+// kind: 1 x-slab planes, 2 y-slab columns, 8 z-slab columns, 4 ADE box, 16
+// TFSF corrections.  Kind indices 0..6: lean, x planes, ADE box, y columns,
+// z columns, y+z corner columns, ADE next to a slab, all without TFSF code;
+// 7: lean with TFSF; 8: lean interior; 9..14: kinds 1..6 with TFSF; 15: lean
+// interior with TFSF; 16..18: y, z and corner columns on the bulk-copy body;
+// 19..21: those with TFSF.  kStepKinds gives the bits of indices 0..15.
 constexpr int kStepKinds[16] = {0, 1, 4, 3, 9, 11, 15, 16, 0, 1 | 16, 4 | 16, 3 | 16, 9 | 16, 11 | 16, 15 | 16, 16};
 
-// kind indices of the lean interior items (step_item_lean, bulk-copy path
+// kind indices of the lean interior items (step_item_fast, bulk-copy path
 // only), without and with TFSF corrections
 constexpr int kLeanInterior = 8, kLeanInteriorTf = 15;
 // kind indices of the y- and z-slab CPML columns run by step_item_fast (the
