@@ -54,7 +54,7 @@ int init_device(xfb_handle* h) {
     std::vector<uint8_t> m(static_cast<size_t>(h->elems), 0);
     for (int i = 0; i < nx; ++i)
       for (int j = 0; j < ny; ++j)
-        for (int k = 0; k < nz; ++k) m[off3(h, i, j, k)] = c.mat_id[(static_cast<size_t>(i) * ny + j) * nz + k];
+        std::memcpy(m.data() + i * h->sx + j * h->sy, c.mat_id.data() + (static_cast<size_t>(i) * ny + j) * nz, nz);
     void* p;  // same guard as the fields (the one-sweep kernel stages halo windows)
     if ((rc = alloc(h, &p, m.size() + 2 * h->guard, false))) return rc;
     if ((rc = copy(h, static_cast<uint8_t*>(p) + h->guard, m.data(), m.size(), cudaMemcpyHostToDevice))) return rc;
@@ -873,8 +873,48 @@ int profile_steps(xfb_handle* h, long long n, double* ms, long long* launches) {
 
 
 
+// Component f in the reference's dense layout, as doubles: the cells of
+// planes [i0, i0 + n / (s1 * s2)) gathered out of the padded layout (src
+// points at plane i0), one thread per cell.
+template <typename T>
+__global__ void k_gather_field(const T* src, double* dst, long long sx, long long sy, int s1, int s2, long long n) {
+  for (long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; q < n;
+       q += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long ij = q / s2;
+    const long long i = ij / s1;
+    const long long j = ij - i * s1, k = q - ij * s2;
+    dst[q] = static_cast<double>(src[i * sx + j * sy + k]);
+  }
+}
+
+// Read-back of component f: gathered on the device in chunks of whole planes
+// (a staging buffer of at most 32 Mi doubles), each chunk copied straight into
+// the caller's array; the host-side gather below when the staging buffer
+// cannot be allocated.
 template <typename T>
 int read_field_t(xfb_handle* h, int f, double* dst) {
+  {
+    int s[3];
+    comp_shape(h->c, f, s);
+    const long long plane = static_cast<long long>(s[1]) * s[2];
+    const long long chunk = std::max(1LL, std::min<long long>(s[0], (32LL << 20) / std::max(1LL, plane)));
+    double* stage = nullptr;
+    if (plane > 0 && cudaMalloc(&stage, static_cast<size_t>(chunk * plane) * sizeof(double)) == cudaSuccess) {
+      const T* src = static_cast<const T*>(field_ptr(h, cur_set(h), f));
+      int rc = XFB_OK;
+      for (long long i0 = 0; i0 < s[0] && !rc; i0 += chunk) {
+        const long long n = std::min<long long>(chunk, s[0] - i0) * plane;
+        const unsigned blocks = static_cast<unsigned>(std::min<long long>((n + 255) / 256, 148LL * 16));
+        k_gather_field<T><<<blocks, 256, 0, h->stream>>>(src + i0 * h->sx, stage, h->sx, h->sy, s[1], s[2], n);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = cuda_err(h, e, "k_gather_field");
+        else rc = copy(h, dst + i0 * plane, stage, static_cast<size_t>(n) * sizeof(double), cudaMemcpyDeviceToHost);
+      }
+      cudaFree(stage);
+      return rc;
+    }
+    cudaGetLastError();  // allocation failed: gather on the host
+  }
   std::vector<T> tmp(static_cast<size_t>(h->elems));
   int rc;
   if ((rc = copy(h, tmp.data(), field_ptr(h, cur_set(h), f), tmp.size() * sizeof(T), cudaMemcpyDeviceToHost))) return rc;
