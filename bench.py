@@ -177,7 +177,27 @@ def build_scene(cells, precision, scene="dispersive"):
     return s
 
 
-def cpu_sample(cells: int, steps: int, precision="fp64"):
+def cpu_model():
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def _omp_threads(n):
+    """Set the OpenMP thread count of the calling thread (the CPU restatement
+    runs its parallel loops from it)."""
+    import ctypes
+    try:
+        ctypes.CDLL("libgomp.so.1").omp_set_num_threads(int(n))
+    except OSError:
+        pass
+
+
+def cpu_sample(cells: int, steps: int, precision="fp64", threads: int | None = None):
     """Time the CPU restatement on a bounded sample of the workload."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import xfdtd_cuda_b200 as X
@@ -186,14 +206,16 @@ def cpu_sample(cells: int, steps: int, precision="fp64"):
     sc, keep = sim.lower()
     h = X.Handle(sc, keep)
     o = OracleSim(h, steps + 2)
+    threads = threads or int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    _omp_threads(threads)
     o.run(2)  # warm-up (first touch of the arrays)
     gi = h.info()
     t0 = time.perf_counter()
     o.run(steps)
     dt = time.perf_counter() - t0
+    _omp_threads(int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)))
     n = gi.nx * gi.ny * gi.nz
-    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {"value": n * steps / dt / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
+    return {"value": n * steps / dt / 1e6, "unit": UNIT, "cores": threads, "kind": "port", "cpu": cpu_model(),
             "sample": f"dispersive sphere {gi.nx}x{gi.ny}x{gi.nz} ({cells}^3 + 12-cell CPML), FP64, {steps} steps, "
                       f"CPU restatement (oracle/, OpenMP {threads} threads), {dt:.1f} s"}
 
@@ -361,7 +383,7 @@ def main():
     ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
     ap.add_argument("--profile-steps", type=int, default=6)
     ap.add_argument("--ref-cells", type=int, default=128)
-    ap.add_argument("--cpu-steps", type=int, default=40)
+    ap.add_argument("--cpu-steps", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--path", choices=["auto", "split", "fused", "plain"], default="auto")
@@ -371,6 +393,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 64-scene leg")
     ap.add_argument("--no-labc", action="store_true", help="skip the learned-boundary leg")
     ap.add_argument("--no-2d", action="store_true", help="skip the 2-D cylinder leg")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the full-size FP32-vs-FP64 accuracy leg")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -449,28 +472,33 @@ def main():
     e2e = None
     if not args.no_e2e:
         barrier()
-        t0 = time.perf_counter()
+        t = [time.perf_counter()]
         sc2, keep2 = sim.lower()
-        h2 = X.Handle(sc2, keep2)
+        h2 = X.Handle(sc2, keep2)  # host scene compiler (voxelisation, coefficients, profiles)
+        t.append(time.perf_counter())
         h2.set_device(local)
         h2.set_kernel_path(path)
         h2.set_launch_hint((1, 1, 1), (32, args.tile_rows, 1))
-        h2.init(args.steps)
+        h2.init(args.steps)  # device buffers, uploads, incident tables
+        t.append(time.perf_counter())
         h2.step(args.steps)
         h2.sync()
-        d2h = 0
+        t.append(time.perf_counter())
         for f in range(6):
-            d2h += h2.read_field(f).size * esize(args.precision)
+            h2.read_field(f)
         for f in range(gi.n_freqs):
             for face in range(6):
                 for w in range(4):
-                    d2h += h2.read_nf2ff(f, face, w).size * 16
-        wall = time.perf_counter() - t0
-        h2d = cells * 1 + 64 * 1024  # material ids + coefficient/profile tables
-        wall = max_over_ranks(wall, dist)
+                    h2.read_nf2ff(f, face, w)
+        t.append(time.perf_counter())
+        wall = max_over_ranks(t[-1] - t[0], dist)
+        gi2 = h2.info()  # bytes the library copied each way (its own counters)
+        parts = dict(zip(("compile", "init", "step", "read_back"), (t[q + 1] - t[q] for q in range(4))))
         e2e = {"value": job_rate(cells, args.steps, world, wall * 1e3), "unit": UNIT,
-               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-               "path": "Handle(scene) + init + step + read-back (SimulationHD.run flow), wall clock"}
+               "h2d_bytes_per_step": gi2.h2d_bytes / args.steps, "d2h_bytes_per_step": gi2.d2h_bytes / args.steps,
+               "seconds": {**parts, "wall": t[-1] - t[0]},
+               "path": "Handle(scene) + init + step + read-back of the six fields (as doubles) and the NF2FF "
+                       "currents (SimulationHD.run flow), wall clock; bytes counted by the library"}
         h2.close()
 
     h.close()
@@ -496,9 +524,22 @@ def main():
         except Exception as exc:
             learned = {"error": str(exc)}
 
+    accuracy = None
+    if not args.no_accuracy and world == 1:
+        try:
+            from xfdtd_cuda_b200 import accuracy as A
+            accuracy = {"what": "relative L2 of the FP32 one-sweep engine against the FP64 engine (bit-identical "
+                                "to the CPU restatement) at full size, per output",
+                        "dielectric_sphere_156cube_2400_steps": A.fp32_vs_fp64("dielectric", 2400, local),
+                        "dispersive_sphere_408cube_6000_steps": A.fp32_vs_fp64("dispersive", 6000, local)}
+        except Exception as exc:
+            accuracy = {"error": str(exc)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_sample(args.ref_cells, args.cpu_steps)
+        one = cpu_sample(args.ref_cells // 2, max(10, args.cpu_steps // 5), threads=1)
+        cpu["one_core"] = {"value": one["value"], "sample": one["sample"]}
 
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -509,7 +550,7 @@ def main():
                           "l2": "resident state 3.3 GB >> 126 MB L2 (no flush needed)"},
                "e2e": e2e, "roofline": roofline, "step_roofline": step_roof, "cpu_baseline": cpu,
                "clocks": clk.summary(), "gpu_launches": launches, "kernels": kernels, "vs_fp64_plain": plain,
-               "batched": batched, "learned_abc": learned, "cylinder_2d": cyl2d}
+               "batched": batched, "learned_abc": learned, "cylinder_2d": cyl2d, "accuracy": accuracy}
         print(json.dumps(out))
     if dist:
         dist[1].barrier()

@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define XFB_ABI_VERSION 1
+#define XFB_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------- */
 #define XFB_OK 0
@@ -130,6 +130,17 @@ typedef struct xfb_nf2ff {
   const double* freqs; /* Hz */
 } xfb_nf2ff;
 
+/* Time-domain near-to-far-field transformation for one observation
+ * direction: the retarded-time potentials of the equivalent surface currents
+ * on a box (the reference's NFFFTTimeDomain path,
+ * src/nf2ff/time_domain/nf2ff_time_domain_data.cu:113-175,
+ * nf2ff_time_domain_hd.cu:1-234). */
+typedef struct xfb_nf2ff_td {
+  int enabled;
+  int inset[3];        /* cells between the inner domain edge and the box    */
+  double theta, phi;   /* observation direction, rad                        */
+} xfb_nf2ff_td;
+
 typedef struct xfb_probe {
   int field;           /* enum xfb_field */
   int index[3];        /* component index (i, j, k) */
@@ -159,6 +170,7 @@ typedef struct xfb_scene {
   const xfb_probe* probes;
   int n_movies;
   const xfb_movie* movies;
+  xfb_nf2ff_td nf2ff_td;
 } xfb_scene;
 
 /* ---- grid information --------------------------------------------------- */
@@ -179,6 +191,9 @@ typedef struct xfb_grid_info {
   long long n_dispersive_cells; /* cells whose material has ADE poles */
   int launches_per_step;     /* engine kernels one time step launches */
   int kernel_path;           /* enum xfb_kernel_path in use (after init) */
+  int nf2ff_td_box[6];       /* time-domain NF2FF box (nodes) or zeros */
+  long long h2d_bytes;       /* bytes the handle has copied host -> device */
+  long long d2h_bytes;       /* bytes the handle has copied device -> host */
 } xfb_grid_info;
 
 typedef struct xfb_handle xfb_handle;
@@ -219,8 +234,20 @@ int xfb_run(xfb_handle* h, long long n_steps);
  * not take the run beyond the steps xfb_init sized for).  Asynchronous. */
 int xfb_step(xfb_handle* h, long long n_steps);
 
-/* Block until the handle's stream is idle; reports device-side errors. */
+/* Block until the handle's stream is idle; reports device-side errors.
+ * XFB_ERR_TIMEOUT: a bounded wait of the step kernel ran out (see
+ * xfb_set_wait_limit); the run's results are incomplete, and this sync and
+ * every read-back return the same status until the next xfb_init. */
 int xfb_sync(xfb_handle* h);
+
+/* Diagnostics, no counterpart in the reference.  The 3-D one-sweep step
+ * stages its planes with asynchronous bulk copies and waits for each with a
+ * bounded poll loop (default limit 4194304 polls, far beyond any copy's
+ * latency).  A wait that runs out lets the copies in flight land, ends its
+ * work item and sets the handle's error flag instead of hanging the device.
+ * This call sets the limit (after xfb_init; 0 makes every wait give up at
+ * once, which tests use to exercise that path without a device fault). */
+int xfb_set_wait_limit(xfb_handle* h, int polls);
 
 /* Advance n steps bracketed by CUDA events on the handle's stream (after a
  * synchronize); *ms = elapsed device time of the n steps. */
@@ -291,6 +318,28 @@ int xfb_far_field(xfb_handle* h, int freq, int n_angles, const double* theta,
 int xfb_far_field_static(xfb_handle* h, int freq, int n_angles, const double* theta,
                          const double* phi, double* out);
 
+/* Time-domain NF2FF (scene.nf2ff_td).  Every step adds, for every face point
+ * and both field kinds, the time difference of the interpolated tangential
+ * field times the face area into the time bins of its retarded arrival, with
+ * linear weights between two bins (nf2ff_time_domain_data.cu:150-170):
+ * W from the electric surface current J = n x H, U from the magnetic surface
+ * current M = -n x E, each a vector of x, y, z components, summed over the
+ * six faces.  The reference runs this update on one GPU thread because its
+ * reduction over face points was never written (nf2ff_time_domain_data.cu:174,
+ * 213-223); here every face point has a thread and the bins are summed by a
+ * deterministic two-level reduction, so results do not depend on the launch
+ * and match a sequential sum to round-off.  Bin n is observation time n*dt
+ * after the wave leaves the box point farthest along the direction. */
+int xfb_nf2ff_td_bins(const xfb_handle* h, long long* n_bins);
+/* which = 0, 1, 2: W_x, W_y, W_z; 3, 4, 5: U_x, U_y, U_z (n_bins doubles). */
+int xfb_read_nf2ff_td(xfb_handle* h, int which, double* dst, size_t dst_len);
+/* r E_theta(t_n) and r E_phi(t_n), n < n_bins, from the potentials
+ * (Luebbers et al., IEEE Trans. Antennas Propag. 39(4), 1991):
+ * r E_theta = -(U_phi + eta W_theta) / (4 pi c dt),
+ * r E_phi = (U_theta - eta W_phi) / (4 pi c dt).  Replaces XFDTD_CORE
+ * NFFFTTimeDomain::processFarField. */
+int xfb_far_field_td(xfb_handle* h, double* e_theta, double* e_phi, size_t len);
+
 /* ---- learned absorbing boundary --------------------------------------------
  * No counterpart in the reference.  A small MLP (8 -> 64 -> 64 -> 1, tanh,
  * BF16 weights, FP32 accumulation) corrects the first-order Mur value of the
@@ -335,7 +384,11 @@ int xfb_batch_set_tile(xfb_batch* b, int rows);
 int xfb_batch_init(xfb_batch* b, long long total_steps);
 /* Advance every scene n steps (asynchronous). */
 int xfb_batch_step(xfb_batch* b, long long n);
+/* XFB_ERR_TIMEOUT as for xfb_sync when a bounded wait of the step ran out. */
 int xfb_batch_sync(xfb_batch* b);
+/* Poll limit of the batch step's bounded waits (after xfb_batch_init), as
+ * xfb_set_wait_limit. */
+int xfb_batch_set_wait_limit(xfb_batch* b, int polls);
 /* n steps between CUDA events on the batch's stream; *ms = device time. */
 int xfb_batch_timed_step(xfb_batch* b, long long n, double* ms);
 /* Cells per step over all scenes, tile rows in use (0 before the first step), work items per step. */
@@ -396,6 +449,11 @@ typedef struct xfb_compiled_view {
   const double* freqs;
   const double* nf2ff_te;       /* [n_freqs][total_steps] complex (re,im)    */
   const double* nf2ff_th;
+  int nf2ff_td_enabled;
+  int nf2ff_td_box[6];          /* is ie js je ks ke (nodes)                 */
+  double nf2ff_td_theta, nf2ff_td_phi;
+  long long nf2ff_td_bins;      /* time bins of the potentials (after init)  */
+  double origin[3];             /* physical position of node (0, 0, 0)      */
 } xfb_compiled_view;
 
 int xfb_compiled_view_get(const xfb_handle* h, xfb_compiled_view* out);

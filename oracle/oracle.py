@@ -51,6 +51,10 @@ def load():
         lib.orc_nf2ff.restype = C.POINTER(C.c_double)
         lib.orc_nf2ff.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
         lib.orc_field_shape.argtypes = [C.c_void_p, C.c_int, C.c_int * 3]
+        lib.orc_nf2ff_td.restype = C.POINTER(C.c_double)
+        lib.orc_nf2ff_td.argtypes = [C.c_void_p, C.c_int]
+        lib.orc_nf2ff_td_bins.restype = C.c_longlong
+        lib.orc_nf2ff_td_bins.argtypes = [C.c_void_p]
         lib.orc_step.restype = C.c_longlong
         lib.orc_step.argtypes = [C.c_void_p]
         lib.orc_e_inc.restype = C.POINTER(C.c_double)
@@ -140,6 +144,11 @@ class OracleSim:
         a = np.ctypeslib.as_array(self.lib.orc_nf2ff(self.s, freq, face, which), shape=tuple(n) + (2,))
         return a[..., 0] + 1j * a[..., 1]
 
+    def nf2ff_td(self, which) -> np.ndarray:
+        """Time-domain NF2FF potential `which` (0..2 W_x..W_z, 3..5 U_x..U_z)."""
+        n = int(self.lib.orc_nf2ff_td_bins(self.s))
+        return np.ctypeslib.as_array(self.lib.orc_nf2ff_td(self.s, which), shape=(n,)).copy()
+
     def incident_tables(self):
         nl = self.view.aux_nl
         e = np.ctypeslib.as_array(self.lib.orc_e_inc(self.s), shape=(self.total, nl + 1)).copy()
@@ -193,3 +202,21 @@ def far_field_numpy(currents, box, origin, d, freq, theta, phi):
     e_th = -1j * f * (l_ph + ETA_0 * n_th)
     e_ph = 1j * f * (l_th - ETA_0 * n_ph)
     return e_th, e_ph
+
+
+def far_field_td_numpy(pot, theta, phi, dt):
+    """r E_theta(t_n), r E_phi(t_n) from the time-domain NF2FF potentials
+    pot[6] = (W_x, W_y, W_z, U_x, U_y, U_z) (time differences of the retarded
+    surface-current integrals): Luebbers et al., "A finite-difference
+    time-domain near zone to far zone transformation", IEEE Trans. Antennas
+    Propag. 39(4), 1991: r E_theta = -(U_phi + eta W_theta) / (4 pi c dt),
+    r E_phi = (U_theta - eta W_phi) / (4 pi c dt)."""
+    c0 = 299792458.0
+    wx, wy, wz, ux, uy, uz = pot
+    st, ct, sp, cp = np.sin(theta), np.cos(theta), np.sin(phi), np.cos(phi)
+    w_th = wx * ct * cp + wy * ct * sp - wz * st
+    w_ph = -wx * sp + wy * cp
+    u_th = ux * ct * cp + uy * ct * sp - uz * st
+    u_ph = -ux * sp + uy * cp
+    f = 1.0 / (4 * np.pi * c0 * dt)
+    return -f * (u_ph + ETA_0 * w_th), f * (u_th - ETA_0 * w_ph)

@@ -22,6 +22,9 @@
  *                    face/component corrections per half step; 2-D: 4)
  *   NF2FF (FD)       src/nf2ff/frequency_domain/nf2ff_frequency_domain.data.cu:80-232,
  *                    src/include/nf2ff/interpolate_scheme.cuh:11-134
+ *   NF2FF (TD)       src/nf2ff/time_domain/nf2ff_time_domain_data.cu:113-175,
+ *                    src/include/nf2ff/time_domain/nf2ff_time_domain_data.cuh:64-183
+ *                    (faces XN..ZP, update<E> then update<H>, :203-223)
  *   movie monitor    src/monitor/movie_monitor.cu:17-46
  * The inputs (coefficients, CPML profiles, TFSF projections, incident tables,
  * NF2FF DFT kernels) are what XFDTD_CORE computes on the host in the
@@ -37,6 +40,7 @@
  *
  * Build: oracle/Makefile (gcc -O2 -ffp-contract=off, so no FMA contraction).
  */
+#include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -92,6 +96,13 @@ typedef struct orc_sim {
   const double *te, *th;
   double* acc[64][6][4]; /* [freq][face][ja jb ma mb] complex, face extent */
   int face_n[6][3];
+  /* NF2FF time domain */
+  int td_on, td[6];
+  double td_dir[3], td_ref, d[3], origin[3];
+  long long td_bins;
+  double* td_pot[6];          /* W_x W_y W_z U_x U_y U_z, [td_bins] */
+  double* td_prev[6][2][2];   /* [face][E, H][a, b], face extent */
+  int td_n[6][3];
   /* monitors */
   int n_probes;
   int* probe; /* field, i, j, k */
@@ -127,6 +138,17 @@ static int coef_index(int attr_h, int comp, int dual) {
   int base = (attr_h ? 9 : 0) + 3 * comp;
   if (dual == ax_a(comp)) return base + 1;
   return base + 2;
+}
+
+/* Sample point (i, j, k) of `face` (indices inside the face extent) of the
+ * time-domain box: the face node along the normal, cell centres along the
+ * tangential axes (rVector, nf2ff_time_domain_data.cu:53-66). */
+static void td_position(const orc_sim* s, int face, int i, int j, int k, double r[3]) {
+  const int c = face / 2, pos = face % 2;
+  const int n[3] = {s->td[0] + i + (c == 0 && pos ? s->td[1] - s->td[0] : 0),
+                    s->td[2] + j + (c == 1 && pos ? s->td[3] - s->td[2] : 0),
+                    s->td[4] + k + (c == 2 && pos ? s->td[5] - s->td[4] : 0)};
+  for (int a = 0; a < 3; ++a) r[a] = s->origin[a] + (n[a] + (a == c ? 0.0 : 0.5)) * s->d[a];
 }
 
 orc_sim* orc_create(const xfb_compiled_view* v, int n_probes, const int* probes, int n_movies, const int* movies) {
@@ -227,6 +249,34 @@ orc_sim* orc_create(const xfb_compiled_view* v, int n_probes, const int* probes,
       memcpy(s->face_n[face], n, sizeof(n));
       for (int fq = 0; fq < s->nfreq && fq < 64; ++fq)
         for (int w = 0; w < 4; ++w) s->acc[fq][face][w] = (double*)calloc((size_t)2 * n[0] * n[1] * n[2], sizeof(double));
+    }
+  }
+  s->td_on = v->nf2ff_td_enabled;
+  s->d[0] = v->dx; s->d[1] = v->dy; s->d[2] = v->dz;
+  memcpy(s->origin, v->origin, sizeof(s->origin));
+  if (s->td_on) {
+    memcpy(s->td, v->nf2ff_td_box, sizeof(s->td));
+    s->td_dir[0] = sin(v->nf2ff_td_theta) * cos(v->nf2ff_td_phi);
+    s->td_dir[1] = sin(v->nf2ff_td_theta) * sin(v->nf2ff_td_phi);
+    s->td_dir[2] = cos(v->nf2ff_td_theta);
+    s->td_bins = v->nf2ff_td_bins;
+    for (int q = 0; q < 6; ++q) s->td_pot[q] = (double*)calloc((size_t)(s->td_bins > 0 ? s->td_bins : 1), sizeof(double));
+    /* reference distance: the largest r . dir over the sample points */
+    s->td_ref = -INFINITY;
+    for (int face = 0; face < 6; ++face) {
+      int n[3] = {s->td[1] - s->td[0], s->td[3] - s->td[2], s->td[5] - s->td[4]};
+      n[face / 2] = 1;
+      memcpy(s->td_n[face], n, sizeof(n));
+      for (int kind = 0; kind < 2; ++kind)
+        for (int w = 0; w < 2; ++w) s->td_prev[face][kind][w] = (double*)calloc((size_t)n[0] * n[1] * n[2], sizeof(double));
+      for (int i = 0; i < n[0]; ++i)
+        for (int j = 0; j < n[1]; ++j)
+          for (int k = 0; k < n[2]; ++k) {
+            double r[3];
+            td_position(s, face, i, j, k, r);
+            const double rd = r[0] * s->td_dir[0] + r[1] * s->td_dir[1] + r[2] * s->td_dir[2];
+            if (rd > s->td_ref) s->td_ref = rd;
+          }
     }
   }
   s->n_probes = n_probes;
@@ -519,6 +569,51 @@ static void nf2ff_update(orc_sim* s) {
   }
 }
 
+/* ---- NF2FF time domain (nf2ff_time_domain_data.cu:113-175) --------------- */
+static void nf2ff_td_update(orc_sim* s) {
+  if (!s->td_on) return;
+  const long long t = s->t;
+  const double c0 = 299792458.0; /* __constant__ C_0, nf2ff_time_domain_data.cu:16 */
+  for (int face = 0; face < 6; ++face) {
+    const int c = face / 2, pos = face % 2, a = ax_a(c), b = ax_b(c);
+    const int* n = s->td_n[face];
+    const int i0 = c == 0 && pos ? s->td[1] : s->td[0];
+    const int j0 = c == 1 && pos ? s->td[3] : s->td[2];
+    const int k0 = c == 2 && pos ? s->td[5] : s->td[4];
+    for (int kind = 0; kind < 2; ++kind) { /* update<E> (U), then update<H> (W) */
+      const double off = kind ? 0.0 : 0.5;
+      double ca = kind ? -1.0 : 1.0, cb = kind ? 1.0 : -1.0;
+      if (!pos) { ca *= -1.0; cb *= -1.0; }
+      double* pa = s->td_pot[(kind ? 0 : 3) + a];
+      double* pb = s->td_pot[(kind ? 0 : 3) + b];
+      const int fa = kind ? 3 + a : a, fb = kind ? 3 + b : b;
+      double* prev_a = s->td_prev[face][kind][0];
+      double* prev_b = s->td_prev[face][kind][1];
+      const double ds = s->d[a] * s->d[b];
+      for (int i = 0; i < n[0]; ++i)
+        for (int j = 0; j < n[1]; ++j)
+          for (int k = 0; k < n[2]; ++k) {
+            const size_t o = ((size_t)i * n[1] + j) * n[2] + k;
+            double r[3];
+            td_position(s, face, i, j, k, r);
+            const double delay = s->td_ref - (r[0] * s->td_dir[0] + r[1] * s->td_dir[1] + r[2] * s->td_dir[2]);
+            const double tsd = delay / (c0 * s->dt);
+            const long long nn = (long long)floor(tsd + off + (double)t);
+            const double f = tsd + off + (double)t - (double)nn;
+            const double av = interp(s, c, fa, i0 + i, j0 + j, k0 + k);
+            const double bv = interp(s, c, fb, i0 + i, j0 + j, k0 + k);
+            const double da = av - prev_a[o], db = bv - prev_b[o];
+            pa[nn] += ca * (1 - f) * ds * db;
+            pa[nn + 1] += ca * f * ds * db;
+            pb[nn] += cb * (1 - f) * ds * da;
+            pb[nn + 1] += cb * f * ds * da;
+            prev_a[o] = av;
+            prev_b[o] = bv;
+          }
+    }
+  }
+}
+
 static void record(orc_sim* s) {
   for (int m = 0; m < s->n_movies; ++m) {
     movie_t* mv = &s->movies[m];
@@ -533,6 +628,7 @@ static void record(orc_sim* s) {
     mv->count++;
   }
   nf2ff_update(s);
+  nf2ff_td_update(s);
   for (int p = 0; p < s->n_probes; ++p) {
     const int* d = s->probe + 4 * p;
     s->probe_out[(size_t)p * s->total + s->t] = AT(s->f[d[0]], d[1], d[2], d[3]);
@@ -563,6 +659,8 @@ double* orc_field_mut(orc_sim* s, int f) { return s->f[f].d; }
 const double* orc_probe(const orc_sim* s, int p) { return s->probe_out + (size_t)p * s->total; }
 const double* orc_movie(const orc_sim* s, int m) { return s->movies[m].data; }
 const double* orc_nf2ff(const orc_sim* s, int fq, int face, int w) { return s->acc[fq][face][w]; }
+const double* orc_nf2ff_td(const orc_sim* s, int which) { return s->td_on ? s->td_pot[which] : NULL; }
+long long orc_nf2ff_td_bins(const orc_sim* s) { return s->td_on ? s->td_bins : 0; }
 long long orc_step(const orc_sim* s) { return s->t; }
 const double* orc_e_inc(const orc_sim* s) { return s->e_inc; }
 const double* orc_h_inc(const orc_sim* s) { return s->h_inc; }
@@ -585,6 +683,12 @@ void orc_destroy(orc_sim* s) {
     for (int fq = 0; fq < s->nfreq && fq < 64; ++fq)
       for (int face = 0; face < 6; ++face)
         for (int w = 0; w < 4; ++w) free(s->acc[fq][face][w]);
+  if (s->td_on) {
+    for (int q = 0; q < 6; ++q) free(s->td_pot[q]);
+    for (int face = 0; face < 6; ++face)
+      for (int kind = 0; kind < 2; ++kind)
+        for (int w = 0; w < 2; ++w) free(s->td_prev[face][kind][w]);
+  }
   free(s->probe); free(s->probe_out);
   for (int m = 0; m < s->n_movies; ++m) free(s->movies[m].data);
   free(s->movies);

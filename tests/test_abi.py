@@ -32,7 +32,7 @@ def test_every_declared_symbol_is_exported_and_bound():
 
 def test_status_strings_and_version():
     lib = L.load()
-    assert lib.xfb_abi_version() == 1
+    assert lib.xfb_abi_version() == 2
     for s in range(9):
         assert lib.xfb_status_string(s)
     assert lib.xfb_status_string(99) == b"unknown status"

@@ -1,0 +1,54 @@
+"""FP32 accuracy at the full-size workloads, and the FP64 engine against the
+CPU restatement at full size.
+
+The north-star bar is a relative L2 error of at most 1e-4 on the far-field
+and probe outputs of the FP32 engine against the FP64 oracle.  At full size
+(C1: 156^3 x 2400 steps; C3: 408^3 x 6000 steps) the FP64 reference run is
+the FP64 engine, which is bit-identical to the CPU restatement: the last test
+shows that on the whole C1 run (about two minutes of CPU on the host).
+"""
+import numpy as np
+import pytest
+
+import xfdtd_cuda_b200 as X
+from xfdtd_cuda_b200 import accuracy
+
+pytestmark = pytest.mark.gpu
+
+BAR = 1e-4  # relative L2, far field and probes
+
+
+def test_fp32_dielectric_sphere_full_size():
+    r = accuracy.fp32_vs_fp64("dielectric", 2400)
+    print(r)
+    assert r["probes"] <= BAR, r
+    assert r["far_field_worst"] <= BAR, r
+
+
+def test_fp32_dispersive_sphere_full_size():
+    r = accuracy.fp32_vs_fp64("dispersive", 6000)
+    print(r)
+    assert r["probes"] <= BAR, r
+    assert r["far_field_worst"] <= BAR, r
+
+
+def test_fp64_dielectric_sphere_full_size_bit_identical_to_oracle():
+    from oracle import OracleSim
+    steps = 2400
+    sim = accuracy.scene("dielectric", "fp64")
+    sc, keep = sim.lower()
+    h = X.Handle(sc, keep)
+    h.init(steps)
+    h.step(steps)
+    h.sync()
+    sc2, keep2 = accuracy.scene("dielectric", "fp64").lower()
+    o = OracleSim(X.Handle(sc2, keep2), steps)
+    o.run(steps)
+    for f in range(6):
+        assert np.array_equal(h.read_field(f), o.field(f)), f"field {f}"
+    for p in range(len(h.probe_desc)):
+        assert np.array_equal(h.read_probe(p), o.probe(p)), f"probe {p}"
+    for face in range(6):
+        for w in range(4):
+            assert np.array_equal(h.read_nf2ff(0, face, w), o.nf2ff(0, face, w)), f"nf2ff face {face} current {w}"
+    h.close()

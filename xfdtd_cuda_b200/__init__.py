@@ -9,7 +9,7 @@ from ._lib import XfbError  # noqa: F401
 from .simulation import (  # noqa: F401
     C_0, EPSILON_0, ETA_0, MU_0, EMF, Axis, Batch, Cube, Cylinder, DebyeMedium, DebyePole, DispersiveMaterial, DrudeMedium,
     DrudePole, ElectroMagneticProperty, FieldMonitor, Handle, LorentzMedium, LorentzPole, Material, MLorentzMaterial,
-    MLorentzPole, MovieMonitor, NFFFTFrequencyDomain, Object, PML, PointMonitor, Simulation, SimulationHD, Sphere,
+    MLorentzPole, MovieMonitor, NFFFTFrequencyDomain, NFFFTTimeDomain, Object, PML, PointMonitor, Simulation, SimulationHD, Sphere,
     TFSF2D, TFSF3D, Vector, Waveform,
 )
 

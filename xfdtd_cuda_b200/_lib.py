@@ -62,6 +62,10 @@ class Nf2ff(C.Structure):
     _fields_ = [("enabled", C.c_int), ("inset", C.c_int * 3), ("n_freqs", C.c_int), ("freqs", C.POINTER(C.c_double))]
 
 
+class Nf2ffTd(C.Structure):
+    _fields_ = [("enabled", C.c_int), ("inset", C.c_int * 3), ("theta", C.c_double), ("phi", C.c_double)]
+
+
 class Probe(C.Structure):
     _fields_ = [("field", C.c_int), ("index", C.c_int * 3)]
 
@@ -80,6 +84,7 @@ class Scene(C.Structure):
         ("pml", Pml), ("tfsf", Tfsf), ("nf2ff", Nf2ff),
         ("n_probes", C.c_int), ("probes", C.POINTER(Probe)),
         ("n_movies", C.c_int), ("movies", C.POINTER(Movie)),
+        ("nf2ff_td", Nf2ffTd),
     ]
 
 
@@ -91,6 +96,7 @@ class GridInfo(C.Structure):
         ("tfsf_box", C.c_int * 6), ("nf2ff_box", C.c_int * 6), ("n_freqs", C.c_int),
         ("current_step", C.c_longlong), ("total_steps", C.c_longlong), ("device_bytes", C.c_size_t),
         ("n_dispersive_cells", C.c_longlong), ("launches_per_step", C.c_int), ("kernel_path", C.c_int),
+        ("nf2ff_td_box", C.c_int * 6), ("h2d_bytes", C.c_longlong), ("d2h_bytes", C.c_longlong),
     ]
 
 
@@ -113,6 +119,8 @@ class CompiledView(C.Structure):
         ("aux_source", _dp), ("total_steps", C.c_longlong),
         ("nf2ff_enabled", C.c_int), ("nf2ff_box", C.c_int * 6), ("n_freqs", C.c_int), ("freqs", _dp),
         ("nf2ff_te", _dp), ("nf2ff_th", _dp),
+        ("nf2ff_td_enabled", C.c_int), ("nf2ff_td_box", C.c_int * 6), ("nf2ff_td_theta", C.c_double),
+        ("nf2ff_td_phi", C.c_double), ("nf2ff_td_bins", C.c_longlong), ("origin", C.c_double * 3),
     ]
 
 
@@ -130,6 +138,7 @@ SIGNATURES = [
     ("xfb_run", C.c_int, [_H, C.c_longlong]),
     ("xfb_step", C.c_int, [_H, C.c_longlong]),
     ("xfb_sync", C.c_int, [_H]),
+    ("xfb_set_wait_limit", C.c_int, [_H, C.c_int]),
     ("xfb_timed_step", C.c_int, [_H, C.c_longlong, C.POINTER(C.c_double)]),
     ("xfb_profile_kernels", C.c_int, [_H, C.c_longlong, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
     ("xfb_set_graph", C.c_int, [_H, C.c_int, C.c_int]),
@@ -144,6 +153,9 @@ SIGNATURES = [
     ("xfb_read_nf2ff", C.c_int, [_H, C.c_int, C.c_int, C.c_int, _dp, C.c_size_t]),
     ("xfb_far_field", C.c_int, [_H, C.c_int, C.c_int, _dp, _dp, _dp]),
     ("xfb_far_field_static", C.c_int, [_H, C.c_int, C.c_int, _dp, _dp, _dp]),
+    ("xfb_nf2ff_td_bins", C.c_int, [_H, C.POINTER(C.c_longlong)]),
+    ("xfb_read_nf2ff_td", C.c_int, [_H, C.c_int, _dp, C.c_size_t]),
+    ("xfb_far_field_td", C.c_int, [_H, _dp, _dp, C.c_size_t]),
     ("xfb_mlp_param_count", C.c_int, []),
     ("xfb_mlp_loss_grad", C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_float),
                                     C.POINTER(C.c_double), C.POINTER(C.c_float)]),
@@ -157,6 +169,7 @@ SIGNATURES = [
     ("xfb_batch_init", C.c_int, [C.c_void_p, C.c_longlong]),
     ("xfb_batch_step", C.c_int, [C.c_void_p, C.c_longlong]),
     ("xfb_batch_sync", C.c_int, [C.c_void_p]),
+    ("xfb_batch_set_wait_limit", C.c_int, [C.c_void_p, C.c_int]),
     ("xfb_batch_timed_step", C.c_int, [C.c_void_p, C.c_longlong, C.POINTER(C.c_double)]),
     ("xfb_batch_info", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("xfb_batch_last_error", C.c_char_p, [C.c_void_p]),

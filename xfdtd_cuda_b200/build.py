@@ -53,7 +53,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     for unit, fmad in UNITS:
         obj = objdir / (unit + ".o")
         cmd = [nvcc(), "-O3", "-std=c++17", *ARCH, "-lineinfo", f"--fmad={'true' if fmad else 'false'}",
-               "-Xcompiler", "-fPIC,-O3", "-I", str(ROOT / "include"), "-c", "-o", str(obj), str(CSRC / unit)]
+               "-Xcompiler", "-fPIC,-O3,-fopenmp", "-I", str(ROOT / "include"), "-c", "-o", str(obj), str(CSRC / unit)]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
             print(" ".join(cmd))
@@ -66,7 +66,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
             raise RuntimeError(f"nvcc failed on {unit}")
         if verbose:
             sys.stderr.write(err)
-    cmd = [nvcc(), "-shared", "-cudart", "static", *ARCH, "-o", str(tmp), *[str(o) for o in objs]]
+    cmd = [nvcc(), "-shared", "-cudart", "static", *ARCH, "-o", str(tmp), *[str(o) for o in objs], "-lgomp"]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         sys.stderr.write(res.stdout + res.stderr)

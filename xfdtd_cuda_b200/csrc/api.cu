@@ -59,6 +59,13 @@ void free_device(xfb_handle* h) {
   h->step_err = nullptr;
   h->ade_runs = nullptr;
   h->n_ade_runs = -1;
+  h->rb_dev = nullptr;  // one of bufs
+  for (int q = 0; q < 2; ++q) {
+    if (h->rb_host[q]) cudaFreeHost(h->rb_host[q]);
+    if (h->rb_ev[q]) cudaEventDestroy(h->rb_ev[q]);
+    h->rb_host[q] = nullptr;
+    h->rb_ev[q] = nullptr;
+  }
   h->inited = false;
 }
 
@@ -84,6 +91,8 @@ int copy(xfb_handle* h, void* dst, const void* src, size_t bytes, cudaMemcpyKind
   if (bytes == 0) return XFB_OK;
   XFB_CUDA(h, cudaMemcpyAsync(dst, src, bytes, kind, h->stream));
   XFB_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (kind == cudaMemcpyHostToDevice) h->h2d_bytes += static_cast<long long>(bytes);
+  if (kind == cudaMemcpyDeviceToHost) h->d2h_bytes += static_cast<long long>(bytes);
   return XFB_OK;
 }
 
@@ -116,14 +125,14 @@ int launches_per_step(const xfb_handle* h) {
   if (plain(h)) {
     int faces = 0;
     for (int f = 0; f < 6; ++f) faces += c.pml[f] > 0;
-    return 6 + 2 * faces + (c.tfsf_on ? 24 : 0) + (c.nf_on ? 1 : 0) + (c.probes.empty() ? 0 : 1) +
+    return 6 + 2 * faces + (c.tfsf_on ? 24 : 0) + (c.nf_on ? 1 : 0) + (c.td_on ? 2 : 0) + (c.probes.empty() ? 0 : 1) +
            static_cast<int>(c.movies.size());
   }
   int bulk = 2;
   if (fused(h)) {
     bulk = c.dim == 2 ? 1 : (h->n_step_items[step_tile_index(h->tj)] > 0 ? 1 : 0) + (h->ade_deferred ? 1 : 0);
   }
-  return bulk + (c.nf_on ? 1 : 0) + (c.probes.empty() ? 0 : 1) +
+  return bulk + (c.nf_on ? 1 : 0) + (c.td_on ? 2 : 0) + (c.probes.empty() ? 0 : 1) +
          static_cast<int>(c.movies.size());
 }
 
@@ -347,18 +356,37 @@ int xfb_step(xfb_handle* h, long long n) {
   return h->c.prec == XFB_FP64 ? run_steps<double>(h, n) : run_steps<float>(h, n);
 }
 
-int xfb_sync(xfb_handle* h) {
-  int rc = check_handle(h, true);
-  if (rc) return rc;
+// Waits for the handle's stream and reads the step kernel's error flag: a
+// staging wait that ran out makes every later sync and read-back of the run
+// return XFB_ERR_TIMEOUT (the step's results are incomplete) until the next
+// xfb_init.
+static int step_status(xfb_handle* h) {
   XFB_CUDA(h, cudaStreamSynchronize(h->stream));
   XFB_CUDA(h, cudaGetLastError());
   if (h->step_err) {
     int e = 0;
     XFB_CUDA(h, cudaMemcpyAsync(&e, h->step_err, sizeof(e), cudaMemcpyDeviceToHost, h->stream));
     XFB_CUDA(h, cudaStreamSynchronize(h->stream));
-    if (e) return set_err(h, XFB_ERR_CUDA, "one-sweep step: a staging copy did not complete (wait limit reached)");
+    if (e)
+      return set_err(h, XFB_ERR_TIMEOUT,
+                     "one-sweep step: a staging copy did not complete within the wait limit; the run's results "
+                     "are incomplete (xfb_init starts it over)");
   }
   return XFB_OK;
+}
+
+int xfb_sync(xfb_handle* h) {
+  int rc = check_handle(h, true);
+  if (rc) return rc;
+  return step_status(h);
+}
+
+int xfb_set_wait_limit(xfb_handle* h, int polls) {
+  int rc = check_handle(h, true);
+  if (rc || (rc = not_batched(h))) return rc;
+  if (polls < 0) return set_err(h, XFB_ERR_INVALID, "negative poll limit");
+  if (!h->step_err) return set_err(h, XFB_ERR_STATE, "only the 3-D one-sweep step has bounded waits");
+  return copy(h, h->step_err + 1, &polls, sizeof(int), cudaMemcpyHostToDevice);
 }
 
 int xfb_timed_step(xfb_handle* h, long long n, double* ms) {
@@ -421,6 +449,9 @@ int xfb_get_grid_info(const xfb_handle* h, xfb_grid_info* o) {
   o->n_dispersive_cells = nd;
   o->launches_per_step = launches_per_step(h);
   o->kernel_path = h->path;
+  o->h2d_bytes = h->h2d_bytes;
+  o->d2h_bytes = h->d2h_bytes;
+  if (c.td_on) for (int q = 0; q < 6; ++q) o->nf2ff_td_box[q] = c.td[q];
   return XFB_OK;
 }
 
@@ -432,6 +463,7 @@ int xfb_read_field(xfb_handle* h, int f, double* dst, size_t len) {
   int s[3];
   comp_shape(h->c, f, s);
   if (len < static_cast<size_t>(s[0]) * s[1] * s[2]) return set_err(h, XFB_ERR_RANGE, "destination too small");
+  if (!h->batch && (rc = step_status(h))) return rc;
   return h->c.prec == XFB_FP64 ? read_field_t<double>(h, f, dst) : read_field_t<float>(h, f, dst);
 }
 
@@ -452,7 +484,7 @@ int xfb_read_probe(xfb_handle* h, int id, double* dst, size_t len, long long* n_
   if (id < 0 || id >= static_cast<int>(h->c.probes.size())) return set_err(h, XFB_ERR_RANGE, "probe id out of range");
   const long long n = h->step;
   if (len < static_cast<size_t>(n)) return set_err(h, XFB_ERR_RANGE, "destination too small");
-  XFB_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (!h->batch && (rc = step_status(h))) return rc;
   if (n > 0 && (rc = copy(h, dst, h->probe_out + id * h->c.total_steps, n * sizeof(double), cudaMemcpyDeviceToHost))) return rc;
   if (n_written) *n_written = n;
   return XFB_OK;
@@ -474,7 +506,7 @@ int xfb_read_movie(xfb_handle* h, int id, double* dst, size_t len) {
   if ((rc = xfb_movie_shape(h, id, s))) return rc;
   const size_t n = static_cast<size_t>(s[0]) * s[1] * s[2] * s[3];
   if (len < n) return set_err(h, XFB_ERR_RANGE, "destination too small");
-  XFB_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (!h->batch && (rc = step_status(h))) return rc;
   if (n && (rc = copy(h, dst, h->movie_out[id], n * sizeof(double), cudaMemcpyDeviceToHost))) return rc;
   return XFB_OK;
 }
@@ -522,7 +554,7 @@ int xfb_read_nf2ff(xfb_handle* h, int freq, int face, int which, double* dst, si
   const size_t n = static_cast<size_t>(s[0]) * s[1] * s[2];
   if (len < 2 * n) return set_err(h, XFB_ERR_RANGE, "destination too small (complex interleaved)");
   if ((rc = nf2ff_flush(h))) return rc;
-  XFB_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (!h->batch && (rc = step_status(h))) return rc;
   const double2* src = h->nf_acc + (static_cast<long long>(freq) * 4 + which) * h->nf_npts + h->nf_off[face];
   if ((rc = copy(h, dst, src, n * sizeof(double2), cudaMemcpyDeviceToHost))) return rc;
   return XFB_OK;
@@ -536,12 +568,22 @@ int xfb_far_field(xfb_handle* h, int freq, int n, const double* theta, const dou
   if (n < 0 || (n > 0 && (!theta || !phi || !out))) return set_err(h, XFB_ERR_INVALID, "bad angle arrays");
   if (n == 0) return XFB_OK;
   if ((rc = nf2ff_flush(h))) return rc;
-  double *d_th = nullptr, *d_ph = nullptr, *d_out = nullptr;
-  XFB_CUDA(h, cudaMalloc(&d_th, n * sizeof(double)));
-  XFB_CUDA(h, cudaMalloc(&d_ph, n * sizeof(double)));
-  XFB_CUDA(h, cudaMalloc(&d_out, 4 * n * sizeof(double)));
-  cudaMemcpyAsync(d_th, theta, n * sizeof(double), cudaMemcpyHostToDevice, h->stream);
-  cudaMemcpyAsync(d_ph, phi, n * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+  // angle and output buffers of this call, released on every return path
+  // (after the stream has finished with them)
+  struct Scratch {
+    xfb_handle* h;
+    double* p[3] = {nullptr, nullptr, nullptr};
+    ~Scratch() {
+      cudaStreamSynchronize(h->stream);
+      for (double* q : p) cudaFree(q);
+    }
+  } sb{h};
+  XFB_CUDA(h, cudaMalloc(&sb.p[0], n * sizeof(double)));
+  XFB_CUDA(h, cudaMalloc(&sb.p[1], n * sizeof(double)));
+  XFB_CUDA(h, cudaMalloc(&sb.p[2], 4 * n * sizeof(double)));
+  double *d_th = sb.p[0], *d_ph = sb.p[1], *d_out = sb.p[2];
+  XFB_CUDA(h, cudaMemcpyAsync(d_th, theta, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  XFB_CUDA(h, cudaMemcpyAsync(d_ph, phi, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   FarP fp{};
   const Compiled& c = h->c;
   for (int q = 0; q < 6; ++q) fp.box[q] = c.nf[q];
@@ -554,10 +596,9 @@ int xfb_far_field(xfb_handle* h, int freq, int n, const double* theta, const dou
   fp.eta = std::sqrt(kMu0 / kEps0);
   fp.theta = d_th; fp.phi = d_ph; fp.out = d_out;
   k_far<<<n, 256, 0, h->stream>>>(fp);
-  cudaError_t e = cudaMemcpyAsync(out, d_out, 4 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-  cudaFree(d_th); cudaFree(d_ph); cudaFree(d_out);
-  if (e != cudaSuccess) return cuda_err(h, e, "far-field kernel");
+  XFB_CUDA(h, cudaGetLastError());
+  XFB_CUDA(h, cudaMemcpyAsync(out, d_out, 4 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  XFB_CUDA(h, cudaStreamSynchronize(h->stream));
   return XFB_OK;
 }
 
@@ -595,6 +636,48 @@ int xfb_far_field_static(xfb_handle* h, int freq, int n, const double* theta, co
   XFB_CUDA(h, cudaGetLastError());
   XFB_CUDA(h, cudaMemcpyAsync(out, d_out, 4 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   XFB_CUDA(h, cudaStreamSynchronize(h->stream));
+  return XFB_OK;
+}
+
+int xfb_nf2ff_td_bins(const xfb_handle* h, long long* n_bins) {
+  if (!h || !n_bins) return set_err(nullptr, XFB_ERR_INVALID, "null argument");
+  if (!h->c.td_on) return set_err(const_cast<xfb_handle*>(h), XFB_ERR_STATE, "scene has no time-domain NF2FF box");
+  *n_bins = h->c.td_bins;
+  return XFB_OK;
+}
+
+int xfb_read_nf2ff_td(xfb_handle* h, int which, double* dst, size_t len) {
+  int rc = check_handle(h, true);
+  if (rc) return rc;
+  if (!h->c.td_on) return set_err(h, XFB_ERR_STATE, "scene has no time-domain NF2FF box");
+  if (which < 0 || which > 5 || !dst) return set_err(h, XFB_ERR_INVALID, "potential index must be 0..5 (W_x..U_z)");
+  const size_t n = static_cast<size_t>(h->c.td_bins);
+  if (len < n) return set_err(h, XFB_ERR_RANGE, "destination too small");
+  if (!h->batch && (rc = step_status(h))) return rc;
+  if (h->batch) XFB_CUDA(h, cudaStreamSynchronize(h->batch->stream));
+  return copy(h, dst, h->td_pot + static_cast<size_t>(which) * n, n * sizeof(double), cudaMemcpyDeviceToHost);
+}
+
+int xfb_far_field_td(xfb_handle* h, double* e_theta, double* e_phi, size_t len) {
+  int rc = check_handle(h, true);
+  if (rc) return rc;
+  if (!h->c.td_on) return set_err(h, XFB_ERR_STATE, "scene has no time-domain NF2FF box");
+  const size_t n = static_cast<size_t>(h->c.td_bins);
+  if (!e_theta || !e_phi || len < n) return set_err(h, XFB_ERR_RANGE, "destination too small");
+  std::vector<double> p(6 * n);
+  for (int q = 0; q < 6; ++q)
+    if ((rc = xfb_read_nf2ff_td(h, q, p.data() + q * n, n))) return rc;
+  const double th = h->c.td_theta, ph = h->c.td_phi;
+  const double st = std::sin(th), ct = std::cos(th), sp = std::sin(ph), cp = std::cos(ph);
+  const double eta = std::sqrt(kMu0 / kEps0);
+  const double f = 1.0 / (4 * kPi * kTdC0 * h->c.dt);
+  for (size_t b = 0; b < n; ++b) {
+    const double wx = p[b], wy = p[n + b], wz = p[2 * n + b], ux = p[3 * n + b], uy = p[4 * n + b], uz = p[5 * n + b];
+    const double w_th = wx * ct * cp + wy * ct * sp - wz * st, w_ph = -wx * sp + wy * cp;
+    const double u_th = ux * ct * cp + uy * ct * sp - uz * st, u_ph = -ux * sp + uy * cp;
+    e_theta[b] = -f * (u_ph + eta * w_th);
+    e_phi[b] = f * (u_th - eta * w_ph);
+  }
   return XFB_OK;
 }
 
@@ -697,6 +780,12 @@ int xfb_compiled_view_get(const xfb_handle* h, xfb_compiled_view* v) {
   v->freqs = c.freqs.data();
   v->nf2ff_te = c.te.data();
   v->nf2ff_th = c.th.data();
+  v->nf2ff_td_enabled = c.td_on;
+  for (int q = 0; q < 6; ++q) v->nf2ff_td_box[q] = c.td[q];
+  v->nf2ff_td_theta = c.td_theta;
+  v->nf2ff_td_phi = c.td_phi;
+  v->nf2ff_td_bins = c.td_bins;
+  for (int a = 0; a < 3; ++a) v->origin[a] = c.origin[a];
   return XFB_OK;
 }
 
@@ -838,8 +927,22 @@ int xfb_batch_sync(xfb_batch* b) {
     int flag = 0;
     e = cudaMemcpy(&flag, b->err_dev, sizeof(int), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return batch_err(b, XFB_ERR_CUDA, cudaGetErrorString(e));
-    if (flag) return batch_err(b, XFB_ERR_CUDA, "batch step: a staging copy did not complete (wait limit reached)");
+    if (flag)
+      return batch_err(b, XFB_ERR_TIMEOUT,
+                       "batch step: a staging copy did not complete within the wait limit; the batch's results are "
+                       "incomplete (xfb_batch_init starts it over)");
   }
+  return XFB_OK;
+}
+
+int xfb_batch_set_wait_limit(xfb_batch* b, int polls) {
+  if (!b) return set_err(nullptr, XFB_ERR_INVALID, "null batch");
+  if (!b->inited) return batch_err(b, XFB_ERR_STATE, "batch not initialised");
+  if (polls < 0) return batch_err(b, XFB_ERR_INVALID, "negative poll limit");
+  cudaSetDevice(b->device);
+  cudaError_t e = cudaMemcpyAsync(b->err_dev + 1, &polls, sizeof(int), cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return batch_err(b, XFB_ERR_CUDA, cudaGetErrorString(e));
   return XFB_OK;
 }
 

@@ -5,6 +5,7 @@
 #pragma once
 
 #include <cudaTypedefs.h>  // PFN_cuTensorMapEncodeTiled
+#include <omp.h>
 
 #include <algorithm>
 #include <cstring>
@@ -19,6 +20,7 @@ namespace xfb {
 
 inline int upload_step_items(xfb_handle* h);
 inline int upload_ade_runs(xfb_handle* h);
+inline int upload_td(xfb_handle* h);
 template <typename T>
 int encode_stage_maps(xfb_handle* h);
 
@@ -52,6 +54,7 @@ int init_device(xfb_handle* h) {
   // material ids in the padded layout
   {
     std::vector<uint8_t> m(static_cast<size_t>(h->elems), 0);
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < nx; ++i)
       for (int j = 0; j < ny; ++j)
         std::memcpy(m.data() + i * h->sx + j * h->sy, c.mat_id.data() + (static_cast<size_t>(i) * ny + j) * nz, nz);
@@ -66,9 +69,11 @@ int init_device(xfb_handle* h) {
   if (fused(h) && c.dim == 3 && h->ade_deferred && (rc = upload_ade_runs(h))) return rc;
   if (fused(h) && c.dim == 3) {
     if ((rc = encode_stage_maps<T>(h))) return rc;
-    void* p;
-    if ((rc = alloc(h, &p, sizeof(int), false))) return rc;
+    void* p;  // error word pair: flag, poll limit of the staging waits
+    if ((rc = alloc(h, &p, 2 * sizeof(int), false))) return rc;
     h->step_err = static_cast<int*>(p);
+    const int words[2] = {0, kWaitPolls};
+    if ((rc = copy(h, p, words, sizeof(words), cudaMemcpyHostToDevice))) return rc;
   }
   if (plain(h)) {  // per-cell coefficient arrays, expanded from the LUT on the device
     PlainCoef<T> pc;
@@ -173,6 +178,7 @@ int init_device(xfb_handle* h) {
     if ((rc = upload<double>(h, &p, c.th))) return rc;
     h->th = static_cast<double2*>(p);
   }
+  if (c.td_on && (rc = upload_td(h))) return rc;
   // probes
   if (!c.probes.empty()) {
     const size_t n = c.probes.size();
@@ -489,6 +495,107 @@ int encode_stage_maps(xfb_handle* h) {
   return XFB_OK;
 }
 
+// Tables of the time-domain NF2FF: the sample points of every (face, field
+// kind), sorted by bin offset d0 = floor(delay + off) (off = 1/2 for E, 0
+// for H) and cut into chunks of at most kTdChunk points with one d0; for
+// every (component, bin offset w) of a step's window, the chunk slots that
+// land there (CSR, chunk order).  Component of a chunk's slot s: W (kind H)
+// or U (kind E) along the face's tangential axis a (s < 3) or b (s >= 3), at
+// bin offset d0 + s % 3.
+struct TdTables {
+  std::vector<int4> ent, chunk;
+  std::vector<double> tsd;
+  std::vector<int> offs, list;
+};
+
+inline void build_td_tables(const Compiled& c, TdTables& tb) {
+  tb = TdTables{};
+  for (int face = 0; face < 6; ++face)
+    for (int kind = 0; kind < 2; ++kind) {
+      const FaceGeom g = td_face_geom(c, face);
+      const double off = kind ? 0.0 : 0.5;
+      std::map<int, std::vector<std::pair<int4, double>>> by_d0;
+      for (int i = g.i0; i < g.i0 + g.ni; ++i)
+        for (int j = g.j0; j < g.j0 + g.nj; ++j)
+          for (int k = g.k0; k < g.k0 + g.nk; ++k) {
+            const double tsd = td_delay_steps(c, face, i, j, k);
+            by_d0[static_cast<int>(std::floor(tsd + off))].push_back({make_int4(i, j, k, face * 2 + kind), tsd});
+          }
+      for (auto& kv : by_d0)
+        for (size_t q0 = 0; q0 < kv.second.size(); q0 += kTdChunk) {
+          const size_t q1 = std::min(kv.second.size(), q0 + kTdChunk);
+          tb.chunk.push_back(make_int4(static_cast<int>(tb.ent.size()), static_cast<int>(q1 - q0), face * 2 + kind, kv.first));
+          for (size_t q = q0; q < q1; ++q) {
+            tb.ent.push_back(kv.second[q].first);
+            tb.tsd.push_back(kv.second[q].second);
+          }
+        }
+    }
+  const int span = c.td_span;
+  std::vector<std::vector<int>> cells(static_cast<size_t>(6) * span);
+  for (size_t q = 0; q < tb.chunk.size(); ++q) {
+    const int4 ch = tb.chunk[q];
+    const int face = ch.z >> 1, kind = ch.z & 1, ax = face >> 1;
+    const int base = kind ? 0 : 3, ca = (ax + 1) % 3, cb = (ax + 2) % 3;
+    for (int slot = 0; slot < 6; ++slot) {
+      const int comp = base + (slot < 3 ? ca : cb), w = ch.w + slot % 3;
+      cells[static_cast<size_t>(comp) * span + w].push_back(static_cast<int>(q) * 6 + slot);
+    }
+  }
+  tb.offs.assign(1, 0);
+  for (const auto& v : cells) {
+    tb.list.insert(tb.list.end(), v.begin(), v.end());
+    tb.offs.push_back(static_cast<int>(tb.list.size()));
+  }
+}
+
+inline int upload_td(xfb_handle* h) {
+  TdTables tb;
+  build_td_tables(h->c, tb);
+  h->td_n = static_cast<long long>(tb.ent.size());
+  h->td_nchunks = static_cast<int>(tb.chunk.size());
+  void* p;
+  int rc;
+  if ((rc = alloc(h, &h->td_ent, tb.ent.size() * sizeof(int4), false))) return rc;
+  if ((rc = copy(h, h->td_ent, tb.ent.data(), tb.ent.size() * sizeof(int4), cudaMemcpyHostToDevice))) return rc;
+  if ((rc = upload<double>(h, &p, tb.tsd))) return rc;
+  h->td_tsd = static_cast<double*>(p);
+  if ((rc = alloc(h, &p, 2 * tb.ent.size() * sizeof(double), true))) return rc;
+  h->td_prev = static_cast<double*>(p);
+  if ((rc = alloc(h, &h->td_chunk, tb.chunk.size() * sizeof(int4), false))) return rc;
+  if ((rc = copy(h, h->td_chunk, tb.chunk.data(), tb.chunk.size() * sizeof(int4), cudaMemcpyHostToDevice))) return rc;
+  if ((rc = alloc(h, &p, tb.chunk.size() * 6 * sizeof(double), false))) return rc;
+  h->td_part = static_cast<double*>(p);
+  if ((rc = alloc(h, &p, tb.offs.size() * sizeof(int), false))) return rc;
+  h->td_offs = static_cast<int*>(p);
+  if ((rc = copy(h, p, tb.offs.data(), tb.offs.size() * sizeof(int), cudaMemcpyHostToDevice))) return rc;
+  if ((rc = alloc(h, &p, std::max<size_t>(1, tb.list.size()) * sizeof(int), false))) return rc;
+  h->td_list = static_cast<int*>(p);
+  if ((rc = copy(h, p, tb.list.data(), tb.list.size() * sizeof(int), cudaMemcpyHostToDevice))) return rc;
+  if ((rc = alloc(h, &p, 6 * static_cast<size_t>(std::max(1LL, h->c.td_bins)) * sizeof(double), true))) return rc;
+  h->td_pot = static_cast<double*>(p);
+  return XFB_OK;
+}
+
+inline TdP td_params(const xfb_handle* h) {
+  TdP td{};
+  td.ent = static_cast<const int4*>(h->td_ent);
+  td.tsd = h->td_tsd;
+  td.prev = h->td_prev;
+  td.n = h->td_n;
+  td.chunk = static_cast<const int4*>(h->td_chunk);
+  td.part = h->td_part;
+  td.offs = h->td_offs;
+  td.list = h->td_list;
+  td.span = h->c.td_span;
+  td.pot = h->td_pot;
+  td.bins = h->c.td_bins;
+  td.ds[0] = h->c.dy * h->c.dz;
+  td.ds[1] = h->c.dz * h->c.dx;
+  td.ds[2] = h->c.dx * h->c.dy;
+  return td;
+}
+
 inline int upload_step_items(xfb_handle* h) {
   h->ade_deferred = ade_can_defer(h->c);
   for (int t = 0; t < 2; ++t) {
@@ -719,6 +826,13 @@ void enqueue_records(xfb_handle* h, int parity, TimeP tp, cudaStream_t s, Prof* 
     k_nf2ff<T><<<static_cast<unsigned>((h->nf_npts + 255) / 256), 256, 0, s>>>(g, nf, tp);
     prof_end(h, pf);
   }
+  if (c.td_on && h->td_nchunks > 0) {
+    const TdP td = td_params(h);
+    prof_begin(h, pf, XFB_K_NF2FF);
+    k_nftd_chunks<T><<<h->td_nchunks, kTdChunk, 0, s>>>(g, td, tp);
+    k_nftd_bins<<<(6 * td.span + 127) / 128, 128, 0, s>>>(td, tp);
+    prof_end(h, pf);
+  }
   if (!c.probes.empty()) {
     ProbeP pr{static_cast<int>(c.probes.size()), h->probe_idx, h->probe_field, h->probe_out, c.total_steps};
     prof_begin(h, pf, XFB_K_PROBE);
@@ -873,53 +987,102 @@ int profile_steps(xfb_handle* h, long long n, double* ms, long long* launches) {
 
 
 
-// Component f in the reference's dense layout, as doubles: the cells of
-// planes [i0, i0 + n / (s1 * s2)) gathered out of the padded layout (src
-// points at plane i0), one thread per cell.
+// Component f in the reference's dense layout, in the compute type: the
+// component elements [q0, q0 + n) of the dense (i, j, k) order (s1 x s2
+// elements per plane) gathered out of the padded layout, one thread per
+// element.
 template <typename T>
-__global__ void k_gather_field(const T* src, double* dst, long long sx, long long sy, int s1, int s2, long long n) {
+__global__ void k_gather_field(const T* src, T* dst, long long sx, long long sy, int s1, int s2, long long q0,
+                               long long n) {
   for (long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; q < n;
        q += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const long long ij = q / s2;
+    const long long e = q0 + q;
+    const long long ij = e / s2;
     const long long i = ij / s1;
-    const long long j = ij - i * s1, k = q - ij * s2;
-    dst[q] = static_cast<double>(src[i * sx + j * sy + k]);
+    const long long j = ij - i * s1, k = e - ij * s2;
+    dst[q] = src[i * sx + j * sy + k];
   }
 }
 
-// Read-back of component f: gathered on the device in chunks of whole planes
-// (a staging buffer of at most 32 Mi doubles), each chunk copied straight into
-// the caller's array; the host-side gather below when the staging buffer
-// cannot be allocated.
+// Elements of one read-back chunk (device gather buffer and each pinned host
+// buffer hold this many elements of the compute type).
+constexpr long long kReadChunk = 4LL << 20;
+
+// dst[q] = double(src[q]) for q < n, split over the host threads.
+template <typename T>
+void widen_to_double(const T* src, double* dst, long long n) {
+  const int threads = std::max(1, std::min(16, omp_get_max_threads()));
+#pragma omp parallel for schedule(static) num_threads(threads)
+  for (long long q = 0; q < n; ++q) dst[q] = static_cast<double>(src[q]);
+}
+
+// Read-back buffers of the handle (device gather buffer, two pinned host
+// buffers, their events), allocated on first use and kept until the next
+// init or destroy.  False when any allocation fails.
+template <typename T>
+bool readback_buffers(xfb_handle* h) {
+  if (h->rb_dev && h->rb_host[0] && h->rb_host[1]) return true;
+  const size_t bytes = static_cast<size_t>(kReadChunk) * sizeof(T);
+  if (!h->rb_dev && alloc(h, &h->rb_dev, bytes, false) != XFB_OK) return false;
+  for (int q = 0; q < 2; ++q) {
+    if (!h->rb_host[q] && cudaHostAlloc(&h->rb_host[q], bytes, cudaHostAllocDefault) != cudaSuccess) {
+      h->rb_host[q] = nullptr;
+      cudaGetLastError();
+      return false;
+    }
+    if (!h->rb_ev[q] && cudaEventCreateWithFlags(&h->rb_ev[q], cudaEventDisableTiming) != cudaSuccess) {
+      h->rb_ev[q] = nullptr;
+      cudaGetLastError();
+      return false;
+    }
+  }
+  return true;
+}
+
+// Read-back of component f into the caller's double array.  Chunks of
+// kReadChunk elements are gathered on the device in the compute type, copied
+// into pinned host buffer c & 1, and widened to double by host threads while
+// the device gathers and copies the next chunk.  The host-side gather below
+// runs when the read-back buffers cannot be allocated.
 template <typename T>
 int read_field_t(xfb_handle* h, int f, double* dst) {
-  {
-    int s[3];
-    comp_shape(h->c, f, s);
-    const long long plane = static_cast<long long>(s[1]) * s[2];
-    const long long chunk = std::max(1LL, std::min<long long>(s[0], (32LL << 20) / std::max(1LL, plane)));
-    double* stage = nullptr;
-    if (plane > 0 && cudaMalloc(&stage, static_cast<size_t>(chunk * plane) * sizeof(double)) == cudaSuccess) {
-      const T* src = static_cast<const T*>(field_ptr(h, cur_set(h), f));
-      int rc = XFB_OK;
-      for (long long i0 = 0; i0 < s[0] && !rc; i0 += chunk) {
-        const long long n = std::min<long long>(chunk, s[0] - i0) * plane;
-        const unsigned blocks = static_cast<unsigned>(std::min<long long>((n + 255) / 256, 148LL * 16));
-        k_gather_field<T><<<blocks, 256, 0, h->stream>>>(src + i0 * h->sx, stage, h->sx, h->sy, s[1], s[2], n);
-        const cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) rc = cuda_err(h, e, "k_gather_field");
-        else rc = copy(h, dst + i0 * plane, stage, static_cast<size_t>(n) * sizeof(double), cudaMemcpyDeviceToHost);
-      }
-      cudaFree(stage);
-      return rc;
+  int s[3];
+  comp_shape(h->c, f, s);
+  const long long total = static_cast<long long>(s[0]) * s[1] * s[2];
+  if (total == 0) return XFB_OK;
+  if (readback_buffers<T>(h)) {
+    const T* src = static_cast<const T*>(field_ptr(h, cur_set(h), f));
+    T* stage = static_cast<T*>(h->rb_dev);
+    const long long nch = (total + kReadChunk - 1) / kReadChunk;
+    auto enqueue = [&](long long c) -> cudaError_t {
+      const long long q0 = c * kReadChunk, n = std::min(kReadChunk, total - q0);
+      const unsigned blocks = static_cast<unsigned>(std::min<long long>((n + 255) / 256, 148LL * 16));
+      k_gather_field<T><<<blocks, 256, 0, h->stream>>>(src, stage, h->sx, h->sy, s[1], s[2], q0, n);
+      cudaError_t e = cudaGetLastError();
+      if (e == cudaSuccess) e = cudaMemcpyAsync(h->rb_host[c & 1], stage, n * sizeof(T), cudaMemcpyDeviceToHost, h->stream);
+      if (e == cudaSuccess) e = cudaEventRecord(h->rb_ev[c & 1], h->stream);
+      return e;
+    };
+    cudaError_t e = enqueue(0);
+    for (long long c = 0; c < nch && e == cudaSuccess; ++c) {
+      // host buffer (c + 1) & 1 was last read when chunk c - 1 was widened
+      if (c + 1 < nch) e = enqueue(c + 1);
+      if (e == cudaSuccess) e = cudaEventSynchronize(h->rb_ev[c & 1]);
+      if (e != cudaSuccess) break;
+      const long long q0 = c * kReadChunk, n = std::min(kReadChunk, total - q0);
+      widen_to_double(static_cast<const T*>(h->rb_host[c & 1]), dst + q0, n);
+      h->d2h_bytes += n * static_cast<long long>(sizeof(T));
     }
-    cudaGetLastError();  // allocation failed: gather on the host
+    if (e != cudaSuccess) {
+      cudaStreamSynchronize(h->stream);  // no copy into the host buffers stays in flight
+      return cuda_err(h, e, "field read-back");
+    }
+    return XFB_OK;
   }
+  h->err.clear();  // no read-back buffers: gather on the host
   std::vector<T> tmp(static_cast<size_t>(h->elems));
   int rc;
   if ((rc = copy(h, tmp.data(), field_ptr(h, cur_set(h), f), tmp.size() * sizeof(T), cudaMemcpyDeviceToHost))) return rc;
-  int s[3];
-  comp_shape(h->c, f, s);
   size_t o = 0;
   for (int i = 0; i < s[0]; ++i)
     for (int j = 0; j < s[1]; ++j)
@@ -1004,10 +1167,9 @@ int batch_init(xfb_batch* b) {
   int rc;
   if ((rc = batch_upload(b, &b->scenes, sc.data(), sc.size() * sizeof(BatchScene<T>)))) return rc;
   if ((rc = batch_upload(b, &b->maps, mp.data(), mp.size() * sizeof(BatchMaps)))) return rc;
-  {
-    cudaError_t e = cudaMalloc(&b->err_dev, sizeof(int));
-    if (e == cudaSuccess) e = cudaMemsetAsync(b->err_dev, 0, sizeof(int), b->stream);
-    if (e != cudaSuccess) return batch_err(b, XFB_ERR_CUDA, cudaGetErrorString(e));
+  {  // error word pair: flag, poll limit of the staging waits
+    static const int words[2] = {0, kWaitPolls};
+    if ((rc = batch_upload(b, reinterpret_cast<void**>(&b->err_dev), words, sizeof(words)))) return rc;
   }
   for (int t = 0; t < kStepTileCount; ++t) {
     const int TJ = kStepTiles[t].r * kStepTiles[t].nwm, NT = (kStepTiles[t].nwm + 1) * 32;
@@ -1069,7 +1231,7 @@ void batch_enqueue_step(xfb_batch* b, int off, int t) {
   for (xfb_handle* h : b->hs) {
     const Compiled& c = h->c;
     if (h->ade_deferred) launch_ade<T>(h, parity, b->stream);
-    if (c.nf_on || !c.probes.empty() || !c.movies.empty()) enqueue_records<T>(h, parity, tp, b->stream, nullptr);
+    if (c.nf_on || c.td_on || !c.probes.empty() || !c.movies.empty()) enqueue_records<T>(h, parity, tp, b->stream, nullptr);
   }
 }
 

@@ -79,10 +79,16 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* b, unsigned parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait for phase `parity` of barrier b: false after 2^22 polls, far
-// beyond the latency of any staging copy (the copies then never completed).
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity) {
-  for (int n = 0; n < (1 << 22); ++n)
+// Default poll limit of the bounded staging waits, far beyond the latency of
+// any staging copy.  The step kernels read their limit from err[1] (the
+// handle's error word pair: flag, poll limit), which the host sets to this
+// value at init; a smaller limit (xfb_set_wait_limit) lets a test make the
+// waits run out.
+constexpr int kWaitPolls = 1 << 22;
+// Bounded wait for phase `parity` of barrier b: false after `polls` polls
+// (the copies then never completed).
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity, int polls = kWaitPolls) {
+  for (int n = 0; n < polls; ++n)
     if (mbar_try_wait(b, parity)) return true;
   return false;
 }
@@ -542,7 +548,8 @@ __device__ __forceinline__ int prefetch_e_psi(const PmlP<T>& pm, const GridP<T>&
 // TMA: staging by tiled bulk copies from `maps` (one thread issues a plane's
 // seven boxes, a barrier per ring slot counts their bytes); otherwise every
 // thread stages 16-byte chunks with cp.async.  A staging wait that runs out
-// sets *err = 1 and ends the item after the copies in flight have landed.
+// (after err[1] polls) sets err[0] = 1 and ends the item after the copies in
+// flight have landed (those waits use the default limit).
 template <typename T, int R, int NWM, int NS_, int KIND, bool TMA>
 __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, const PmlP<T>& pm, const PsiH<T>& ps,
                                           const PsiH<T>& pd, const TfsfP& tf, const AdeP<T>& ad, int4 item,
@@ -649,8 +656,9 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
   auto phase = [&](int p) { return static_cast<unsigned>(((p - i_first) / NS) & 1); };
   int waited = i_first - 1;  // last plane whose staging barrier was passed
   bool ok = true;
+  const int polls = TMA ? err[1] : 0;  // poll limit of the staging waits
   if (TMA) {
-    ok = mbar_wait(bar + slot, phase(i_first));
+    ok = mbar_wait(bar + slot, phase(i_first), polls);
     if (ok) waited = i_first;
   }
 
@@ -719,7 +727,7 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
     const int slot_p = slot == 0 ? NS - 1 : slot - 1;      // plane i-1, refilled with plane i+NS-1
     if (TMA) {
       if (i + 1 <= i_end && ok) {  // plane i+1 has landed (plane i did one iteration earlier)
-        ok = mbar_wait(bar + slot_n, phase(i + 1));
+        ok = mbar_wait(bar + slot_n, phase(i + 1), polls);
         if (ok) waited = i + 1;
       }
       // every thread saw its planes land; iteration i-1 is complete everywhere
@@ -1056,7 +1064,8 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
   }
   int slot = i_first % NS;
   int waited = i_first - 1;
-  bool ok = mbar_wait(bar + slot, phase(i_first));
+  const int polls = err[1];  // poll limit of the staging waits
+  bool ok = mbar_wait(bar + slot, phase(i_first), polls);
   if (ok) waited = i_first;
   for (int i = i_first; i <= i_end; ++i) {
     const int ie = i - 1;
@@ -1064,7 +1073,7 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
     const int slot_n = slot + 1 == NS ? 0 : slot + 1;
     const int slot_p = slot == 0 ? NS - 1 : slot - 1;
     if (i + 1 <= i_end && ok) {
-      ok = mbar_wait(bar + slot_n, phase(i + 1));
+      ok = mbar_wait(bar + slot_n, phase(i + 1), polls);
       if (ok) waited = i + 1;
     }
     if (__syncthreads_or(!ok)) {

@@ -70,6 +70,17 @@ struct xfb_handle {
   double2* th = nullptr;
   int nf_off[7] = {};
   long long nf_npts = 0;
+  // time-domain NF2FF (k_nftd_chunks / k_nftd_bins)
+  void* td_ent = nullptr;     // int4 per point
+  double* td_tsd = nullptr;   // delay in steps per point
+  double* td_prev = nullptr;  // [2][td_n]
+  long long td_n = 0;
+  void* td_chunk = nullptr;   // int4 per chunk
+  int td_nchunks = 0;
+  double* td_part = nullptr;  // [td_nchunks][6]
+  int* td_offs = nullptr;
+  int* td_list = nullptr;
+  double* td_pot = nullptr;   // [6][td_bins]
   // monitors
   long long* probe_idx = nullptr;
   int* probe_field = nullptr;
@@ -103,6 +114,15 @@ struct xfb_handle {
   bool labc_on = false;
   void* labc_w = nullptr;
   float* labc_hist = nullptr;
+  // field read-back (read_field_t): a device gather buffer of kReadChunk
+  // elements of the compute type, two pinned host buffers of the same size
+  // (chunk c lands in buffer c & 1 while the host widens chunk c - 1 to
+  // double), their completion events; allocated by the first read-back
+  void* rb_dev = nullptr;
+  void* rb_host[2] = {};
+  cudaEvent_t rb_ev[2] = {};
+  // bytes this handle has copied host -> device and device -> host
+  long long h2d_bytes = 0, d2h_bytes = 0;
 };
 
 // A batch of scenes stepped together: one launch of the one-sweep kernel per

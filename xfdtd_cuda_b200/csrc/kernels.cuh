@@ -731,23 +731,14 @@ static __global__ void k_nf2ff_done(long long* done, long long v) { *done = v; }
 template <typename T>
 __device__ __forceinline__ double ld(const T* p, long long i) { return static_cast<double>(p[i]); }
 
+// Tangential fields at the centre of the face-normal `axis` cell face whose
+// node is element x: H_a, H_b, E_a, E_b of the face's tangential axes (a, b)
+// = (y, z), (z, x), (x, y) (interpolateSurfaceCenter,
+// src/include/nf2ff/interpolate_scheme.cuh:11-134).
 template <typename T>
-__global__ void k_nf2ff(GridP<T> g, NfP nf, TimeP tp) {
-  const long long pt = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (pt >= nf.npts) return;
-  const long long t = cur_step(tp);
-  int face = 0;
-  while (face < 5 && pt >= nf.off[face + 1]) ++face;
-  const long long q = pt - nf.off[face];
-  const int axis = face >> 1, pos = face & 1;
-  const int* b = nf.box;
-  int i, j, k;
-  if (axis == 0) { const int nk = b[5] - b[4]; i = pos ? b[1] : b[0]; j = b[2] + static_cast<int>(q / nk); k = b[4] + static_cast<int>(q % nk); }
-  else if (axis == 1) { const int nk = b[5] - b[4]; j = pos ? b[3] : b[2]; i = b[0] + static_cast<int>(q / nk); k = b[4] + static_cast<int>(q % nk); }
-  else { const int nj = b[3] - b[2]; k = pos ? b[5] : b[4]; i = b[0] + static_cast<int>(q / nj); j = b[2] + static_cast<int>(q % nj); }
+__device__ __forceinline__ void nf_face_samples(const GridP<T>& g, int axis, long long x, double& ha, double& hb,
+                                                double& ea, double& eb) {
   const long long sx = g.sx, sy = g.sy;
-  const long long x = static_cast<long long>(i) * sx + static_cast<long long>(j) * sy + k;
-  double hb, ha, eb, ea;  // interpolated H_b, H_a, E_b, E_a at the face centre
   if (axis == 0) {
     hb = 0.25 * (ld(g.hz, x + 1) + ld(g.hz, x) + ld(g.hz, x - sx + 1) + ld(g.hz, x - sx));  // HzFaceX
     ha = 0.25 * (ld(g.hy, x + sy) + ld(g.hy, x) + ld(g.hy, x - sx + sy) + ld(g.hy, x - sx));  // HyFaceX
@@ -764,6 +755,25 @@ __global__ void k_nf2ff(GridP<T> g, NfP nf, TimeP tp) {
     eb = 0.5 * (ld(g.ey, x + sx) + ld(g.ey, x));  // EyFaceZ
     ea = 0.5 * (ld(g.ex, x + sy) + ld(g.ex, x));  // ExFaceZ
   }
+}
+
+template <typename T>
+__global__ void k_nf2ff(GridP<T> g, NfP nf, TimeP tp) {
+  const long long pt = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (pt >= nf.npts) return;
+  const long long t = cur_step(tp);
+  int face = 0;
+  while (face < 5 && pt >= nf.off[face + 1]) ++face;
+  const long long q = pt - nf.off[face];
+  const int axis = face >> 1, pos = face & 1;
+  const int* b = nf.box;
+  int i, j, k;
+  if (axis == 0) { const int nk = b[5] - b[4]; i = pos ? b[1] : b[0]; j = b[2] + static_cast<int>(q / nk); k = b[4] + static_cast<int>(q % nk); }
+  else if (axis == 1) { const int nk = b[5] - b[4]; j = pos ? b[3] : b[2]; i = b[0] + static_cast<int>(q / nk); k = b[4] + static_cast<int>(q % nk); }
+  else { const int nj = b[3] - b[2]; k = pos ? b[5] : b[4]; i = b[0] + static_cast<int>(q / nj); j = b[2] + static_cast<int>(q % nj); }
+  const long long x = static_cast<long long>(i) * g.sx + static_cast<long long>(j) * g.sy + k;
+  double hb, ha, eb, ea;  // interpolated H_b, H_a, E_b, E_a at the face centre
+  nf_face_samples(g, axis, x, ha, hb, ea, eb);
   const double cja = pos ? -1.0 : 1.0, cjb = pos ? 1.0 : -1.0;
   const double cma = pos ? 1.0 : -1.0, cmb = pos ? -1.0 : 1.0;
   const double smp[4] = {cja * hb, cjb * ha, cma * eb, cmb * ea};  // J_a, J_b, M_a, M_b samples
@@ -775,6 +785,96 @@ __global__ void k_nf2ff(GridP<T> g, NfP nf, TimeP tp) {
     return;
   }
   nf_advance(nf, pt, max(t - (kNfRing - 1), *nf.done), t, true, smp);
+}
+
+// ---------------------------------------------------------------------------
+// Time-domain NF2FF (NF2FFTimeDomainData<D>::update,
+// src/nf2ff/time_domain/nf2ff_time_domain_data.cu:113-175).  The reference
+// runs the whole surface on one thread per face because several face points
+// add into the same time bin ("Here need to reduce sum", :174, and the
+// <<<1,1>>> launches at :213-223).  Here the sample points of each (face,
+// field kind) are sorted at init by their bin offset d0 = floor(delay + off)
+// and cut into chunks of at most kTdChunk points with one d0.  At step t a
+// point's two bins are t + d0 + rel and t + d0 + rel + 1 with rel = 0 or 1
+// (the rounding of delay + off + t can carry into the next integer), so a
+// chunk's contributions fall into three bins per tangential component:
+// k_nftd_chunks sums them per chunk (warp shuffles, then the warps in
+// order), k_nftd_bins adds, for every (component, bin) of the step's window,
+// the chunk sums that land there, in chunk order.  Both levels have a fixed
+// order: the potentials are reproducible run to run.
+constexpr int kTdChunk = 256;
+
+struct TdP {
+  const int4* ent;      // per point (chunk order): i, j, k, face * 2 + kind (0: E, 1: H)
+  const double* tsd;    // per point: delay in steps, (ref - r . dir) / (c dt)
+  double* prev;         // [2][n]: the a and b samples of the previous step
+  long long n;          // points (both kinds)
+  const int4* chunk;    // first point, count, face * 2 + kind, d0
+  double* part;         // [chunks][6]: (a, b) x bins t + d0 + {0, 1, 2}
+  const int* offs;      // [6 * span + 1] CSR over (component, bin offset)
+  const int* list;      // chunk * 6 + slot entries
+  int span;             // bin offsets 0 .. span - 1 of a step
+  double* pot;          // [6][bins]: W_x W_y W_z U_x U_y U_z
+  long long bins;
+  double ds[3];         // face area per normal axis
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kTdChunk) k_nftd_chunks(GridP<T> g, TdP td, TimeP tp) {
+  const int4 ch = td.chunk[blockIdx.x];
+  const long long t = cur_step(tp);
+  const int face = ch.z >> 1, kind = ch.z & 1, axis = face >> 1;
+  const bool neg = (face & 1) == 0;
+  double v[6] = {0, 0, 0, 0, 0, 0};
+  if (static_cast<int>(threadIdx.x) < ch.y) {
+    const long long id = ch.x + threadIdx.x;
+    const int4 p = td.ent[id];
+    const long long x = static_cast<long long>(p.x) * g.sx + static_cast<long long>(p.y) * g.sy + p.z;
+    double ha, hb, ea, eb;
+    nf_face_samples(g, axis, x, ha, hb, ea, eb);
+    const double a = kind ? ha : ea, b = kind ? hb : eb;
+    const double da = a - td.prev[id], db = b - td.prev[td.n + id];
+    td.prev[id] = a;
+    td.prev[td.n + id] = b;
+    // coefficients and time offset of the field kind (nf2ff_time_domain_data.cu:121-131)
+    const double off = kind ? 0.0 : 0.5;
+    double ca = kind ? -1.0 : 1.0, cb = kind ? 1.0 : -1.0;
+    if (neg) { ca *= -1.0; cb *= -1.0; }
+    const double u = td.tsd[id] + off + static_cast<double>(t);
+    const double nn = floor(u);
+    const double f = u - nn;
+    const int rel = static_cast<int>(static_cast<long long>(nn) - t - ch.w);  // 0 or 1
+    const double ds = td.ds[axis];
+    v[rel] = ca * (1 - f) * ds * db;
+    v[rel + 1] = ca * f * ds * db;
+    v[3 + rel] = cb * (1 - f) * ds * da;
+    v[3 + rel + 1] = cb * f * ds * da;
+  }
+  __shared__ double red[kTdChunk / 32][6];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    double s = v[q];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) red[wid][q] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double s = 0;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) s += red[w][threadIdx.x];
+    td.part[static_cast<long long>(blockIdx.x) * 6 + threadIdx.x] = s;
+  }
+}
+
+static __global__ void k_nftd_bins(TdP td, TimeP tp) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= 6 * td.span) return;
+  const int lo = td.offs[q], hi = td.offs[q + 1];
+  if (lo == hi) return;
+  const long long t = cur_step(tp);
+  double s = 0;
+  for (int e = lo; e < hi; ++e) s += td.part[td.list[e]];
+  td.pot[(q / td.span) * td.bins + t + q % td.span] += s;
 }
 
 // ---------------------------------------------------------------------------

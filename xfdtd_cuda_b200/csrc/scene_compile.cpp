@@ -91,6 +91,7 @@ double waveform(const Compiled& c, double t) {
 
 void size_tables(Compiled& c, long long total_steps) {
   c.total_steps = total_steps;
+  c.td_bins = c.td_on ? total_steps + c.td_span : 0;
   c.aux_source.assign(static_cast<size_t>(total_steps + 1), 0.0);
   if (c.tfsf_on)
     for (long long t = 0; t <= total_steps; ++t) c.aux_source[t] = waveform(c, t * c.dt);
@@ -113,17 +114,35 @@ void size_tables(Compiled& c, long long total_steps) {
   }
 }
 
-FaceGeom face_geom(const Compiled& c, int face) {
+static FaceGeom box_face(const int* b, int face) {
   FaceGeom g{};
   g.axis = face / 2;
   g.positive = face % 2;
-  const int* b = c.nf;
   g.i0 = b[0]; g.j0 = b[2]; g.k0 = b[4];
   g.ni = b[1] - b[0]; g.nj = b[3] - b[2]; g.nk = b[5] - b[4];
   if (g.axis == 0) { g.i0 = g.positive ? b[1] : b[0]; g.ni = 1; }
   if (g.axis == 1) { g.j0 = g.positive ? b[3] : b[2]; g.nj = 1; }
   if (g.axis == 2) { g.k0 = g.positive ? b[5] : b[4]; g.nk = 1; }
   return g;
+}
+
+FaceGeom face_geom(const Compiled& c, int face) { return box_face(c.nf, face); }
+FaceGeom td_face_geom(const Compiled& c, int face) { return box_face(c.td, face); }
+
+static void td_position(const Compiled& c, int face, int i, int j, int k, double r[3]) {
+  const int ax = face / 2;
+  const double d[3] = {c.dx, c.dy, c.dz};
+  const int n[3] = {i, j, k};
+  for (int a = 0; a < 3; ++a) r[a] = c.origin[a] + (n[a] + (a == ax ? 0.0 : 0.5)) * d[a];
+}
+
+double td_delay_steps(const Compiled& c, int face, int i, int j, int k) {
+  double r[3];
+  td_position(c, face, i, j, k, r);
+  // timeDelay / (C_0 dt) in the reference's operation order
+  // (nf2ff_time_domain_data.cuh:64-71, nf2ff_time_domain_data.cu:145-147)
+  const double delay = c.td_ref - (r[0] * c.td_dir[0] + r[1] * c.td_dir[1] + r[2] * c.td_dir[2]);
+  return delay / (kTdC0 * c.dt);
 }
 
 int compile_scene(const xfb_scene& s, Compiled& c, std::string* err) {
@@ -295,6 +314,8 @@ int compile_scene(const xfb_scene& s, Compiled& c, std::string* err) {
         hi[a] = std::min(n[a], static_cast<int>(std::ceil((ob.p[a] + ob.p[3] - c.origin[a]) / d[a])) + 1);
       }
     }
+    // planes are independent (each cell is written by one plane's thread)
+#pragma omp parallel for schedule(static)
     for (int i = lo[0]; i < hi[0]; ++i) {
       const double x = c.origin[0] + (i + 0.5) * s.dx;
       for (int j = lo[1]; j < hi[1]; ++j) {
@@ -308,17 +329,19 @@ int compile_scene(const xfb_scene& s, Compiled& c, std::string* err) {
   }
   // ADE box: bounding box of cells holding a dispersive material.
   if (c.ade_kind != XFB_ADE_NONE) {
-    int b[6] = {c.nx, 0, c.ny, 0, c.nz, 0};
+    int b0 = c.nx, b1 = 0, b2 = c.ny, b3 = 0, b4 = c.nz, b5 = 0;
+#pragma omp parallel for schedule(static) reduction(min : b0, b2, b4) reduction(max : b1, b3, b5)
     for (int i = 0; i < c.nx; ++i)
       for (int j = 0; j < c.ny; ++j)
         for (int kk = 0; kk < c.nz; ++kk) {
           const int m = c.mat_id[(static_cast<size_t>(i) * c.ny + j) * c.nz + kk];
           if (c.ade_mat[static_cast<size_t>(m) * kAdeMat] != 0) {
-            b[0] = std::min(b[0], i); b[1] = std::max(b[1], i + 1);
-            b[2] = std::min(b[2], j); b[3] = std::max(b[3], j + 1);
-            b[4] = std::min(b[4], kk); b[5] = std::max(b[5], kk + 1);
+            b0 = std::min(b0, i); b1 = std::max(b1, i + 1);
+            b2 = std::min(b2, j); b3 = std::max(b3, j + 1);
+            b4 = std::min(b4, kk); b5 = std::max(b5, kk + 1);
           }
         }
+    int b[6] = {b0, b1, b2, b3, b4, b5};
     if (b[0] >= b[1]) {
       // dispersive materials exist but occupy no cell
       for (int q = 0; q < 6; ++q) b[q] = 0;
@@ -436,6 +459,47 @@ int compile_scene(const xfb_scene& s, Compiled& c, std::string* err) {
       if (c.nf[2 * a] < 1 || c.nf[2 * a + 1] >= nax[a] || c.nf[2 * a + 1] <= c.nf[2 * a])
         return fail("NF2FF box does not fit inside the grid");
     c.freqs.assign(n.freqs, n.freqs + n.n_freqs);
+  }
+  if (s.nf2ff_td.enabled) {
+    if (s.dim != 3) return fail("time-domain NF2FF is supported on 3-D scenes");
+    const xfb_nf2ff_td& n = s.nf2ff_td;
+    if (!std::isfinite(n.theta) || !std::isfinite(n.phi)) return fail("time-domain NF2FF direction must be finite");
+    c.td_on = 1;
+    c.td[0] = c.pml[0] + n.inset[0]; c.td[1] = c.nx - c.pml[1] - n.inset[0];
+    c.td[2] = c.pml[2] + n.inset[1]; c.td[3] = c.ny - c.pml[3] - n.inset[1];
+    c.td[4] = c.pml[4] + n.inset[2]; c.td[5] = c.nz - c.pml[5] - n.inset[2];
+    for (int a = 0; a < 3; ++a)
+      if (c.td[2 * a] < 1 || c.td[2 * a + 1] >= nax[a] || c.td[2 * a + 1] <= c.td[2 * a])
+        return fail("time-domain NF2FF box does not fit inside the grid");
+    c.td_theta = n.theta;
+    c.td_phi = n.phi;
+    c.td_dir[0] = std::sin(n.theta) * std::cos(n.phi);
+    c.td_dir[1] = std::sin(n.theta) * std::sin(n.phi);
+    c.td_dir[2] = std::cos(n.theta);
+    // reference distance: the largest r . dir over the sample points, so every
+    // delay is >= 0; then the largest bin offset a step reaches
+    double best = -std::numeric_limits<double>::infinity();
+    for (int f = 0; f < 6; ++f) {
+      const FaceGeom g = td_face_geom(c, f);
+      for (int i = g.i0; i < g.i0 + g.ni; ++i)
+        for (int j = g.j0; j < g.j0 + g.nj; ++j)
+          for (int k = g.k0; k < g.k0 + g.nk; ++k) {
+            double r[3];
+            td_position(c, f, i, j, k, r);
+            best = std::max(best, r[0] * c.td_dir[0] + r[1] * c.td_dir[1] + r[2] * c.td_dir[2]);
+          }
+    }
+    c.td_ref = best;
+    double dmax = 0;
+    for (int f = 0; f < 6; ++f) {
+      const FaceGeom g = td_face_geom(c, f);
+      for (int i = g.i0; i < g.i0 + g.ni; ++i)
+        for (int j = g.j0; j < g.j0 + g.nj; ++j)
+          for (int k = g.k0; k < g.k0 + g.nk; ++k) dmax = std::max(dmax, td_delay_steps(c, f, i, j, k));
+    }
+    // bins t + floor(delay + 1/2) + {0, 1, 2} (the rounding of the sum with t
+    // can add one)
+    c.td_span = static_cast<int>(std::floor(dmax + 0.5)) + 3;
   }
 
   // ---- monitors ------------------------------------------------------------

@@ -66,6 +66,15 @@ struct Compiled {
   int nf_on = 0;
   int nf[6] = {0, 0, 0, 0, 0, 0};  // is ie js je ks ke (nodes)
   std::vector<double> freqs;
+  // time-domain NF2FF: box, observation direction, reference distance (the
+  // largest r . dir over the sample points) and the bins one step can reach
+  int td_on = 0;
+  int td[6] = {0, 0, 0, 0, 0, 0};  // is ie js je ks ke (nodes)
+  double td_theta = 0, td_phi = 0;
+  double td_dir[3] = {0, 0, 0};
+  double td_ref = 0;
+  int td_span = 0;
+  long long td_bins = 0;           // total_steps + td_span (size_tables)
   // monitors
   std::vector<xfb_probe> probes;
   std::vector<xfb_movie> movies;
@@ -93,5 +102,15 @@ struct FaceGeom {
   int ni, nj, nk;  // extents in i, j, k (normal extent 1)
 };
 FaceGeom face_geom(const Compiled& c, int face);
+// The same geometry for the time-domain NF2FF box.
+FaceGeom td_face_geom(const Compiled& c, int face);
+// Speed of light of the reference's time-domain NF2FF
+// (src/nf2ff/time_domain/nf2ff_time_domain_data.cu:16).
+constexpr double kTdC0 = 299792458.0;
+// Time-domain NF2FF sample point (i, j, k) of `face`: its position (the face
+// node along the normal, cell centres along the tangential axes,
+// nf2ff_time_domain_data.cu:53-66) and its delay in steps,
+// (ref - r . dir) / (c dt).
+double td_delay_steps(const Compiled& c, int face, int i, int j, int k);
 
 }  // namespace xfb

@@ -360,6 +360,40 @@ class NFFFTFrequencyDomain:
         return et, ep
 
 
+class NFFFTTimeDomain:
+    """Time-domain near-to-far-field transformation for one observation
+    direction (the reference's NFFFTTimeDomain, constructed as in its sphere
+    test: NFFFTTimeDomain(dx, dy, dz, out_dir, theta, phi))."""
+
+    def __init__(self, distance_x, distance_y, distance_z, out_dir: str = "", theta: float = 0.0, phi: float = 0.0):
+        self.inset = (int(distance_x), int(distance_y), int(distance_z))
+        self.out_dir = out_dir
+        self.theta, self.phi = float(theta), float(phi)
+        self._hd: "SimulationHD | None" = None
+        self.potentials = None  # [6][bins]: W_x W_y W_z U_x U_y U_z after run()
+
+    def setOutputDir(self, d: str):
+        self.out_dir = d
+
+    def observationDirection(self):
+        st = math.sin(self.theta)
+        return Vector(st * math.cos(self.phi), st * math.sin(self.phi), math.cos(self.theta))
+
+    def processFarField(self):
+        """(t, r E_theta(t), r E_phi(t)) in the observation direction, t = n dt
+        from the moment the wave leaves the box point farthest along it.
+        Writes ``far_field_td.npy`` under the output directory when set."""
+        if self._hd is None:
+            raise RuntimeError("run the simulation first")
+        et, ep = self._hd.handle.far_field_td()
+        t = np.arange(len(et)) * self._hd.handle.info().dt
+        if self.out_dir:
+            os.makedirs(self.out_dir, exist_ok=True)
+            np.save(Path(self.out_dir) / "far_field_td.npy",
+                    {"t": t, "theta": self.theta, "phi": self.phi, "e_theta": et, "e_phi": ep}, allow_pickle=True)
+        return t, et, ep
+
+
 class Simulation:
     """Scene container with the XFDTD_CORE Simulation surface used by the reference drivers."""
 
@@ -387,7 +421,8 @@ class Simulation:
     def addMonitor(self, m):
         self.monitor_list.append(m)
 
-    def addNF2FF(self, n: NFFFTFrequencyDomain):
+    def addNF2FF(self, n):
+        """Add an NFFFTFrequencyDomain or an NFFFTTimeDomain (one of each at most)."""
         self.nf2ff_list.append(n)
 
     def monitors(self):
@@ -462,8 +497,15 @@ class Simulation:
             w = tf.waveform()
             sc.tfsf.waveform, sc.tfsf.tau, sc.tfsf.t0, sc.tfsf.freq = w.kind, w.tau, w.t0, w.freq
         keep = [cm, co]
-        if self.nf2ff_list:
-            nf = self.nf2ff_list[0]
+        td = next((n for n in self.nf2ff_list if isinstance(n, NFFFTTimeDomain)), None)
+        if td is not None:
+            sc.nf2ff_td.enabled = 1
+            for a in range(3):
+                sc.nf2ff_td.inset[a] = td.inset[a]
+            sc.nf2ff_td.theta, sc.nf2ff_td.phi = td.theta, td.phi
+        fds = [n for n in self.nf2ff_list if isinstance(n, NFFFTFrequencyDomain)]
+        if fds:
+            nf = fds[0]
             fr = (C.c_double * len(nf.freqs))(*nf.freqs)
             keep.append(fr)
             sc.nf2ff.enabled = 1
@@ -594,6 +636,10 @@ class Handle:
     def sync(self):
         self._c(self.lib.xfb_sync(self.h))
 
+    def set_wait_limit(self, polls: int):
+        """Poll limit of the step kernel's bounded staging waits (diagnostics)."""
+        self._c(self.lib.xfb_set_wait_limit(self.h, int(polls)))
+
     def timed_step(self, n) -> float:
         ms = C.c_double()
         self._c(self.lib.xfb_timed_step(self.h, int(n), C.byref(ms)))
@@ -645,6 +691,23 @@ class Handle:
         self._c(self.lib.xfb_far_field(self.h, freq, len(th), th.ctypes.data_as(L._dp), ph.ctypes.data_as(L._dp),
                                        out.ctypes.data_as(L._dp)))
         return out[:, 0] + 1j * out[:, 1], out[:, 2] + 1j * out[:, 3]
+
+    def read_nf2ff_td(self, which) -> np.ndarray:
+        """Time-domain NF2FF potential `which` (0..2 W_x..W_z, 3..5 U_x..U_z)."""
+        n = C.c_longlong()
+        self._c(self.lib.xfb_nf2ff_td_bins(self.h, C.byref(n)))
+        out = np.empty(n.value, dtype=np.float64)
+        self._c(self.lib.xfb_read_nf2ff_td(self.h, which, out.ctypes.data_as(L._dp), out.size))
+        return out
+
+    def far_field_td(self):
+        """(r E_theta(t_n), r E_phi(t_n)) of the time-domain NF2FF."""
+        n = C.c_longlong()
+        self._c(self.lib.xfb_nf2ff_td_bins(self.h, C.byref(n)))
+        et = np.empty(n.value, dtype=np.float64)
+        ep = np.empty(n.value, dtype=np.float64)
+        self._c(self.lib.xfb_far_field_td(self.h, et.ctypes.data_as(L._dp), ep.ctypes.data_as(L._dp), n.value))
+        return et, ep
 
     def set_learned_abc(self, weights):
         """Learned absorbing boundary on every wall (3-D one-sweep scene
@@ -721,6 +784,10 @@ class Batch:
     def sync(self):
         self._c(self.lib.xfb_batch_sync(self.b))
 
+    def set_wait_limit(self, polls: int):
+        """Poll limit of the batch step's bounded staging waits (diagnostics)."""
+        self._c(self.lib.xfb_batch_set_wait_limit(self.b, int(polls)))
+
     def timed_step(self, n: int) -> float:
         ms = C.c_double()
         self._c(self.lib.xfb_batch_timed_step(self.b, n, C.byref(ms)))
@@ -794,8 +861,11 @@ class SimulationHD:
                 m.data = h.read_movie(mi)
                 mi += 1
                 m.output()
-        for nf in self._host.nf2ff_list[:1]:
+        for nf in self._host.nf2ff_list:
             nf._hd = self
+            if isinstance(nf, NFFFTTimeDomain):
+                nf.potentials = [h.read_nf2ff_td(w) for w in range(6)]
+                continue
             nf.currents = [[[h.read_nf2ff(f, face, w) for w in range(4)] for face in range(6)]
                            for f in range(nf.freqCount())]
 
