@@ -342,22 +342,25 @@ def cylinder2d_compare(local: int, steps: int = 4000):
 def learned_abc_compare(local: int, steps: int, warmup: int, side: int = 768):
     """C5: a side^3 FP32 scattering domain whose walls use the learned
     absorbing boundary (shipped weights) against the same interior wrapped in
-    a 12-cell CPML ((side+24)^3), device-timed; with the probe error of the
-    learned boundary, of the plain Mur boundary and of bare PEC walls against
-    the CPML judge on a 48^3 validation scene."""
+    a 12-cell CPML ((side+24)^3) and in a 3-cell CPML ((side+6)^3, the depth
+    of the learned stencil), device-timed, with k_labc_apply's share of the
+    learned step; and the probe error of the learned boundary, of the plain
+    Mur boundary, of bare PEC walls and of the 3-cell CPML against the 12-cell
+    CPML judge on a 48^3 validation scene."""
     import xfdtd_cuda_b200 as X
     from xfdtd_cuda_b200 import _lib as L
     from xfdtd_cuda_b200 import labc
     w = labc.shipped_weights()
-    out = {"workload": f"scatterer in {side}^3 FP32, learned 3-cell boundary vs 12-cell CPML ({side + 24}^3)",
-           "unit": UNIT}
-    for mode in ("learned", "cpml"):
-        sim = labc.scatter_scene(5, interior=side, pml=12 if mode == "cpml" else 0, dl=1e-3, inset=64)
+    out = {"workload": f"scatterer in {side}^3 FP32, learned 3-cell boundary vs 12-cell CPML ({side + 24}^3) and "
+                       f"3-cell CPML ({side + 6}^3)", "unit": UNIT}
+    for mode in ("learned", "cpml", "cpml3"):
+        thick = {"cpml": 12, "cpml3": 3}.get(mode, 0)
+        sim = labc.scatter_scene(5, interior=side, pml=thick, dl=1e-3, inset=64)
         sc, keep = sim.lower()
         h = X.Handle(sc, keep)
         h.set_device(local)
         h.set_kernel_path(L.PATH_FUSED)
-        h.init(warmup + steps)
+        h.init(warmup + steps + 3)
         if mode == "learned":
             h.set_learned_abc(w)
         h.step(warmup)
@@ -367,9 +370,12 @@ def learned_abc_compare(local: int, steps: int, warmup: int, side: int = 768):
         cells = gi.nx * gi.ny * gi.nz
         out[mode] = {"cells": cells, "value": cells * steps / (ms / 1e3) / 1e6, "ms_per_step": ms / steps,
                      "interior_cell_updates_per_s": side ** 3 * steps / (ms / 1e3) / 1e6}
+        if mode == "learned":  # k_labc_apply's share of the step (launches bracketed by events)
+            kms, kcnt = h.profile_kernels(3)
+            out[mode]["k_labc_apply_share"] = kms[L.K_CORRECT] / sum(kms)
         h.close()
     out["probe_error_vs_cpml"] = labc.reflection_errors(w, seed=10, interior=48, steps=300, device=local,
-                                                        modes=("pec", "mur", "learned"))
+                                                        modes=("pec", "mur", "learned", "cpml3"))
     return out
 
 
@@ -531,7 +537,11 @@ def main():
             accuracy = {"what": "relative L2 of the FP32 one-sweep engine against the FP64 engine (bit-identical "
                                 "to the CPU restatement) at full size, per output",
                         "dielectric_sphere_156cube_2400_steps": A.fp32_vs_fp64("dielectric", 2400, local),
-                        "dispersive_sphere_408cube_6000_steps": A.fp32_vs_fp64("dispersive", 6000, local)}
+                        "dispersive_sphere_408cube_6000_steps": A.fp32_vs_fp64("dispersive", 6000, local),
+                        "coefficient_storage_trial": {
+                            "what": "C1 (156^3, 2400 steps) with the FP32 engine's coefficient LUT rounded to 16 bits",
+                            "fp16": A.fp32_vs_fp64("dielectric", 2400, local, fields=False, coeff_storage=1),
+                            "bf16": A.fp32_vs_fp64("dielectric", 2400, local, fields=False, coeff_storage=2)}}
         except Exception as exc:
             accuracy = {"error": str(exc)}
 

@@ -266,6 +266,16 @@ int xfb_profile_kernels(xfb_handle* h, long long n, double* ms, long long* launc
 /* Select the 3-D kernel path (enum xfb_kernel_path); before xfb_init. */
 int xfb_set_kernel_path(xfb_handle* h, int path);
 
+/* Storage trial of the update coefficients, no counterpart in the reference
+ * (its 18 per-cell coefficient arrays are FP64, fdtd_coefficient.cuh:15-168).
+ * NATIVE keeps them in the compute precision; FP16 / BF16 round every entry
+ * of the material LUT to that 16-bit format at xfb_init (the arithmetic
+ * stays in the compute precision), to measure what 16-bit storage would cost
+ * in accuracy.  The LUT sits in shared memory, not on the HBM stream, so
+ * 16-bit storage would save no bandwidth.  Before xfb_init. */
+enum xfb_coeff_storage { XFB_COEFF_NATIVE = 0, XFB_COEFF_FP16 = 1, XFB_COEFF_BF16 = 2 };
+int xfb_set_coeff_storage(xfb_handle* h, int storage);
+
 /* Use CUDA-graph replay of the step loop (default 1) and the steps per
  * captured graph (default 64). */
 int xfb_set_graph(xfb_handle* h, int enabled, int steps_per_graph);
@@ -396,6 +406,40 @@ int xfb_batch_info(const xfb_batch* b, long long* cells, int* tile_rows, int* wo
 const char* xfb_batch_last_error(const xfb_batch* b);
 /* Release the batch; its handles become independent again. */
 int xfb_batch_destroy(xfb_batch* b);
+
+/* ---- x-slab decomposition -----------------------------------------------
+ * No counterpart in the reference (its one multi-node path is XFDTD_CORE's
+ * CPU MPI).  A handle can update only the cells [i0, i1) along x of its
+ * scene, so N handles on N devices step one grid together.  Every step is:
+ * xfb_slab_update on every slab (the one-sweep update of the owned planes;
+ * the H plane below the slab is recomputed from the halo), then the halo
+ * exchange -- each slab's first owned plane to the lower neighbour's upper
+ * halo, its last owned plane to the upper neighbour's lower halo (the six
+ * components of the set the update wrote, and upward the H-side psi of the y
+ * and z CPML slabs) -- then xfb_slab_record on every slab (monitors of the
+ * owned planes, step counter).  Monitors record only what a slab owns (probes,
+ * movie planes, NF2FF face points and time-domain sums by plane), so the sum
+ * over the slabs of every read-back is the whole grid's.  The arrays are
+ * allocated at full size on every device.  A slab boundary s must leave the
+ * plane s - 1 outside the x CPML; learned boundaries and batches take whole
+ * grids only. */
+int xfb_set_slab(xfb_handle* h, int i0, int i1);  /* before xfb_init */
+int xfb_get_slab(const xfb_handle* h, int* i0, int* i1);
+int xfb_slab_update(xfb_handle* h);
+/* The device buffers of one side of the exchange, in the set the pending
+ * update wrote: which = 0 the first owned plane (sent down), 1 the last owned
+ * plane (sent up), 2 the lower halo (received from below), 3 the upper halo
+ * (received from above).  *n buffers (at most 10): the plane of Ex Ey Ez Hx
+ * Hy Hz, and on the upward direction (1 and 2) also the plane of the H-side
+ * CPML psi of the y and z slabs, which the H halo of the slab above reads.
+ * Buffer q of side 1 of a slab goes to buffer q of side 2 of the slab above;
+ * buffer q of side 0 to buffer q of side 3 of the slab below.  Between update
+ * and record only. */
+int xfb_slab_planes(xfb_handle* h, int which, void* ptrs[10], size_t sizes[10], int* n);
+/* The exchange between two neighbouring slabs of one process (peer copies,
+ * same or different devices; waits for both updates, returns when done). */
+int xfb_slab_exchange(xfb_handle* lo, xfb_handle* hi);
+int xfb_slab_record(xfb_handle* h);
 
 /* ---- checkpoint / resume ------------------------------------------------ */
 /* Byte size of the full solver state (fields, CPML psi, ADE state, TFSF

@@ -52,3 +52,16 @@ def test_fp64_dielectric_sphere_full_size_bit_identical_to_oracle():
         for w in range(4):
             assert np.array_equal(h.read_nf2ff(0, face, w), o.nf2ff(0, face, w)), f"nf2ff face {face} current {w}"
     h.close()
+
+
+def test_coefficient_storage_trial_reports_its_error():
+    # 16-bit storage of the coefficient LUT (the north star's trial): the
+    # rounding changes every coefficient by up to 2^-11 (FP16) / 2^-8 (BF16)
+    # relative, far above FP32's; measured here, not assumed
+    nat = accuracy.fp32_vs_fp64("dielectric", 600, cells=60, fields=False)
+    f16 = accuracy.fp32_vs_fp64("dielectric", 600, cells=60, fields=False, coeff_storage=1)
+    b16 = accuracy.fp32_vs_fp64("dielectric", 600, cells=60, fields=False, coeff_storage=2)
+    print({"native": nat, "fp16": f16, "bf16": b16})
+    assert nat["far_field_worst"] <= BAR
+    for r in (f16, b16):
+        assert np.isfinite(r["probes"]) and r["probes"] > nat["probes"]

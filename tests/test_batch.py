@@ -90,3 +90,31 @@ def test_fp64_batch_against_oracle():
         o.run(n)
         assert bit_equal(fields_of(h, 3), fields_of(o, 3))
     b.close()
+
+
+@pytest.mark.gpu
+def test_autotune_cache_reused(tmp_path, monkeypatch):
+    # the first batch autotunes and records its choice per (GPU, precision,
+    # scene sizes); a second batch of the same scenes takes it without probing
+    cache = tmp_path / "tiles.txt"
+    monkeypatch.setenv("XFB_AUTOTUNE_CACHE", str(cache))
+    sims = configs.batched_sweep(n=3, lo=20, hi=30, seed=12)
+
+    def batch():
+        hs = [X.Handle(*s.lower()) for s in sims]
+        b = X.Batch(hs)
+        b.init(30)
+        return b, hs
+
+    b, hs = batch()
+    b.step(20)
+    b.sync()
+    rows = b.info()["tile_rows"]
+    b.close()
+    lines = cache.read_text().splitlines()
+    assert len(lines) == 1 and lines[0].split()[-1] in ("0", "1", "2")
+    b2, hs2 = batch()
+    b2.step(1)  # too few steps to autotune: without the cache it would take 16-row tiles
+    b2.sync()
+    assert b2.info()["tile_rows"] == rows
+    b2.close()

@@ -28,8 +28,10 @@ MAX_POLES = 4
 FAR_FIELD_STATIC_MAX_ANGLES = 4096  # XFB_FAR_FIELD_STATIC_MAX_ANGLES
 K_UPDATE_H, K_AUX, K_UPDATE_E, K_NF2FF, K_PROBE, K_MOVIE, K_STEP, K_CORRECT, K_COUNT = range(9)
 KERNEL_NAMES = ("k_h3/k_h2 (H half-step)", "k_aux (TFSF aux grid)", "k_e3/k_e2 (E half-step)", "k_nf2ff",
-                "k_probe", "k_movie", "k_step3 (one-sweep H+E step)", "plain CPML/TFSF corrector launches")
+                "k_probe", "k_movie", "k_step3 (one-sweep H+E step)",
+                "boundary corrections (plain CPML/TFSF launches; k_labc_apply of the learned boundary)")
 PATH_AUTO, PATH_SPLIT, PATH_FUSED, PATH_PLAIN = 0, 1, 2, 3
+COEFF_NATIVE, COEFF_FP16, COEFF_BF16 = 0, 1, 2
 
 
 class Pole(C.Structure):
@@ -143,6 +145,7 @@ SIGNATURES = [
     ("xfb_profile_kernels", C.c_int, [_H, C.c_longlong, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
     ("xfb_set_graph", C.c_int, [_H, C.c_int, C.c_int]),
     ("xfb_set_kernel_path", C.c_int, [_H, C.c_int]),
+    ("xfb_set_coeff_storage", C.c_int, [_H, C.c_int]),
     ("xfb_get_grid_info", C.c_int, [_H, C.POINTER(GridInfo)]),
     ("xfb_read_field", C.c_int, [_H, C.c_int, _dp, C.c_size_t]),
     ("xfb_write_field", C.c_int, [_H, C.c_int, _dp, C.c_size_t]),
@@ -174,6 +177,12 @@ SIGNATURES = [
     ("xfb_batch_info", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("xfb_batch_last_error", C.c_char_p, [C.c_void_p]),
     ("xfb_batch_destroy", C.c_int, [C.c_void_p]),
+    ("xfb_set_slab", C.c_int, [_H, C.c_int, C.c_int]),
+    ("xfb_get_slab", C.c_int, [_H, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("xfb_slab_update", C.c_int, [_H]),
+    ("xfb_slab_planes", C.c_int, [_H, C.c_int, C.c_void_p * 10, C.c_size_t * 10, C.POINTER(C.c_int)]),
+    ("xfb_slab_exchange", C.c_int, [_H, _H]),
+    ("xfb_slab_record", C.c_int, [_H]),
     ("xfb_state_size", C.c_int, [_H, C.POINTER(C.c_size_t)]),
     ("xfb_get_state", C.c_int, [_H, C.c_void_p, C.c_size_t]),
     ("xfb_set_state", C.c_int, [_H, C.c_void_p, C.c_size_t]),

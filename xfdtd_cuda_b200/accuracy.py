@@ -54,11 +54,13 @@ def scene(name: str, precision: str, cells: int | None = None):
     return configs.dispersive_sphere(cells=c, precision=precision, probes=seeded_probes(c * 1e-3 / 2))
 
 
-def run_outputs(sim, steps: int, device: int = 0, fields: bool = True):
+def run_outputs(sim, steps: int, device: int = 0, fields: bool = True, coeff_storage: int = 0):
     """Run `steps` steps and collect probes, far-field cuts and final fields."""
     sc, keep = sim.lower()
     h = Handle(sc, keep)
     h.set_device(device)
+    if coeff_storage:
+        h.set_coeff_storage(coeff_storage)
     h.init(steps)
     h.step(steps)
     h.sync()
@@ -76,9 +78,11 @@ def run_outputs(sim, steps: int, device: int = 0, fields: bool = True):
     return out
 
 
-def fp32_vs_fp64(name: str, steps: int, device: int = 0, cells: int | None = None, fields: bool = True):
-    """Relative L2 error of every output of the FP32 run against the FP64 run."""
-    r32 = run_outputs(scene(name, "fp32", cells), steps, device, fields)
+def fp32_vs_fp64(name: str, steps: int, device: int = 0, cells: int | None = None, fields: bool = True,
+                 coeff_storage: int = 0):
+    """Relative L2 error of every output of the FP32 run (its coefficient LUT
+    optionally rounded to FP16 / BF16, the storage trial) against the FP64 run."""
+    r32 = run_outputs(scene(name, "fp32", cells), steps, device, fields, coeff_storage)
     r64 = run_outputs(scene(name, "fp64", cells), steps, device, fields)
     per_probe = [rel_l2(a, b) for a, b in zip(r32["probes"], r64["probes"])]
     res = {

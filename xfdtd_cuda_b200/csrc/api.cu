@@ -296,6 +296,14 @@ int xfb_set_kernel_path(xfb_handle* h, int path) {
   return XFB_OK;
 }
 
+int xfb_set_coeff_storage(xfb_handle* h, int storage) {
+  if (!h) return set_err(nullptr, XFB_ERR_INVALID, "null handle");
+  if (storage < XFB_COEFF_NATIVE || storage > XFB_COEFF_BF16) return set_err(h, XFB_ERR_INVALID, "unknown coefficient storage");
+  if (h->inited) return set_err(h, XFB_ERR_STATE, "set the coefficient storage before xfb_init");
+  h->coeff_storage = storage;
+  return XFB_OK;
+}
+
 int xfb_set_graph(xfb_handle* h, int enabled, int steps_per_graph) {
   if (!h) return set_err(nullptr, XFB_ERR_INVALID, "null handle");
   if (steps_per_graph < 1 || steps_per_graph > 4096) return set_err(h, XFB_ERR_INVALID, "steps_per_graph must be in [1, 4096]");
@@ -314,6 +322,9 @@ int xfb_prepare_tables(xfb_handle* h, long long total_steps) {
 int xfb_init(xfb_handle* h, long long total_steps) {
   if (!h) return set_err(nullptr, XFB_ERR_INVALID, "null handle");
   if (int rc = not_batched(h)) return rc;
+  h->slab_pending = false;
+  if (is_slab(h) && (h->path == XFB_PATH_SPLIT || h->path == XFB_PATH_PLAIN))
+    return set_err(h, XFB_ERR_INVALID, "x slabs run on the one-sweep path");
   if (total_steps < 0 || total_steps > (1LL << 31)) return set_err(h, XFB_ERR_INVALID, "total_steps out of range");
   if (h->device < 0) {
     int n = 0;
@@ -350,6 +361,7 @@ int xfb_init(xfb_handle* h, long long total_steps) {
 int xfb_step(xfb_handle* h, long long n) {
   int rc = check_handle(h, true);
   if (rc || (rc = not_batched(h))) return rc;
+  if (is_slab(h)) return set_err(h, XFB_ERR_STATE, "an x slab steps through xfb_slab_update / xfb_slab_record");
   if (n < 0) return set_err(h, XFB_ERR_INVALID, "negative step count");
   if (h->step + n > h->c.total_steps)
     return set_err(h, XFB_ERR_RANGE, "steps beyond the count xfb_init sized the run for");
@@ -537,6 +549,8 @@ static int nf2ff_flush(xfb_handle* h) {
   nf.total_steps = c.total_steps;
   nf.ring = h->nf_ring;
   nf.done = h->nf_done;
+  nf.own_lo = own_lo(h);
+  nf.own_hi = own_hi(h);
   k_nf2ff_flush<<<static_cast<unsigned>((h->nf_npts + 255) / 256), 256, 0, s>>>(nf, h->step);
   k_nf2ff_done<<<1, 1, 0, s>>>(h->nf_done, h->step);
   XFB_CUDA(h, cudaGetLastError());
@@ -681,6 +695,119 @@ int xfb_far_field_td(xfb_handle* h, double* e_theta, double* e_phi, size_t len) 
   return XFB_OK;
 }
 
+// ---- x-slab decomposition ---------------------------------------------------
+
+int xfb_set_slab(xfb_handle* h, int i0, int i1) {
+  if (!h) return set_err(nullptr, XFB_ERR_INVALID, "null handle");
+  if (h->inited) return set_err(h, XFB_ERR_STATE, "set the slab before xfb_init");
+  const Compiled& c = h->c;
+  if (c.dim != 3) return set_err(h, XFB_ERR_INVALID, "x slabs are 3-D");
+  if (i0 < 0 || i1 > c.nx || i1 <= i0) return set_err(h, XFB_ERR_RANGE, "slab planes outside [0, nx)");
+  if (c.nx >= 65536 || c.ny >= 65536 || c.nz >= 65536) return set_err(h, XFB_ERR_INVALID, "x slabs need sides below 65536 cells");
+  // the H halo plane below a slab is recomputed from the read set; its x-CPML
+  // psi would be another slab's, so no split may put it in an x slab
+  for (int s0 : {i0, i1})
+    if (s0 > 0 && s0 < c.nx && (s0 - 1 < c.pml[0] || s0 - 1 >= c.nx - c.pml[1]))
+      return set_err(h, XFB_ERR_RANGE, "a slab boundary's plane below lies in the x CPML");
+  h->slab_i0 = i0;
+  h->slab_i1 = i1;
+  return XFB_OK;
+}
+
+int xfb_get_slab(const xfb_handle* h, int* i0, int* i1) {
+  if (!h || !i0 || !i1) return set_err(nullptr, XFB_ERR_INVALID, "null argument");
+  *i0 = is_slab(h) ? h->slab_i0 : 0;
+  *i1 = is_slab(h) ? h->slab_i1 : h->c.nx;
+  return XFB_OK;
+}
+
+int xfb_slab_update(xfb_handle* h) {
+  int rc = check_handle(h, true);
+  if (rc) return rc;
+  if (!is_slab(h)) return set_err(h, XFB_ERR_STATE, "not an x slab (xfb_set_slab)");
+  if (h->slab_pending) return set_err(h, XFB_ERR_STATE, "the previous update awaits xfb_slab_record");
+  if (h->step + 1 > h->c.total_steps) return set_err(h, XFB_ERR_RANGE, "steps beyond the count xfb_init sized the run for");
+  return h->c.prec == XFB_FP64 ? slab_update<double>(h) : slab_update<float>(h);
+}
+
+int xfb_slab_record(xfb_handle* h) {
+  int rc = check_handle(h, true);
+  if (rc) return rc;
+  if (!h->slab_pending) return set_err(h, XFB_ERR_STATE, "no update awaits its record");
+  return h->c.prec == XFB_FP64 ? slab_record<double>(h) : slab_record<float>(h);
+}
+
+// The buffers of one exchange side in the set the pending update wrote:
+// which = 0 the first owned plane (sent down), 1 the last owned plane (sent
+// up), 2 the lower halo (received from below), 3 the upper halo (received
+// from above).  Six field planes; the upward direction (1, 2) also carries
+// the H-side psi of the y and z CPML slabs at that plane, which the H halo of
+// the slab above reads.
+static int slab_buffers(xfb_handle* h, int which, void* ptrs[10], size_t sizes[10], int* n) {
+  const int plane[4] = {h->slab_i0, h->slab_i1 - 1, h->slab_i0 - 1, h->slab_i1};
+  const long long p = plane[which];
+  if (p < 0 || p > h->c.nx) return set_err(h, XFB_ERR_RANGE, "the slab has no halo on that side (grid wall)");
+  const int set = static_cast<int>((h->step + 1) & 1);  // the set the pending update wrote
+  int q = 0;
+  for (int f = 0; f < 6; ++f, ++q) {
+    ptrs[q] = static_cast<char*>(field_ptr(h, set, f)) + p * h->sx * h->esize;
+    sizes[q] = static_cast<size_t>(h->sx) * h->esize;
+  }
+  if (which == 1 || which == 2) {
+    void* const* hp = set ? h->psi_h1 : h->psi + 6;  // hy_x hz_x hz_y hx_y hx_z hy_z
+    const long long ys = h->ysx, zs = h->zsx;
+    if (ys > 0)
+      for (int r : {2, 3}) {
+        ptrs[q] = static_cast<char*>(hp[r]) + p * ys * h->esize;
+        sizes[q++] = static_cast<size_t>(ys) * h->esize;
+      }
+    if (zs > 0 && h->c.pml[4] + h->c.pml[5] > 0)
+      for (int r : {4, 5}) {
+        ptrs[q] = static_cast<char*>(hp[r]) + p * zs * h->esize;
+        sizes[q++] = static_cast<size_t>(zs) * h->esize;
+      }
+  }
+  *n = q;
+  return XFB_OK;
+}
+
+int xfb_slab_planes(xfb_handle* h, int which, void* ptrs[10], size_t sizes[10], int* n) {
+  int rc = check_handle(h, true);
+  if (rc) return rc;
+  if (!is_slab(h) || !h->slab_pending) return set_err(h, XFB_ERR_STATE, "planes exist between xfb_slab_update and xfb_slab_record");
+  if (which < 0 || which > 3 || !ptrs || !sizes || !n) return set_err(h, XFB_ERR_INVALID, "which must be 0..3");
+  return slab_buffers(h, which, ptrs, sizes, n);
+}
+
+int xfb_slab_exchange(xfb_handle* lo, xfb_handle* hi) {
+  if (!lo || !hi) return set_err(nullptr, XFB_ERR_INVALID, "null handle");
+  int rc = check_handle(lo, true);
+  if (rc || (rc = check_handle(hi, true))) return rc;
+  if (!is_slab(lo) || !is_slab(hi) || lo->slab_i1 != hi->slab_i0)
+    return set_err(lo, XFB_ERR_INVALID, "the slabs are not neighbours (lo's end must be hi's start)");
+  if (!lo->slab_pending || !hi->slab_pending || lo->step != hi->step)
+    return set_err(lo, XFB_ERR_STATE, "both slabs must hold the update of the same step");
+  if (lo->sx != hi->sx || lo->esize != hi->esize) return set_err(lo, XFB_ERR_INVALID, "the slabs have different layouts");
+  // the updates have finished on both devices before their planes move
+  XFB_CUDA(hi, cudaSetDevice(hi->device));
+  XFB_CUDA(hi, cudaStreamSynchronize(hi->stream));
+  XFB_CUDA(lo, cudaSetDevice(lo->device));
+  XFB_CUDA(lo, cudaStreamSynchronize(lo->stream));
+  void *up_src[10], *up_dst[10], *dn_src[10], *dn_dst[10];
+  size_t up_sz[10], up_dsz[10], dn_sz[10], dn_dsz[10];
+  int nus, nud, nds, ndd;
+  if ((rc = slab_buffers(lo, 1, up_src, up_sz, &nus)) || (rc = slab_buffers(hi, 2, up_dst, up_dsz, &nud)) ||
+      (rc = slab_buffers(hi, 0, dn_src, dn_sz, &nds)) || (rc = slab_buffers(lo, 3, dn_dst, dn_dsz, &ndd)))
+    return rc;
+  if (nus != nud || nds != ndd) return set_err(lo, XFB_ERR_INVALID, "the slabs' exchange lists differ");
+  for (int q = 0; q < nus; ++q)
+    XFB_CUDA(lo, cudaMemcpyPeerAsync(up_dst[q], hi->device, up_src[q], lo->device, up_sz[q], lo->stream));
+  for (int q = 0; q < nds; ++q)
+    XFB_CUDA(lo, cudaMemcpyPeerAsync(dn_dst[q], lo->device, dn_src[q], hi->device, dn_sz[q], lo->stream));
+  XFB_CUDA(lo, cudaStreamSynchronize(lo->stream));
+  return XFB_OK;
+}
+
 int xfb_state_size(const xfb_handle* h, size_t* bytes) {
   if (!h || !bytes) return set_err(nullptr, XFB_ERR_INVALID, "null argument");
   if (!h->inited) return set_err(const_cast<xfb_handle*>(h), XFB_ERR_STATE, "handle not initialised");
@@ -809,6 +936,7 @@ int xfb_set_learned_abc(xfb_handle* h, const float* weights, int n_weights) {
   }
   if (n_weights != kMlpParams) return set_err(h, XFB_ERR_INVALID, "weight count must be xfb_mlp_param_count()");
   if (!fused(h) || h->c.dim != 3) return set_err(h, XFB_ERR_STATE, "the learned boundary runs on the 3-D one-sweep path");
+  if (is_slab(h)) return set_err(h, XFB_ERR_STATE, "the learned boundary runs on whole grids, not x slabs");
   for (int f = 0; f < 6; ++f)
     if (h->c.pml[f]) return set_err(h, XFB_ERR_INVALID, "the learned boundary replaces the CPML: the scene must have none");
   // BF16 weights, round to nearest even
@@ -840,6 +968,7 @@ int xfb_batch_create(xfb_handle* const* handles, int n, xfb_batch** out) {
     if (!h) return set_err(nullptr, XFB_ERR_INVALID, "null handle in the batch");
     if (h->batch) return set_err(h, XFB_ERR_STATE, "handle already belongs to a batch");
     if (h->c.dim != 3) return set_err(h, XFB_ERR_INVALID, "batches hold 3-D scenes only");
+    if (is_slab(h)) return set_err(h, XFB_ERR_INVALID, "batches hold whole scenes, not x slabs");
     if (h->c.prec != handles[0]->c.prec) return set_err(h, XFB_ERR_INVALID, "all scenes of a batch share one precision");
     for (int r = 0; r < q; ++r)
       if (handles[r] == h) return set_err(h, XFB_ERR_INVALID, "a handle appears twice in the batch");

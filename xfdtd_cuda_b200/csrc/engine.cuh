@@ -5,10 +5,15 @@
 #pragma once
 
 #include <cudaTypedefs.h>  // PFN_cuTensorMapEncodeTiled
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <omp.h>
 
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <mutex>
 
 #include "fused3d.cuh"
 #include "handle.h"
@@ -23,6 +28,18 @@ inline int upload_ade_runs(xfb_handle* h);
 inline int upload_td(xfb_handle* h);
 template <typename T>
 int encode_stage_maps(xfb_handle* h);
+
+// Update coefficients rounded to a 16-bit storage format (round to nearest
+// even) and widened back: what a LUT stored in that format would hold.
+inline std::vector<double> round_coefficients(const std::vector<double>& v, int storage) {
+  std::vector<double> out(v.size());
+  for (size_t q = 0; q < v.size(); ++q) {
+    const float f = static_cast<float>(v[q]);
+    out[q] = storage == XFB_COEFF_FP16 ? static_cast<double>(__half2float(__float2half_rn(f)))
+                                       : static_cast<double>(__bfloat162float(__float2bfloat16_rn(f)));
+  }
+  return out;
+}
 
 template <typename T>
 int init_device(xfb_handle* h) {
@@ -63,8 +80,13 @@ int init_device(xfb_handle* h) {
     if ((rc = copy(h, static_cast<uint8_t*>(p) + h->guard, m.data(), m.size(), cudaMemcpyHostToDevice))) return rc;
     h->mid = static_cast<uint8_t*>(p) + h->guard;
   }
-  if ((rc = upload<T>(h, &h->lut, c.coeff))) return rc;
-  if ((rc = upload<T>(h, &h->lut8, c.coeff8))) return rc;
+  if (h->coeff_storage == XFB_COEFF_NATIVE) {
+    if ((rc = upload<T>(h, &h->lut, c.coeff))) return rc;
+    if ((rc = upload<T>(h, &h->lut8, c.coeff8))) return rc;
+  } else {  // the storage trial: every coefficient rounded to FP16 or BF16 first
+    if ((rc = upload<T>(h, &h->lut, round_coefficients(c.coeff, h->coeff_storage)))) return rc;
+    if ((rc = upload<T>(h, &h->lut8, round_coefficients(c.coeff8, h->coeff_storage)))) return rc;
+  }
   if (fused(h) && c.dim == 3 && (rc = upload_step_items(h))) return rc;
   if (fused(h) && c.dim == 3 && h->ade_deferred && (rc = upload_ade_runs(h))) return rc;
   if (fused(h) && c.dim == 3) {
@@ -186,7 +208,8 @@ int init_device(xfb_handle* h) {
     std::vector<int> fld(n);
     for (size_t p = 0; p < n; ++p) {
       idx[p] = off3(h, c.probes[p].index[0], c.probes[p].index[1], c.dim == 3 ? c.probes[p].index[2] : 0);
-      fld[p] = c.probes[p].field;
+      const int pi = c.probes[p].index[0];
+      fld[p] = pi >= own_lo(h) && pi < own_hi(h) ? c.probes[p].field : -1;  // -1: another x slab's probe
     }
     void* p;
     if ((rc = alloc(h, &p, n * sizeof(long long), false))) return rc;
@@ -359,12 +382,13 @@ inline bool tfsf_touch(const Compiled& c, int p, int q, int j0, int TJ, int k0) 
 // below the range and the halo row and column of the tile) need no more than
 // the range's kind handles.  Ranges are at most `ich` planes long.
 inline void build_step_items(const Compiled& c, int TJ, int NT, bool ade_deferred, std::vector<int4> (&out)[kStepKindCount],
-                             int plane_chunk = 0, bool lean_interior = false) {
+                             int plane_chunk = 0, bool lean_interior = false, int p0 = 0, int p1 = -1) {
   const int nx = c.nx, ny = c.ny, nz = c.nz;
+  if (p1 < 0) p1 = nx;  // planes [p0, p1): the whole grid, or an x slab
   const int* L = c.pml;
   const int gx = (nz + 31) / 32, gy = (ny + TJ - 1) / TJ;
-  const int nch = chunks_for(gx * gy, nx, NT);
-  const int ich = plane_chunk > 0 ? plane_chunk : std::max(8, (nx + nch - 1) / nch);
+  const int nch = chunks_for(gx * gy, p1 - p0, NT);
+  const int ich = plane_chunk > 0 ? plane_chunk : std::max(8, (p1 - p0 + nch - 1) / nch);
   auto xs = [&](int p) { return p < L[0] || p >= nx - L[1]; };
   const int* b = c.ade_box;
   const bool ade = !ade_deferred && c.ade_kind != XFB_ADE_NONE && b[1] > b[0];
@@ -388,17 +412,17 @@ inline void build_step_items(const Compiled& c, int TJ, int NT, bool ade_deferre
       const bool yz = ycol || zcol;
       const bool adecol = ade && j0 < b[3] && j0 + TJ > b[2] && k0 < b[5] && k0 + 32 > b[4];
       auto need = [&](int p) { return (xs(p) ? 1 : 0) | (adecol && p >= b[0] && p < b[1] ? 4 : 0); };
-      int p = 0;
-      while (p < nx) {
+      int p = p0;
+      while (p < p1) {
         int q = p + 1, bits;
         if (yz) {
           bits = 1 | (ycol ? 2 : 0) | (zcol ? 8 : 0) | (adecol ? 4 : 0);
-          q = std::min(nx, p + ich);
+          q = std::min(p1, p + ich);
         } else {
           const int nd = need(p), halo = p > 0 && xs(p - 1) ? 1 : 0;
           bits = nd | halo;
           if (!(halo & ~nd))  // the halo plane adds nothing: extend over equal needs
-            while (q < nx && need(q) == nd && q - p < ich) ++q;
+            while (q < p1 && need(q) == nd && q - p < ich) ++q;
         }
         int kind = kind_of(bits);
         if (tfsf_touch(c, p, q, j0, TJ, k0)) kind = kind == 0 ? 7 : kind + 8;
@@ -508,14 +532,14 @@ struct TdTables {
   std::vector<int> offs, list;
 };
 
-inline void build_td_tables(const Compiled& c, TdTables& tb) {
+inline void build_td_tables(const Compiled& c, TdTables& tb, int own_lo = 0, int own_hi = 1 << 30) {
   tb = TdTables{};
   for (int face = 0; face < 6; ++face)
     for (int kind = 0; kind < 2; ++kind) {
       const FaceGeom g = td_face_geom(c, face);
       const double off = kind ? 0.0 : 0.5;
       std::map<int, std::vector<std::pair<int4, double>>> by_d0;
-      for (int i = g.i0; i < g.i0 + g.ni; ++i)
+      for (int i = std::max(g.i0, own_lo); i < std::min(g.i0 + g.ni, own_hi); ++i)
         for (int j = g.j0; j < g.j0 + g.nj; ++j)
           for (int k = g.k0; k < g.k0 + g.nk; ++k) {
             const double tsd = td_delay_steps(c, face, i, j, k);
@@ -551,7 +575,7 @@ inline void build_td_tables(const Compiled& c, TdTables& tb) {
 
 inline int upload_td(xfb_handle* h) {
   TdTables tb;
-  build_td_tables(h->c, tb);
+  build_td_tables(h->c, tb, own_lo(h), own_hi(h));
   h->td_n = static_cast<long long>(tb.ent.size());
   h->td_nchunks = static_cast<int>(tb.chunk.size());
   void* p;
@@ -601,7 +625,8 @@ inline int upload_step_items(xfb_handle* h) {
   for (int t = 0; t < 2; ++t) {
     std::vector<int4> items[kStepKindCount];
     const int nt = (kStepTiles[t].nwm + 1) * 32;
-    build_step_items(h->c, kStepTiles[t].r * kStepTiles[t].nwm, nt, h->ade_deferred, items, 0, true);
+    build_step_items(h->c, kStepTiles[t].r * kStepTiles[t].nwm, nt, h->ade_deferred, items, 0, true,
+                     is_slab(h) ? h->slab_i0 : 0, is_slab(h) ? h->slab_i1 : -1);
     // one list, the kind in the high half of .x: first the costly kinds (y/z
     // CPML columns, in-kernel ADE), costliest first, so the long items start
     // early; then the lean and x-slab items ordered by first plane, then row
@@ -632,11 +657,12 @@ inline int upload_step_items(xfb_handle* h) {
 // Work list of the deferred ADE pass: the dispersive cells of the ADE box as
 // runs along k, cut at multiples of 32 (k_ade_runs), in (i, j, k) order.
 // False (no list: k_ade_box) for grids with a side of 2^16 cells or more.
-inline bool build_ade_runs(const Compiled& c, std::vector<int2>& runs) {
+inline bool build_ade_runs(const Compiled& c, std::vector<int2>& runs, int p0 = 0, int p1 = -1) {
   const int* b = c.ade_box;
   runs.clear();
   if (c.nx >= 65536 || c.ny >= 65536 || c.nz >= 65536) return false;
-  for (int i = b[0]; i < b[1]; ++i)
+  if (p1 < 0) p1 = c.nx;  // planes [p0, p1) (an x slab)
+  for (int i = std::max(b[0], p0); i < std::min(b[1], p1); ++i)
     for (int j = b[2]; j < b[3]; ++j) {
       const uint8_t* row = c.mat_id.data() + (static_cast<size_t>(i) * c.ny + j) * c.nz;
       int k = b[4];
@@ -655,7 +681,7 @@ inline bool build_ade_runs(const Compiled& c, std::vector<int2>& runs) {
 
 inline int upload_ade_runs(xfb_handle* h) {
   std::vector<int2> runs;
-  if (!build_ade_runs(h->c, runs)) return XFB_OK;
+  if (!build_ade_runs(h->c, runs, is_slab(h) ? h->slab_i0 : 0, is_slab(h) ? h->slab_i1 : -1)) return XFB_OK;
   h->n_ade_runs = static_cast<int>(runs.size());
   if (runs.empty()) return XFB_OK;
   int rc = alloc(h, &h->ade_runs, runs.size() * sizeof(int2), false);
@@ -822,6 +848,8 @@ void enqueue_records(xfb_handle* h, int parity, TimeP tp, cudaStream_t s, Prof* 
     nf.total_steps = c.total_steps;
     nf.ring = h->nf_ring;
     nf.done = h->nf_done;
+    nf.own_lo = own_lo(h);
+    nf.own_hi = own_hi(h);
     prof_begin(h, pf, XFB_K_NF2FF);
     k_nf2ff<T><<<static_cast<unsigned>((h->nf_npts + 255) / 256), 256, 0, s>>>(g, nf, tp);
     prof_end(h, pf);
@@ -846,13 +874,24 @@ void enqueue_records(xfb_handle* h, int parity, TimeP tp, cudaStream_t s, Prof* 
     const int blocks = static_cast<int>(std::min<long long>((per + 255) / 256, 1024));
     prof_begin(h, pf, XFB_K_MOVIE);
     k_movie<T><<<blocks, 256, 0, s>>>(as<const T>(field_ptr(h, fused(h) ? 1 - parity : 0, mv.field)), h->sx, h->sy, mv.lo[0], mv.lo[1], mv.lo[2], n0, n1, n2,
-                                      mv.interval, h->movie_out[m], h->movie_frames[m], tp);
+                                      mv.interval, h->movie_out[m], h->movie_frames[m], tp, own_lo(h), own_hi(h));
     prof_end(h, pf);
   }
 }
 
 template <typename T>
+void enqueue_update(xfb_handle* h, int off, Prof* pf);
+
+template <typename T>
 void enqueue_step(xfb_handle* h, int off, Prof* pf = nullptr) {
+  enqueue_update<T>(h, off, pf);
+  TimeP tp{h->t_dev, off};
+  enqueue_records<T>(h, static_cast<int>((h->step + off) & 1), tp, h->stream, pf);
+}
+
+// The update of one step (the field kernels, no monitors).
+template <typename T>
+void enqueue_update(xfb_handle* h, int off, Prof* pf) {
   const Compiled& c = h->c;
   TimeP tp{h->t_dev, off};
   const int parity = static_cast<int>((h->step + off) & 1);
@@ -890,12 +929,14 @@ void enqueue_step(xfb_handle* h, int off, Prof* pf = nullptr) {
       launch_fused<T>(h, parity, tp, s);
     }
     if (h->ade_deferred) launch_ade<T>(h, parity, s);
+    prof_end(h, pf);
     if (h->labc_on) {
       const LabcP lp = labc_params(h);
+      prof_begin(h, pf, XFB_K_CORRECT);
       k_labc_apply<T><<<static_cast<unsigned>((lp.off[12] + 127) / 128), 128, 0, s>>>(
           grid_params<T>(h, parity), grid_params<T>(h, 1 - parity), lp);
+      prof_end(h, pf);
     }
-    prof_end(h, pf);
   } else if (c.dim == 3) {
     const int tj = tile_rows<T>(h);
     dim3 blk(h->tk, tj);
@@ -922,7 +963,28 @@ void enqueue_step(xfb_handle* h, int off, Prof* pf = nullptr) {
     k_e2<T><<<grd, bx, 0, s>>>(g, pm, tf, tp, ich);
     prof_end(h, pf);
   }
-  enqueue_records<T>(h, parity, tp, s, pf);
+}
+
+// One step of an x slab, in two parts around the halo exchange: the update
+// writes the owned planes of the new field set; the record samples the
+// monitors on the owned planes (whose interpolations read the refilled halo
+// planes) and advances the step counter.
+template <typename T>
+int slab_update(xfb_handle* h) {
+  enqueue_update<T>(h, 0, nullptr);
+  XFB_CUDA(h, cudaGetLastError());
+  h->slab_pending = true;
+  return XFB_OK;
+}
+
+template <typename T>
+int slab_record(xfb_handle* h) {
+  enqueue_records<T>(h, static_cast<int>(h->step & 1), TimeP{h->t_dev, 0}, h->stream, nullptr);
+  k_bump<<<1, 1, 0, h->stream>>>(h->t_dev, 1);
+  XFB_CUDA(h, cudaGetLastError());
+  h->slab_pending = false;
+  h->step += 1;
+  return XFB_OK;
 }
 
 template <typename T>
@@ -1273,9 +1335,67 @@ int batch_chunk(xfb_batch* b, int n, int t, bool graph) {
 // steps once with each tile configuration (untimed: the first launch of a
 // kernel loads its module), then times a few steps with each (results do
 // not depend on the tile) and keeps the fastest for the rest of the run.
+// Autotuned tile configurations of batches, per (device name, precision,
+// scene sizes), for the life of the process and, when the environment names
+// a file in XFB_AUTOTUNE_CACHE, across processes (one "key tile" line each).
+inline std::string tile_cache_key(const xfb_batch* b) {
+  cudaDeviceProp prop{};
+  cudaGetDeviceProperties(&prop, b->device);
+  std::string k = std::string(prop.name) + "|" + (b->prec == XFB_FP64 ? "fp64" : "fp32");
+  for (const xfb_handle* h : b->hs)
+    k += "|" + std::to_string(h->c.nx) + "x" + std::to_string(h->c.ny) + "x" + std::to_string(h->c.nz);
+  for (char& ch : k)
+    if (ch == ' ') ch = '_';
+  return k;
+}
+
+inline std::map<std::string, int>& tile_cache() {
+  static std::map<std::string, int> m;
+  return m;
+}
+inline std::mutex& tile_cache_mutex() {
+  static std::mutex mu;
+  return mu;
+}
+
+inline int tile_cache_get(const std::string& key) {
+  std::lock_guard<std::mutex> lock(tile_cache_mutex());
+  auto& m = tile_cache();
+  if (m.count(key)) return m[key];
+  if (const char* path = std::getenv("XFB_AUTOTUNE_CACHE")) {
+    std::FILE* f = std::fopen(path, "r");
+    if (f) {
+      char line[4096];
+      while (std::fgets(line, sizeof(line), f)) {
+        std::string s(line);
+        const size_t sp = s.rfind(' ');
+        if (sp != std::string::npos && s.substr(0, sp) == key) m[key] = std::atoi(s.c_str() + sp + 1);
+      }
+      std::fclose(f);
+    }
+  }
+  return m.count(key) ? m[key] : -1;
+}
+
+inline void tile_cache_put(const std::string& key, int tile) {
+  std::lock_guard<std::mutex> lock(tile_cache_mutex());
+  tile_cache()[key] = tile;
+  if (const char* path = std::getenv("XFB_AUTOTUNE_CACHE")) {
+    std::FILE* f = std::fopen(path, "a");
+    if (f) {
+      std::fprintf(f, "%s %d\n", key.c_str(), tile);
+      std::fclose(f);
+    }
+  }
+}
+
 template <typename T>
 int batch_run(xfb_batch* b, long long n) {
   int rc;
+  if (b->tile < 0 && b->tile_req == 0) {  // an earlier autotune of the same scenes on this GPU
+    const int t = tile_cache_get(tile_cache_key(b));
+    if (t >= 0 && t < kStepTileCount) b->tile = t;
+  }
   if (b->tile < 0) {
     if (b->tile_req != 0 || n < 2 * kStepTileCount) {
       b->tile = 1;
@@ -1305,6 +1425,7 @@ int batch_run(xfb_batch* b, long long n) {
       b->tile = 0;
       for (int t = 1; t < kStepTileCount; ++t)
         if (ms[t] < ms[b->tile]) b->tile = t;
+      tile_cache_put(tile_cache_key(b), b->tile);
       n -= kStepTileCount * probe;
     }
   }
@@ -1322,6 +1443,8 @@ int batch_run(xfb_batch* b, long long n) {
   namespace xfb {                                                                          \
   template int init_device<T>(xfb_handle*);                                                \
   template int run_steps<T>(xfb_handle*, long long);                                       \
+  template int slab_update<T>(xfb_handle*);                                                \
+  template int slab_record<T>(xfb_handle*);                                                \
   template int profile_steps<T>(xfb_handle*, long long, double*, long long*);              \
   template int read_field_t<T>(xfb_handle*, int, double*);                                 \
   template int write_field_t<T>(xfb_handle*, int, const double*);                          \

@@ -357,64 +357,65 @@ struct Cell {
 };
 
 // TFSF H corrections of cell (i, jj, kk), in the reference's agency order
-// (TFSFCorrector3DAgency::correctH, src/waveform_source/tfsf/tfsf_corrector.cu:237-271).
-template <typename T>
-__device__ __forceinline__ void tfsf_h(const TfsfP& tf, int i, int jj, int kk, T& hxv, T& hyv, T& hzv) {
+// (TFSFCorrector3DAgency::correctH, src/waveform_source/tfsf/tfsf_corrector.cu:237-271);
+// the incident fields come from `in`.
+template <typename T, class Inc>
+__device__ __forceinline__ void tfsf_h(const TfsfP& tf, const Inc& in, int i, int jj, int kk, T& hxv, T& hyv, T& hzv) {
   const bool iin = i >= tf.is && i <= tf.ie, jin = jj >= tf.js && jj <= tf.je, kin = kk >= tf.ks && kk <= tf.ke;
   if (jin && jj < tf.je && kin) {
-    if (i == tf.is - 1) add_inc(hzv, ey_inc(tf, tf.is, jj, kk), tf.cb[0]);
-    if (i == tf.ie) add_inc(hzv, ey_inc(tf, tf.ie, jj, kk), -tf.cb[0]);
+    if (i == tf.is - 1) add_inc(hzv, in.ey(tf.is, jj, kk), tf.cb[0]);
+    if (i == tf.ie) add_inc(hzv, in.ey(tf.ie, jj, kk), -tf.cb[0]);
   }
   if (iin && i < tf.ie && kin) {
-    if (jj == tf.js - 1) add_inc(hzv, ex_inc(tf, i, tf.js, kk), -tf.cb[1]);
-    if (jj == tf.je) add_inc(hzv, ex_inc(tf, i, tf.je, kk), tf.cb[1]);
+    if (jj == tf.js - 1) add_inc(hzv, in.ex(i, tf.js, kk), -tf.cb[1]);
+    if (jj == tf.je) add_inc(hzv, in.ex(i, tf.je, kk), tf.cb[1]);
   }
   if (iin && jin && jj < tf.je) {
-    if (kk == tf.ks - 1) add_inc(hxv, ey_inc(tf, i, jj, tf.ks), -tf.cb[2]);
-    if (kk == tf.ke) add_inc(hxv, ey_inc(tf, i, jj, tf.ke), tf.cb[2]);
+    if (kk == tf.ks - 1) add_inc(hxv, in.ey(i, jj, tf.ks), -tf.cb[2]);
+    if (kk == tf.ke) add_inc(hxv, in.ey(i, jj, tf.ke), tf.cb[2]);
   }
   if (iin && kin && kk < tf.ke) {
-    if (jj == tf.js - 1) add_inc(hxv, ez_inc(tf, i, tf.js, kk), tf.cb[1]);
-    if (jj == tf.je) add_inc(hxv, ez_inc(tf, i, tf.je, kk), -tf.cb[1]);
+    if (jj == tf.js - 1) add_inc(hxv, in.ez(i, tf.js, kk), tf.cb[1]);
+    if (jj == tf.je) add_inc(hxv, in.ez(i, tf.je, kk), -tf.cb[1]);
   }
   if (iin && i < tf.ie && jin) {
-    if (kk == tf.ks - 1) add_inc(hyv, ex_inc(tf, i, jj, tf.ks), tf.cb[2]);
-    if (kk == tf.ke) add_inc(hyv, ex_inc(tf, i, jj, tf.ke), -tf.cb[2]);
+    if (kk == tf.ks - 1) add_inc(hyv, in.ex(i, jj, tf.ks), tf.cb[2]);
+    if (kk == tf.ke) add_inc(hyv, in.ex(i, jj, tf.ke), -tf.cb[2]);
   }
   if (jin && kin && kk < tf.ke) {
-    if (i == tf.is - 1) add_inc(hyv, ez_inc(tf, tf.is, jj, kk), -tf.cb[0]);
-    if (i == tf.ie) add_inc(hyv, ez_inc(tf, tf.ie, jj, kk), tf.cb[0]);
+    if (i == tf.is - 1) add_inc(hyv, in.ez(tf.is, jj, kk), -tf.cb[0]);
+    if (i == tf.ie) add_inc(hyv, in.ez(tf.ie, jj, kk), tf.cb[0]);
   }
 }
 
 // TFSF E corrections of cell (i, j, k) (TFSFCorrector3DAgency::correctE,
 // src/waveform_source/tfsf/tfsf_corrector.cu:201-236).
-template <typename T>
-__device__ __forceinline__ void tfsf_e(const TfsfP& tf, int i, int j, int k, T& exv, T& eyv, T& ezv) {
+template <typename T, class Inc>
+__device__ __forceinline__ void tfsf_e(const TfsfP& tf, const Inc& in, int i, int j, int k, T& exv, T& eyv, T& ezv) {
   const bool iin = i >= tf.is && i <= tf.ie, jin = j >= tf.js && j <= tf.je, kin = k >= tf.ks && k <= tf.ke;
   if (jin && kin && k < tf.ke) {
-    if (i == tf.is) add_inc(ezv, hy_inc(tf, tf.is - 1, j, k), -tf.ca[0]);
-    if (i == tf.ie) add_inc(ezv, hy_inc(tf, tf.ie, j, k), tf.ca[0]);
+    if (i == tf.is) add_inc(ezv, in.hy(tf.is - 1, j, k), -tf.ca[0]);
+    if (i == tf.ie) add_inc(ezv, in.hy(tf.ie, j, k), tf.ca[0]);
   }
   if (iin && kin && k < tf.ke) {
-    if (j == tf.js) add_inc(ezv, hx_inc(tf, i, tf.js - 1, k), tf.ca[1]);
-    if (j == tf.je) add_inc(ezv, hx_inc(tf, i, tf.je, k), -tf.ca[1]);
+    if (j == tf.js) add_inc(ezv, in.hx(i, tf.js - 1, k), tf.ca[1]);
+    if (j == tf.je) add_inc(ezv, in.hx(i, tf.je, k), -tf.ca[1]);
   }
   if (iin && i < tf.ie && jin) {
-    if (k == tf.ks) add_inc(exv, hy_inc(tf, i, j, tf.ks - 1), tf.ca[2]);
-    if (k == tf.ke) add_inc(exv, hy_inc(tf, i, j, tf.ke), -tf.ca[2]);
+    if (k == tf.ks) add_inc(exv, in.hy(i, j, tf.ks - 1), tf.ca[2]);
+    if (k == tf.ke) add_inc(exv, in.hy(i, j, tf.ke), -tf.ca[2]);
   }
   if (iin && i < tf.ie && kin) {
-    if (j == tf.js) add_inc(exv, hz_inc(tf, i, tf.js - 1, k), -tf.ca[1]);
-    if (j == tf.je) add_inc(exv, hz_inc(tf, i, tf.je, k), tf.ca[1]);
+    if (j == tf.js) add_inc(exv, in.hz(i, tf.js - 1, k), -tf.ca[1]);
+    if (j == tf.je) add_inc(exv, in.hz(i, tf.je, k), tf.ca[1]);
   }
   if (iin && jin && j < tf.je) {
-    if (k == tf.ks) add_inc(eyv, hx_inc(tf, i, j, tf.ks - 1), -tf.ca[2]);
-    if (k == tf.ke) add_inc(eyv, hx_inc(tf, i, j, tf.ke), tf.ca[2]);
+    if (k == tf.ks) add_inc(eyv, in.hx(i, j, tf.ks - 1), -tf.ca[2]);
+    if (k == tf.ke) add_inc(eyv, in.hx(i, j, tf.ke), tf.ca[2]);
   }
   if (jin && j < tf.je && kin) {
-    if (i == tf.is) add_inc(eyv, hz_inc(tf, tf.is - 1, j, k), tf.ca[0]);
-    if (i == tf.ie) add_inc(eyv, hz_inc(tf, tf.ie, j, k), -tf.ca[0]);
+    if (i == tf.is) add_inc(eyv, in.hz(tf.is - 1, j, k), tf.ca[0]);
+    if (i == tf.ie) add_inc(eyv, in.hz(tf.ie, j, k), -tf.ca[0]);
   }
 }
 
@@ -447,7 +448,7 @@ __device__ __forceinline__ void h_cell(const HCtx<T>& x, const T* Fc, const T* F
   hzv = cf.c * f[5 * PL] + cf.y * d_hz_a - cf.x * d_hz_b;
   const TfsfP& tf = x.tf;
   const int j = c.j, k = c.k;
-  if (((KIND & 16) != 0) && (tf_hplane || (c.tfl & 1))) tfsf_h(tf, i, j, k, hxv, hyv, hzv);
+  if (((KIND & 16) != 0) && (tf_hplane || (c.tfl & 1))) tfsf_h(tf, IncTables{tf}, i, j, k, hxv, hyv, hzv);
   constexpr bool PX = (KIND & 1) != 0, PY = (KIND & 2) != 0, PZ = (KIND & 8) != 0;
   if (PX || PY || PZ) {
     const PmlP<T>& pm = x.pm;
@@ -758,6 +759,13 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
           h_cell<T, KIND, L>(x, Fc, Fn, Mc, lut, Hc, i, cell[u], write_h, ox, oy, oz, sxp, tf_hplane, pha[u], ph0[u],
                              ph1[u], hnx[u], hny[u], hnz[u], enx[u], eny[u], enz[u], enm[u]);
     }
+    // H psi of plane i+1, issued now that plane i's is consumed
+    if (PML && i + 1 < i_end) {
+      const int sxp = PX ? slab(i + 1, s.nx, pm.L[0], pm.L[1]) : -1;
+#pragma unroll
+      for (int u = 0; u < R; ++u)
+        pha[u] = prefetch_h_psi<T, KIND>(x, i + 1, sxp, cell[u], (valid >> u) & 1u, ph0[u], ph1[u]);
+    }
     // ---- E pass, plane ie = i-1 ----------------------------------------------
     if (row_warp && ie >= i_start) {
       const int sxe = PX ? slab(ie, s.nx, pm.L[0], pm.L[1]) : -1;
@@ -800,7 +808,7 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
           if (upd_y) eyv = ade_e(ad, 1, abi, m, ey_o, eyv);
           if (upd_z) ezv = ade_e(ad, 2, abi, m, ez_o, ezv);
         }
-        if (TFC && (tf_eplane || (c.tfl & 2))) tfsf_e(tf, ie, j, k, exv, eyv, ezv);
+        if (TFC && (tf_eplane || (c.tfl & 2))) tfsf_e(tf, IncTables{tf}, ie, j, k, exv, eyv, ezv);
         if (PML) {
           const int sy_pml = c.py, sz_pml = c.pz;
           if (sxe >= 0 || sy_pml >= 0 || sz_pml >= 0) {
@@ -841,14 +849,8 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
         eox[u] = enx[u]; eoy[u] = eny[u]; eoz[u] = enz[u];
       }
     }
-    // CPML psi of the next iteration: H of plane i+1, E of plane i
+    // CPML psi of the next iteration: E of plane i
     if (PML) {
-      if (i + 1 < i_end) {
-        const int sxp = PX ? slab(i + 1, s.nx, pm.L[0], pm.L[1]) : -1;
-#pragma unroll
-        for (int u = 0; u < R; ++u)
-          pha[u] = prefetch_h_psi<T, KIND>(x, i + 1, sxp, cell[u], (valid >> u) & 1u, ph0[u], ph1[u]);
-      }
       if (row_warp && do_h && i >= i_start) {
         const int sxe = PX ? slab(i, s.nx, pm.L[0], pm.L[1]) : -1;
 #pragma unroll
@@ -1124,7 +1126,7 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
         T hxv = cf.c * f[3 * PL] + cf.z * d_hx_a - cf.y * d_hx_b;
         T hyv = cf.c * f[4 * PL] + cf.x * d_hy_a - cf.z * d_hy_b;
         T hzv = cf.c * f[5 * PL] + cf.y * d_hz_a - cf.x * d_hz_b;
-        if (TF && (tf_hplane || (tfl[u] & 1))) tfsf_h(tf, i, cj[u], ck[u], hxv, hyv, hzv);
+        if (TF && (tf_hplane || (tfl[u] & 1))) tfsf_h(tf, IncTables{tf}, i, cj[u], ck[u], hxv, hyv, hzv);
         if (PX && sxp >= 0 && in_grid[u]) {
           const long long p = static_cast<long long>(sxp) * s.sx + go[u];
           const T a = pm.ah[0][i], b = pm.bh[0][i];
@@ -1167,6 +1169,15 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
         enm[u] = m;
       }
     }
+    // column-axis H psi of plane i+1, issued now that plane i's is consumed:
+    // the E pass, the stores and the barrier cover its latency
+    if (PML && (PY || PZ) && i + 1 < i_end) {
+      const T* a0 = hr0 + static_cast<long long>(i + 1) * psx;
+      const T* a1 = hr1 + static_cast<long long>(i + 1) * psx;
+#pragma unroll
+      for (int u = 0; u < R; ++u)
+        if (sp[u] >= 0) { ph0[u] = a0[so[u]]; ph1[u] = a1[so[u]]; }
+    }
     // ---- E pass, plane ie = i-1 ------------------------------------------------
     const bool tf_eplane = TF && tf.on && (ie == tf.is || ie == tf.ie);
     if (row_warp && ie >= i_start) {
@@ -1193,7 +1204,7 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
         T exv = cf.c * eox[u] - cf.z * d_ex_a + cf.y * d_ex_b;
         T eyv = cf.c * eoy[u] - cf.x * d_ey_a + cf.z * d_ey_b;
         T ezv = cf.c * eoz[u] - cf.y * d_ez_a + cf.x * d_ez_b;
-        if (TF && (tf_eplane || (tfl[u] & 2))) tfsf_e(tf, ie, cj[u], ck[u], exv, eyv, ezv);
+        if (TF && (tf_eplane || (tfl[u] & 2))) tfsf_e(tf, IncTables{tf}, ie, cj[u], ck[u], exv, eyv, ezv);
         if (PML) {
           const bool jpos = cj[u] > 0, kpos = ck[u] > 0;
           const bool upd_x = jpos && kpos, upd_y = ipos && kpos, upd_z = ipos && jpos;
@@ -1237,19 +1248,13 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
         eox[u] = enx[u]; eoy[u] = eny[u]; eoz[u] = enz[u];
       }
     }
-    // column-axis psi of the next iteration: H of plane i+1, E of plane i
-    if (PML && (PY || PZ)) {
-      const T* a0 = hr0 + static_cast<long long>(i + 1) * psx;
-      const T* a1 = hr1 + static_cast<long long>(i + 1) * psx;
+    // column-axis E psi of the next iteration (plane i)
+    if (PML && (PY || PZ) && row_warp && do_h && i >= i_start) {
       const T* b0 = er0 + static_cast<long long>(i) * psx;
       const T* b1 = er1 + static_cast<long long>(i) * psx;
-      const bool nh = i + 1 < i_end, ne = row_warp && do_h && i >= i_start;
 #pragma unroll
       for (int u = 0; u < R; ++u)
-        if (sp[u] >= 0) {
-          if (nh) { ph0[u] = a0[so[u]]; ph1[u] = a1[so[u]]; }
-          if (ne) { pe0[u] = b0[so[u]]; pe1[u] = b1[so[u]]; }
-        }
+        if (sp[u] >= 0) { pe0[u] = b0[so[u]]; pe1[u] = b1[so[u]]; }
     }
     fence_proxy_async();             // this thread's tile writes before the next iteration's bulk stores
     if (tid == 0) bulk_wait_read();  // this iteration's stores have read their tiles

@@ -33,6 +33,7 @@ struct xfb_handle {
   int tk = 32, tj = 16;
   int path = XFB_PATH_AUTO;  // resolved at init: XFB_PATH_SPLIT or XFB_PATH_FUSED
   int graph_on = 1, graph_steps = 64;
+  int coeff_storage = XFB_COEFF_NATIVE;  // rounding of the update-coefficient LUT (xfb_set_coeff_storage)
   std::map<int, cudaGraphExec_t> graphs;
   std::vector<Buf> bufs;
   size_t bytes = 0;
@@ -123,6 +124,12 @@ struct xfb_handle {
   cudaEvent_t rb_ev[2] = {};
   // bytes this handle has copied host -> device and device -> host
   long long h2d_bytes = 0, d2h_bytes = 0;
+  // x-slab decomposition (xfb_set_slab): the handle updates cells
+  // [slab_i0, slab_i1) along x of the full grid; planes slab_i0 - 1 and
+  // slab_i1 are halos, refilled between xfb_slab_update and xfb_slab_record
+  // (xfb_slab_exchange, or the host's own collective); -1: the whole grid
+  int slab_i0 = 0, slab_i1 = -1;
+  bool slab_pending = false;  // an update awaits its record
 };
 
 // A batch of scenes stepped together: one launch of the one-sweep kernel per
@@ -190,6 +197,13 @@ inline int step_tile_index(int tj) { return tj <= 8 ? 0 : 1; }
 constexpr int kStepTileCount = 3;
 constexpr int kStepTileRows[kStepTileCount] = {8, 16, 14};
 bool plain(const xfb_handle* h);
+inline bool is_slab(const xfb_handle* h) { return h->slab_i1 >= 0; }
+// planes i whose cells and monitors this handle owns (the last slab also owns
+// the node plane i = nx of the E components)
+inline int own_lo(const xfb_handle* h) { return is_slab(h) ? h->slab_i0 : 0; }
+inline int own_hi(const xfb_handle* h) {
+  return is_slab(h) && h->slab_i1 < h->c.nx ? h->slab_i1 : h->c.nx + 1;
+}
 int cur_set(const xfb_handle* h);
 void* field_ptr(const xfb_handle* h, int set, int q);
 long long off3(const xfb_handle* h, int i, int j, int k);
@@ -201,6 +215,8 @@ int check_handle(xfb_handle* h, bool need_init);
 // ---- engine (engine.cuh, instantiated for float and double) -------------
 template <typename T> int init_device(xfb_handle* h);
 template <typename T> int run_steps(xfb_handle* h, long long n);
+template <typename T> int slab_update(xfb_handle* h);
+template <typename T> int slab_record(xfb_handle* h);
 template <typename T> int profile_steps(xfb_handle* h, long long n, double* ms, long long* launches);
 template <typename T> int read_field_t(xfb_handle* h, int f, double* dst);
 template <typename T> int write_field_t(xfb_handle* h, int f, const double* src);

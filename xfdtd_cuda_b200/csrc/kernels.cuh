@@ -120,6 +120,18 @@ __device__ __forceinline__ double hz_inc(const TfsfP& s, int i, int j, int k) {
   return s.trh[2] * aux_lerp(s.h_aux, p);
 }
 
+// The incident fields of a step's tables (projection arrays, the step's
+// auxiliary rows) behind one interface for the correction routines.
+struct IncTables {
+  const TfsfP& s;
+  __device__ __forceinline__ double ex(int i, int j, int k) const { return ex_inc(s, i, j, k); }
+  __device__ __forceinline__ double ey(int i, int j, int k) const { return ey_inc(s, i, j, k); }
+  __device__ __forceinline__ double ez(int i, int j, int k) const { return ez_inc(s, i, j, k); }
+  __device__ __forceinline__ double hx(int i, int j, int k) const { return hx_inc(s, i, j, k); }
+  __device__ __forceinline__ double hy(int i, int j, int k) const { return hy_inc(s, i, j, k); }
+  __device__ __forceinline__ double hz(int i, int j, int k) const { return hz_inc(s, i, j, k); }
+};
+
 // field += inc * coefficient (tfsf_corrector.cuh:137,151,166), in double.
 template <typename T>
 __device__ __forceinline__ void add_inc(T& f, double inc, double coef) {
@@ -669,6 +681,7 @@ struct NfP {
   long long total_steps;
   double* ring;               // [kNfRing][4][npts] samples of the buffered steps
   long long* done;            // steps accumulated by the last flush
+  int own_lo, own_hi;         // planes i this handle samples (an x slab: the planes it owns)
 };
 
 // Advance the accumulators of point pt over steps lo .. hi-1 taken from the
@@ -771,6 +784,7 @@ __global__ void k_nf2ff(GridP<T> g, NfP nf, TimeP tp) {
   if (axis == 0) { const int nk = b[5] - b[4]; i = pos ? b[1] : b[0]; j = b[2] + static_cast<int>(q / nk); k = b[4] + static_cast<int>(q % nk); }
   else if (axis == 1) { const int nk = b[5] - b[4]; j = pos ? b[3] : b[2]; i = b[0] + static_cast<int>(q / nk); k = b[4] + static_cast<int>(q % nk); }
   else { const int nj = b[3] - b[2]; k = pos ? b[5] : b[4]; i = b[0] + static_cast<int>(q / nj); j = b[2] + static_cast<int>(q % nj); }
+  if (i < nf.own_lo || i >= nf.own_hi) return;  // another slab's point: its ring and sums stay zero here
   const long long x = static_cast<long long>(i) * g.sx + static_cast<long long>(j) * g.sy + k;
   double hb, ha, eb, ea;  // interpolated H_b, H_a, E_b, E_a at the face centre
   nf_face_samples(g, axis, x, ha, hb, ea, eb);
@@ -892,15 +906,17 @@ __global__ void k_probe(GridP<T> g, ProbeP pr, TimeP tp) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= pr.n) return;
   const long long t = cur_step(tp);
+  const int fld = pr.field[p];
+  if (fld < 0) return;  // a probe of another x slab
   const T* f[6] = {g.ex, g.ey, g.ez, g.hx, g.hy, g.hz};
-  pr.out[p * pr.total_steps + t] = static_cast<double>(f[pr.field[p]][pr.idx[p]]);
+  pr.out[p * pr.total_steps + t] = static_cast<double>(f[fld][pr.idx[p]]);
 }
 
 // Movie frame: copies the component box every `interval` steps
 // (MovieMonitor<F>::update, src/monitor/movie_monitor.cu:17-46).
 template <typename T>
 __global__ void k_movie(const T* fld, long long sx, long long sy, int lo0, int lo1, int lo2, int n0, int n1, int n2,
-                        int interval, double* out, long long n_frames, TimeP tp) {
+                        int interval, double* out, long long n_frames, TimeP tp, int own_lo, int own_hi) {
   const long long t = cur_step(tp);
   if (t % interval != 0) return;
   const long long frame = t / interval;
@@ -911,6 +927,7 @@ __global__ void k_movie(const T* fld, long long sx, long long sy, int lo0, int l
     const int c = static_cast<int>(e % n2);
     const int b = static_cast<int>((e / n2) % n1);
     const int a = static_cast<int>(e / (static_cast<long long>(n1) * n2));
+    if (lo0 + a < own_lo || lo0 + a >= own_hi) continue;  // a plane of another x slab
     out[frame * per + e] = static_cast<double>(fld[static_cast<long long>(lo0 + a) * sx + static_cast<long long>(lo1 + b) * sy + lo2 + c]);
   }
 }

@@ -245,8 +245,10 @@ def reflection_errors(weights: np.ndarray, seed: int = 9, interior: int = 40, st
                       device: int = 0, courant: float = 0.9, modes=("pec", "learned")):
     """Probe error against the CPML judge of the same scene (relative L2 over
     all probe series) for each of `modes`: "pec" (bare walls), "mur" (the
-    boundary with an all-zero network), "learned" (the given weights).
-    Probes sit in the scattered-field region two cells inside every wall."""
+    boundary with an all-zero network), "learned" (the given weights),
+    "cpml3" (a 3-cell CPML outside the interior: the depth of the learned
+    stencil).  Probes sit in the scattered-field region two cells inside
+    every wall of the interior."""
     dl = 5e-3
     h_ = interior * dl / 2
     q = h_ - 2.5 * dl
@@ -254,7 +256,8 @@ def reflection_errors(weights: np.ndarray, seed: int = 9, interior: int = 40, st
              [((-0.1 * q, 0.25 * q, sz * q), 0) for sz in (-1, 1)]
     series = {}
     for mode in ("cpml",) + tuple(modes):
-        sim = scatter_scene(seed, interior=interior, pml=pml if mode == "cpml" else 0, probes=probes, courant=courant)
+        thick = {"cpml": pml, "cpml3": 3}.get(mode, 0)
+        sim = scatter_scene(seed, interior=interior, pml=thick, probes=probes, courant=courant)
         sc, keep = sim.lower()
         h = Handle(sc, keep)
         h.set_device(device)

@@ -621,6 +621,10 @@ class Handle:
     def set_kernel_path(self, path: int):
         self._c(self.lib.xfb_set_kernel_path(self.h, int(path)))
 
+    def set_coeff_storage(self, storage: int):
+        """Round the coefficient LUT to FP16 / BF16 at init (storage trial)."""
+        self._c(self.lib.xfb_set_coeff_storage(self.h, int(storage)))
+
     def set_graph(self, enabled: bool, steps: int = 64):
         self._c(self.lib.xfb_set_graph(self.h, int(enabled), int(steps)))
 
