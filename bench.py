@@ -312,27 +312,30 @@ def batched_compare(local: int, steps: int, warmup: int, solo_steps: int = 8):
 
 def cylinder2d_compare(local: int, steps: int = 4000):
     """C2: 2-D TMz PEC cylinder (r = 50 cells) in 1024^2 cells + 10-cell CPML
-    (1044^2), TFSF Gaussian, 4000 steps, in FP32 and FP64; device-timed
-    Mcell-updates/s of each and the relative L2 error of the FP32 probe
-    series against the FP64 run (the FP64 engine is bit-identical to the CPU
-    restatement of the reference)."""
+    (1044^2), TFSF Gaussian, 4000 steps, in FP32 and FP64 on the temporally
+    blocked kernel (9 steps per launch), and FP32 with one launch per step;
+    device-timed Mcell-updates/s of each and the relative L2 error of the
+    FP32 probe series against the FP64 run (the FP64 engine is bit-identical
+    to the CPU restatement of the reference)."""
     import numpy as np
     import xfdtd_cuda_b200 as X
     from xfdtd_cuda_b200 import configs
     out, series = {"workload": "2-D TMz PEC cylinder, 1044^2 cells (1024^2 + 10-cell CPML), TFSF, 8 probes, "
                                f"{steps} steps", "unit": UNIT}, {}
-    for prec in ("fp32", "fp64"):
+    for key, prec, tb in (("fp32", "fp32", 9), ("fp64", "fp64", 9), ("fp32_one_launch_per_step", "fp32", 0)):
         sim = configs.cylinder_2d(precision=prec)
         sc, keep = sim.lower()
         h = X.Handle(sc, keep)
         h.set_device(local)
+        h.set_temporal_block(tb)
         h.init(steps)
         ms = h.timed_step(steps)
         gi = h.info()
         cells = gi.nx * gi.ny
-        series[prec] = np.concatenate([h.read_probe(p) for p in range(len(h.probe_desc))])
-        out[prec] = {"value": cells * steps / (ms / 1e3) / 1e6, "ms_per_step": ms / steps,
-                     "launches_per_step": gi.launches_per_step}
+        series[key] = np.concatenate([h.read_probe(p) for p in range(len(h.probe_desc))])
+        out[key] = {"value": cells * steps / (ms / 1e3) / 1e6, "ms_per_step": ms / steps,
+                    "launches_per_step": gi.launches_per_step if tb == 0 else 1.0 / tb,
+                    "steps_per_launch": tb or 1}
         h.close()
     out["fp32_probe_rel_l2_vs_fp64"] = float(np.linalg.norm(series["fp32"] - series["fp64"]) /
                                              np.linalg.norm(series["fp64"]))

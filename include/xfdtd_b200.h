@@ -266,6 +266,14 @@ int xfb_profile_kernels(xfb_handle* h, long long n, double* ms, long long* launc
 /* Select the 3-D kernel path (enum xfb_kernel_path); before xfb_init. */
 int xfb_set_kernel_path(xfb_handle* h, int path);
 
+/* 2-D TMz scenes on the one-sweep path: steps advanced per launch by the
+ * temporally blocked kernel (each CTA advances its tile plus a halo of that
+ * many cells in shared memory and records its probes every step), odd, at
+ * most 31; default 9; 0 launches once per step.  Scenes with movie monitors
+ * or CPML slabs wider than a tile's psi tables step once per launch.  Results
+ * are identical either way.  Before xfb_init. */
+int xfb_set_temporal_block(xfb_handle* h, int steps);
+
 /* Storage trial of the update coefficients, no counterpart in the reference
  * (its 18 per-cell coefficient arrays are FP64, fdtd_coefficient.cuh:15-168).
  * NATIVE keeps them in the compute precision; FP16 / BF16 round every entry

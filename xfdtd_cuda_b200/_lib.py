@@ -146,6 +146,7 @@ SIGNATURES = [
     ("xfb_set_graph", C.c_int, [_H, C.c_int, C.c_int]),
     ("xfb_set_kernel_path", C.c_int, [_H, C.c_int]),
     ("xfb_set_coeff_storage", C.c_int, [_H, C.c_int]),
+    ("xfb_set_temporal_block", C.c_int, [_H, C.c_int]),
     ("xfb_get_grid_info", C.c_int, [_H, C.POINTER(GridInfo)]),
     ("xfb_read_field", C.c_int, [_H, C.c_int, _dp, C.c_size_t]),
     ("xfb_write_field", C.c_int, [_H, C.c_int, _dp, C.c_size_t]),

@@ -132,6 +132,7 @@ int launches_per_step(const xfb_handle* h) {
   if (fused(h)) {
     bulk = c.dim == 2 ? 1 : (h->n_step_items[step_tile_index(h->tj)] > 0 ? 1 : 0) + (h->ade_deferred ? 1 : 0);
   }
+  if (h->tb_on) return 1;  // one blocked launch per tb_steps steps, probes recorded inside
   return bulk + (c.nf_on ? 1 : 0) + (c.td_on ? 2 : 0) + (c.probes.empty() ? 0 : 1) +
          static_cast<int>(c.movies.size());
 }
@@ -293,6 +294,15 @@ int xfb_set_kernel_path(xfb_handle* h, int path) {
   if (path < XFB_PATH_AUTO || path > XFB_PATH_PLAIN) return set_err(h, XFB_ERR_INVALID, "unknown kernel path");
   if (h->inited) return set_err(h, XFB_ERR_STATE, "set the kernel path before xfb_init");
   h->path = path;
+  return XFB_OK;
+}
+
+int xfb_set_temporal_block(xfb_handle* h, int steps) {
+  if (!h) return set_err(nullptr, XFB_ERR_INVALID, "null handle");
+  if (steps < 0 || (steps > 0 && (steps % 2 == 0 || steps > 31)))
+    return set_err(h, XFB_ERR_INVALID, "steps per launch must be 0 (off) or odd, at most 31");
+  if (h->inited) return set_err(h, XFB_ERR_STATE, "set the temporal blocking before xfb_init");
+  h->tb_steps = steps;
   return XFB_OK;
 }
 

@@ -20,6 +20,7 @@
 #include "kernels.cuh"
 #include "labc.cuh"
 #include "plain.cuh"
+#include "tb2d.cuh"
 
 namespace xfb {
 
@@ -28,6 +29,39 @@ inline int upload_ade_runs(xfb_handle* h);
 inline int upload_td(xfb_handle* h);
 template <typename T>
 int encode_stage_maps(xfb_handle* h);
+
+// Tile of the blocked 2-D step: TJ + 2 S + 1 columns fill a shared row of
+// kTbPitch, TI rows keep the tile count within two CTAs per SM when it can
+// and the tile's shared memory within a CTA's 227 KB.
+// False (one launch per step) when blocking is off, the scene has movie
+// monitors (recorded between steps), or a tile's region would hold more CPML
+// rows or columns than its psi tables.
+template <typename T>
+bool tb2d_plan(xfb_handle* h) {
+  const Compiled& c = h->c;
+  const int S = h->tb_steps;
+  if (c.dim != 2 || S <= 0 || !c.movies.empty()) return false;
+  const int TJ = kTbPitch - 1 - 2 * S;
+  if (TJ < 16) return false;
+  const int ntj = (c.ny + TJ - 1) / TJ;
+  int TI = (c.nx + std::max(1, 296 / ntj) - 1) / std::max(1, 296 / ntj);
+  TI = std::min(64, std::max(16, TI));
+  // the tile's shared memory within the 227 KB a CTA may use
+  while (TI > 16 && TbLayout<T>(TI + 2 * S + 1, c.n_mat).bytes > 227u * 1024u) --TI;
+  if (TbLayout<T>(TI + 2 * S + 1, c.n_mat).bytes > 227u * 1024u) return false;
+  auto fits = [&](int n, int tile, int lo, int hi) {  // slab cells of every tile's region along one axis
+    for (int a0 = 0; a0 < n; a0 += tile) {
+      int cnt = 0;
+      for (int q = std::max(0, a0 - S); q <= std::min(n - 1, a0 + tile + S); ++q) cnt += (q < lo || q >= n - hi) ? 1 : 0;
+      if (cnt > kTbSlab) return false;
+    }
+    return true;
+  };
+  if (!fits(c.nx, TI, c.pml[0], c.pml[1]) || !fits(c.ny, TJ, c.pml[2], c.pml[3])) return false;
+  h->tb_ti = TI;
+  h->tb_tj = TJ;
+  return true;
+}
 
 // Update coefficients rounded to a 16-bit storage format (round to nearest
 // even) and widened back: what a LUT stored in that format would hold.
@@ -143,6 +177,16 @@ int init_device(xfb_handle* h) {
       if ((rc = alloc(h, &h->psi_h1[0], bx, true))) return rc;
       if ((rc = alloc(h, &h->psi_h1[3], by, true))) return rc;
     }
+    h->tb_on = fused(h) && tb2d_plan<T>(h);
+    if (h->tb_on) {  // the E-side psi alternates too on the blocked path
+      if ((rc = alloc(h, &h->psi_e1[0], bx, true))) return rc;
+      if ((rc = alloc(h, &h->psi_e1[1], by, true))) return rc;
+      // the kernel's shared-memory limit, set (and the kernel loaded) here,
+      // outside any stream capture of the step loop
+      const TbLayout<T> lay(h->tb_ti + 2 * h->tb_steps + 1, c.n_mat);
+      XFB_CUDA(h, cudaFuncSetAttribute(k_step2_tb<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(lay.bytes)));
+    }
   }
   // TFSF
   if (c.tfsf_on) {
@@ -235,6 +279,8 @@ int init_device(xfb_handle* h) {
   h->t_dev = static_cast<long long*>(p);
   if ((rc = alloc(h, &p, sizeof(unsigned long long), false))) return rc;
   h->scratch_u64 = static_cast<unsigned long long*>(p);
+  if ((rc = alloc(h, &p, sizeof(int), false))) return rc;
+  h->scratch_err = static_cast<int*>(p);
   XFB_CUDA(h, cudaStreamSynchronize(h->stream));
   return XFB_OK;
 }
@@ -861,7 +907,7 @@ void enqueue_records(xfb_handle* h, int parity, TimeP tp, cudaStream_t s, Prof* 
     k_nftd_bins<<<(6 * td.span + 127) / 128, 128, 0, s>>>(td, tp);
     prof_end(h, pf);
   }
-  if (!c.probes.empty()) {
+  if (!c.probes.empty() && !h->tb_on) {  // the blocked 2-D kernel records its own
     ProbeP pr{static_cast<int>(c.probes.size()), h->probe_idx, h->probe_field, h->probe_out, c.total_steps};
     prof_begin(h, pf, XFB_K_PROBE);
     k_probe<T><<<(pr.n + 127) / 128, 128, 0, s>>>(g, pr, tp);
@@ -881,6 +927,8 @@ void enqueue_records(xfb_handle* h, int parity, TimeP tp, cudaStream_t s, Prof* 
 
 template <typename T>
 void enqueue_update(xfb_handle* h, int off, Prof* pf);
+template <typename T>
+void launch_tb2d(xfb_handle* h, int off, int S);
 
 template <typename T>
 void enqueue_step(xfb_handle* h, int off, Prof* pf = nullptr) {
@@ -917,7 +965,9 @@ void enqueue_update(xfb_handle* h, int off, Prof* pf) {
     prof_end(h, pf);
   } else if (fused(h)) {
     prof_begin(h, pf, XFB_K_STEP);
-    if (c.dim == 2) {
+    if (c.dim == 2 && h->tb_on) {
+      launch_tb2d<T>(h, off, 1);  // a single step (profiling): the blocked kernel with S = 1
+    } else if (c.dim == 2) {
       // one-sweep 2-D step: 128-column blocks over plane chunks
       const int gx = (c.ny + 127) / 128;
       const int nch = chunks_for(gx, c.nx, 160);
@@ -987,9 +1037,35 @@ int slab_record(xfb_handle* h) {
   return XFB_OK;
 }
 
+// One blocked 2-D launch: steps [off, off + S) of the chunk (S odd), read
+// set and E-side psi buffer (step & 1), write the others.
+template <typename T>
+void launch_tb2d(xfb_handle* h, int off, int S) {
+  const Compiled& c = h->c;
+  const int parity = static_cast<int>((h->step + off) & 1);
+  const TbLayout<T> lay(h->tb_ti + 2 * S + 1, c.n_mat);
+  T* ez_x[2] = {as<T>(h->psi[1]), as<T>(h->psi_e1[0])};
+  T* ez_y[2] = {as<T>(h->psi[2]), as<T>(h->psi_e1[1])};
+  ProbeP pr{static_cast<int>(c.probes.size()), h->probe_idx, h->probe_field, h->probe_out, c.total_steps};
+  const dim3 grid((c.ny + h->tb_tj - 1) / h->tb_tj, (c.nx + h->tb_ti - 1) / h->tb_ti);
+  k_step2_tb<T><<<grid, kTbThreads, lay.bytes, h->stream>>>(
+      grid_params<T>(h, parity), grid_params<T>(h, 1 - parity), pml_params<T>(h), psi_h_set<T>(h, parity),
+      psi_h_set<T>(h, 1 - parity), ez_x[parity], ez_y[parity], ez_x[1 - parity], ez_y[1 - parity], tfsf_params(h),
+      TimeP{h->t_dev, off}, pr, S, h->tb_ti, h->tb_tj, c.n_mat, h->scratch_err);
+}
+
 template <typename T>
 void enqueue_chunk(xfb_handle* h, int n) {
-  for (int s = 0; s < n; ++s) enqueue_step<T>(h, s);
+  if (h->tb_on) {  // blocked 2-D: launches of odd step counts (each flips the sets once)
+    for (int off = 0; off < n;) {
+      int S = std::min(h->tb_steps, n - off);
+      if (S % 2 == 0) --S;
+      launch_tb2d<T>(h, off, S);
+      off += S;
+    }
+  } else {
+    for (int s = 0; s < n; ++s) enqueue_step<T>(h, s);
+  }
   k_bump<<<1, 1, 0, h->stream>>>(h->t_dev, n);
 }
 

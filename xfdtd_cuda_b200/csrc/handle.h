@@ -34,6 +34,13 @@ struct xfb_handle {
   int path = XFB_PATH_AUTO;  // resolved at init: XFB_PATH_SPLIT or XFB_PATH_FUSED
   int graph_on = 1, graph_steps = 64;
   int coeff_storage = XFB_COEFF_NATIVE;  // rounding of the update-coefficient LUT (xfb_set_coeff_storage)
+  // 2-D temporal blocking (k_step2_tb): steps per launch (odd; 0: one launch
+  // per step), whether init enabled it, the tile rows / columns, and the
+  // second set of the E-side psi (ez_x, ez_y) it alternates with psi[1], psi[2]
+  int tb_steps = 9;
+  bool tb_on = false;
+  int tb_ti = 0, tb_tj = 0;
+  void* psi_e1[2] = {};
   std::map<int, cudaGraphExec_t> graphs;
   std::vector<Buf> bufs;
   size_t bytes = 0;
@@ -90,6 +97,7 @@ struct xfb_handle {
   std::vector<long long> movie_frames;
   long long* t_dev = nullptr;
   unsigned long long* scratch_u64 = nullptr;
+  int* scratch_err = nullptr;  // blocked 2-D kernel: 2 when a tile's region outgrew its psi tables
   void* plain_c[18] = {};  // per-cell coefficient arrays of the plain path
   // one-sweep step work items per tile configuration
   // (int4: k tile | region kind << 16, j tile, first plane, end plane)

@@ -621,6 +621,10 @@ class Handle:
     def set_kernel_path(self, path: int):
         self._c(self.lib.xfb_set_kernel_path(self.h, int(path)))
 
+    def set_temporal_block(self, steps: int):
+        """Steps per launch of the blocked 2-D kernel (odd; 0: one launch per step)."""
+        self._c(self.lib.xfb_set_temporal_block(self.h, int(steps)))
+
     def set_coeff_storage(self, storage: int):
         """Round the coefficient LUT to FP16 / BF16 at init (storage trial)."""
         self._c(self.lib.xfb_set_coeff_storage(self.h, int(storage)))
