@@ -464,6 +464,73 @@ const char* xfb_last_error(const xfb_handle* h);
 const char* xfb_status_string(int status);
 int xfb_abi_version(void);
 
+/* ---- scenes compiled by XFDTD_CORE ----------------------------------------
+ * The arrays XFDTD_CORE's Simulation::init computes and the reference's *HD
+ * wrappers copy to the device (src/simulation/simulation_hd.cu:259-398:
+ * FDTDCoefficientHD, fdtd_coefficient_hd.cu:9-51; PMLCorrectorHD,
+ * pml_corrector_hd.cu:8-34; TFSFCorrectorHD, tfsf_corrector_hd.cu:9-73;
+ * the NF2FF and monitor wrappers; ADEMethodStorageHD, ade_method_hd.cu:5-24),
+ * as plain host arrays.  include/xfdtd_b200/xfdtd_core_adapter.hpp fills this
+ * struct from an xfdtd::Simulation.  3-D scenes; every array is row-major
+ * (k fastest) and is read, not kept, by xfb_create_from_arrays. */
+typedef struct xfb_core_arrays {
+  int precision;                /* enum xfb_precision of the device engine  */
+  int nx, ny, nz;               /* cells, CPML included                      */
+  double dx, dy, dz, dt;
+  double origin[3];             /* position of node (0, 0, 0)                */
+  /* the 18 FDTDCoefficient arrays (cexe cexhy cexhz ceye ceyhz ceyhx ceze
+   * cezhx cezhy chxh chxey chxez chyh chyez chyex chzh chzex chzey), each in
+   * the shape of its field (Ex (nx, ny+1, nz+1) ... Hz (nx, ny, nz+1)) */
+  const double* coeff[18];
+  /* ADE (enum xfb_ade_kind, NONE without dispersive media): per cell
+   * (nx, ny, nz) the dispersive flag, ceep and cejsum; per cell and pole
+   * (nx, ny, nz, poles) cjj cjjp cjen cje cjep cjsj cjsjp */
+  int ade_kind, ade_poles;
+  const double* ade_cell[3];
+  const double* ade_pole[7];
+  /* CPML thickness per face and the profiles along each axis: a/b of the E
+   * nodes (length n + 1), of the H half nodes (length n), zero outside */
+  int pml[6];
+  const double* pml_ae[3];
+  const double* pml_be[3];
+  const double* pml_ah[3];
+  const double* pml_bh[3];
+  /* TFSF: box nodes, projections (length box_n + 1 and box_n + 2), field
+   * transforms, ca/cb per axis, and the incident tables: e_inc row t = E at
+   * t dt (aux_nl + 1 entries, inc_steps + 1 rows), h_inc row t = H at
+   * (t + 1/2) dt (aux_nl entries, inc_steps rows) */
+  int tfsf_enabled;
+  int tfsf_box[6];
+  const double* tfsf_proj_int[3];
+  const double* tfsf_proj_half[3];
+  double tfsf_transform_e[3], tfsf_transform_h[3], tfsf_ca[3], tfsf_cb[3];
+  int aux_nl;
+  long long inc_steps;
+  const double* e_inc;
+  const double* h_inc;
+  /* frequency-domain NF2FF: box nodes and frequencies */
+  int nf2ff_enabled;
+  int nf2ff_box[6];
+  int n_freqs;
+  const double* freqs;
+  /* time-domain NF2FF: box nodes and the observation direction (rad) */
+  int nf2ff_td_enabled;
+  int nf2ff_td_box[6];
+  double nf2ff_td_theta, nf2ff_td_phi;
+  int n_probes;
+  const xfb_probe* probes;
+  int n_movies;
+  const xfb_movie* movies;
+} xfb_core_arrays;
+
+/* A handle from arrays XFDTD_CORE compiled: the replacement of
+ * SimulationHD(xfdtd::Simulation*) for callers that keep XFDTD_CORE.  Cells
+ * whose 18 coefficients (and ADE coefficients) are bitwise equal share a
+ * material of the engine's coefficient table: at most 255 distinct sets, each
+ * of the isotropic form the update uses (cexhy = -ceyhx, ...), else
+ * XFB_ERR_INVALID.  xfb_init may not size a run beyond inc_steps. */
+int xfb_create_from_arrays(const xfb_core_arrays* arrays, xfb_handle** out);
+
 /* ---- compiled-scene export (host only; used by the CPU restatement) ------ */
 /* The arrays the host scene compiler produced, i.e. what XFDTD_CORE would hand
  * to the reference's *HD wrappers.  Pointers stay valid until xfb_destroy. */

@@ -1,0 +1,2 @@
+#pragma once
+#include "xfdtd/fake_core.h"

@@ -77,6 +77,20 @@ def test_fp64_dielectric_sphere_bitexact(path):
 
 
 @pytest.mark.parametrize("path", PATHS)
+def test_fp64_h_field_movies_bitexact(path):
+    # movies of the three H components (the reference instantiates
+    # MovieMonitor<HX..HZ>, movie_monitor.cu:136-138, but never dispatches them)
+    sim = small_sphere()
+    for f in (3, 4, 5):
+        add_movie(sim, field=f, interval=6)
+    h, o = run_pair(sim, 60, path)
+    check_all(h, o, 3, 3, 3, nf=False)
+    for m in range(3):
+        assert np.array_equal(h.read_movie(m), o.movie(m))
+        assert np.abs(h.read_movie(m)).max() > 0
+
+
+@pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("kind", ["drude", "debye", "drude_lorentz", "mlorentz"])
 @pytest.mark.parametrize("radius", [0.03, 0.018])
 def test_fp64_ade_bitexact(kind, path, radius):

@@ -130,6 +130,7 @@ def _dielectric(prec="fp64"):
     sim.addNF2FF(X.NFFFTTimeDomain(2, 2, 2, "", 0.7, 1.9))
     from xfdtd_cuda_b200.simulation import Cube, FieldMonitor, MovieMonitor, Vector
     sim.addMonitor(MovieMonitor(FieldMonitor(Cube(Vector(-0.07, -0.07, 0.0), Vector(0.14, 0.14, 0.005)), L.EZ), 7))
+    sim.addMonitor(MovieMonitor(FieldMonitor(Cube(Vector(-0.07, 0.0, -0.07), Vector(0.14, 0.005, 0.14)), L.HY), 5))
     return sim
 
 
@@ -164,7 +165,8 @@ def test_slab_group_matches_whole_grid_fp64(scene, n):
         for w in range(4):
             assert np.array_equal(g.read_nf2ff(0, face, w), ref.read_nf2ff(0, face, w)), (face, w)
     if scene == "dielectric":
-        assert np.array_equal(g.read_movie(0), ref.read_movie(0))
+        for m in range(2):  # an E-field and an H-field movie across the slab boundaries
+            assert np.array_equal(g.read_movie(m), ref.read_movie(m))
         for w in range(6):  # time-domain sums: the same terms split by slab, then added
             a, b = g.read_nf2ff_td(w), ref.read_nf2ff_td(w)
             assert np.linalg.norm(a - b) <= 1e-12 * max(np.linalg.norm(b), 1e-300)

@@ -105,6 +105,22 @@ class GridInfo(C.Structure):
 _dp = C.POINTER(C.c_double)
 
 
+class CoreArrays(C.Structure):
+    """xfb_core_arrays: a scene as the arrays XFDTD_CORE compiles."""
+    _fields_ = [
+        ("precision", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double), ("dt", C.c_double), ("origin", C.c_double * 3),
+        ("coeff", _dp * 18), ("ade_kind", C.c_int), ("ade_poles", C.c_int), ("ade_cell", _dp * 3), ("ade_pole", _dp * 7),
+        ("pml", C.c_int * 6), ("pml_ae", _dp * 3), ("pml_be", _dp * 3), ("pml_ah", _dp * 3), ("pml_bh", _dp * 3),
+        ("tfsf_enabled", C.c_int), ("tfsf_box", C.c_int * 6), ("tfsf_proj_int", _dp * 3), ("tfsf_proj_half", _dp * 3),
+        ("tfsf_transform_e", C.c_double * 3), ("tfsf_transform_h", C.c_double * 3), ("tfsf_ca", C.c_double * 3),
+        ("tfsf_cb", C.c_double * 3), ("aux_nl", C.c_int), ("inc_steps", C.c_longlong), ("e_inc", _dp), ("h_inc", _dp),
+        ("nf2ff_enabled", C.c_int), ("nf2ff_box", C.c_int * 6), ("n_freqs", C.c_int), ("freqs", _dp),
+        ("nf2ff_td_enabled", C.c_int), ("nf2ff_td_box", C.c_int * 6), ("nf2ff_td_theta", C.c_double),
+        ("nf2ff_td_phi", C.c_double), ("n_probes", C.c_int), ("probes", C.POINTER(Probe)), ("n_movies", C.c_int), ("movies", C.POINTER(Movie)),
+    ]
+
+
 class CompiledView(C.Structure):
     _fields_ = [
         ("dim", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
@@ -133,6 +149,7 @@ SIGNATURES = [
     ("xfb_status_string", C.c_char_p, [C.c_int]),
     ("xfb_last_error", C.c_char_p, [_H]),
     ("xfb_create", C.c_int, [C.POINTER(Scene), C.POINTER(_H)]),
+    ("xfb_create_from_arrays", C.c_int, [C.POINTER(CoreArrays), C.POINTER(_H)]),
     ("xfb_destroy", C.c_int, [_H]),
     ("xfb_set_device", C.c_int, [_H, C.c_int]),
     ("xfb_set_launch_hint", C.c_int, [_H, C.POINTER(C.c_uint), C.POINTER(C.c_uint)]),

@@ -245,6 +245,25 @@ int xfb_create(const xfb_scene* scene, xfb_handle** out) {
   return XFB_OK;
 }
 
+int xfb_create_from_arrays(const xfb_core_arrays* arrays, xfb_handle** out) {
+  if (!arrays || !out) return set_err(nullptr, XFB_ERR_INVALID, "null arrays or output pointer");
+  *out = nullptr;
+  std::unique_ptr<xfb_handle> h(new (std::nothrow) xfb_handle());
+  if (!h) return set_err(nullptr, XFB_ERR_OOM, "host allocation failed");
+  std::string err;
+  int rc;
+  try {
+    rc = compile_arrays(*arrays, h->c, &err);
+  } catch (const std::bad_alloc&) {
+    return set_err(nullptr, XFB_ERR_OOM, "host allocation failed while reading the arrays");
+  }
+  if (rc) return set_err(nullptr, rc, err);
+  h->esize = h->c.prec == XFB_FP64 ? 8 : 4;
+  *out = h.release();
+  g_err.clear();
+  return XFB_OK;
+}
+
 int xfb_destroy(xfb_handle* h) {
   if (!h) return XFB_OK;
   if (int rc = not_batched(h)) return rc;
@@ -336,6 +355,8 @@ int xfb_init(xfb_handle* h, long long total_steps) {
   if (is_slab(h) && (h->path == XFB_PATH_SPLIT || h->path == XFB_PATH_PLAIN))
     return set_err(h, XFB_ERR_INVALID, "x slabs run on the one-sweep path");
   if (total_steps < 0 || total_steps > (1LL << 31)) return set_err(h, XFB_ERR_INVALID, "total_steps out of range");
+  if (h->c.inc_given && total_steps > h->c.inc_steps)
+    return set_err(h, XFB_ERR_RANGE, "the run is longer than the incident tables the arrays handed over");
   if (h->device < 0) {
     int n = 0;
     cudaError_t e = cudaGetDeviceCount(&n);

@@ -204,11 +204,18 @@ int init_device(xfb_handle* h) {
     h->e_aux = static_cast<double*>(p);
     if ((rc = alloc(h, &p, std::max<size_t>(1, steps) * c.aux_nl * sizeof(double), false))) return rc;
     h->h_aux = static_cast<double*>(p);
-    if ((rc = upload<double>(h, &p, c.aux_source))) return rc;
-    h->src = static_cast<double*>(p);
-    k_aux_table<<<1, 1024, 0, h->stream>>>(h->e_aux, h->h_aux, c.aux_nl, c.aux_ceih, c.aux_chie, c.aux_abc, h->src,
-                                            c.total_steps);
-    XFB_CUDA(h, cudaGetLastError());
+    if (c.inc_given) {  // the caller's tables (rows of every step of the run)
+      if ((rc = copy(h, h->e_aux, c.e_inc.data(), (steps + 1) * (c.aux_nl + 1) * sizeof(double), cudaMemcpyHostToDevice)))
+        return rc;
+      if (steps > 0 && (rc = copy(h, h->h_aux, c.h_inc.data(), steps * c.aux_nl * sizeof(double), cudaMemcpyHostToDevice)))
+        return rc;
+    } else {
+      if ((rc = upload<double>(h, &p, c.aux_source))) return rc;
+      h->src = static_cast<double*>(p);
+      k_aux_table<<<1, 1024, 0, h->stream>>>(h->e_aux, h->h_aux, c.aux_nl, c.aux_ceih, c.aux_chie, c.aux_abc, h->src,
+                                              c.total_steps);
+      XFB_CUDA(h, cudaGetLastError());
+    }
   }
   // ADE
   if (c.ade_kind != XFB_ADE_NONE) {

@@ -93,7 +93,7 @@ void size_tables(Compiled& c, long long total_steps) {
   c.total_steps = total_steps;
   c.td_bins = c.td_on ? total_steps + c.td_span : 0;
   c.aux_source.assign(static_cast<size_t>(total_steps + 1), 0.0);
-  if (c.tfsf_on)
+  if (c.tfsf_on && !c.inc_given)
     for (long long t = 0; t <= total_steps; ++t) c.aux_source[t] = waveform(c, t * c.dt);
   const size_t nf = c.freqs.size();
   c.te.assign(nf * static_cast<size_t>(total_steps) * 2, 0.0);
@@ -143,6 +143,40 @@ double td_delay_steps(const Compiled& c, int face, int i, int j, int k) {
   // (nf2ff_time_domain_data.cuh:64-71, nf2ff_time_domain_data.cu:145-147)
   const double delay = c.td_ref - (r[0] * c.td_dir[0] + r[1] * c.td_dir[1] + r[2] * c.td_dir[2]);
   return delay / (kTdC0 * c.dt);
+}
+
+// Direction, reference distance and bin span of a time-domain NF2FF whose
+// box c.td is set.
+void compile_td(Compiled& c, double theta, double phi) {
+  c.td_theta = theta;
+  c.td_phi = phi;
+  c.td_dir[0] = std::sin(theta) * std::cos(phi);
+  c.td_dir[1] = std::sin(theta) * std::sin(phi);
+  c.td_dir[2] = std::cos(theta);
+  // reference distance: the largest r . dir over the sample points, so every
+  // delay is >= 0; then the largest bin offset a step reaches
+  double best = -std::numeric_limits<double>::infinity();
+  for (int f = 0; f < 6; ++f) {
+    const FaceGeom g = td_face_geom(c, f);
+    for (int i = g.i0; i < g.i0 + g.ni; ++i)
+      for (int j = g.j0; j < g.j0 + g.nj; ++j)
+        for (int k = g.k0; k < g.k0 + g.nk; ++k) {
+          double r[3];
+          td_position(c, f, i, j, k, r);
+          best = std::max(best, r[0] * c.td_dir[0] + r[1] * c.td_dir[1] + r[2] * c.td_dir[2]);
+        }
+  }
+  c.td_ref = best;
+  double dmax = 0;
+  for (int f = 0; f < 6; ++f) {
+    const FaceGeom g = td_face_geom(c, f);
+    for (int i = g.i0; i < g.i0 + g.ni; ++i)
+      for (int j = g.j0; j < g.j0 + g.nj; ++j)
+        for (int k = g.k0; k < g.k0 + g.nk; ++k) dmax = std::max(dmax, td_delay_steps(c, f, i, j, k));
+  }
+  // bins t + floor(delay + 1/2) + {0, 1, 2} (the rounding of the sum with t
+  // can add one)
+  c.td_span = static_cast<int>(std::floor(dmax + 0.5)) + 3;
 }
 
 int compile_scene(const xfb_scene& s, Compiled& c, std::string* err) {
@@ -471,35 +505,7 @@ int compile_scene(const xfb_scene& s, Compiled& c, std::string* err) {
     for (int a = 0; a < 3; ++a)
       if (c.td[2 * a] < 1 || c.td[2 * a + 1] >= nax[a] || c.td[2 * a + 1] <= c.td[2 * a])
         return fail("time-domain NF2FF box does not fit inside the grid");
-    c.td_theta = n.theta;
-    c.td_phi = n.phi;
-    c.td_dir[0] = std::sin(n.theta) * std::cos(n.phi);
-    c.td_dir[1] = std::sin(n.theta) * std::sin(n.phi);
-    c.td_dir[2] = std::cos(n.theta);
-    // reference distance: the largest r . dir over the sample points, so every
-    // delay is >= 0; then the largest bin offset a step reaches
-    double best = -std::numeric_limits<double>::infinity();
-    for (int f = 0; f < 6; ++f) {
-      const FaceGeom g = td_face_geom(c, f);
-      for (int i = g.i0; i < g.i0 + g.ni; ++i)
-        for (int j = g.j0; j < g.j0 + g.nj; ++j)
-          for (int k = g.k0; k < g.k0 + g.nk; ++k) {
-            double r[3];
-            td_position(c, f, i, j, k, r);
-            best = std::max(best, r[0] * c.td_dir[0] + r[1] * c.td_dir[1] + r[2] * c.td_dir[2]);
-          }
-    }
-    c.td_ref = best;
-    double dmax = 0;
-    for (int f = 0; f < 6; ++f) {
-      const FaceGeom g = td_face_geom(c, f);
-      for (int i = g.i0; i < g.i0 + g.ni; ++i)
-        for (int j = g.j0; j < g.j0 + g.nj; ++j)
-          for (int k = g.k0; k < g.k0 + g.nk; ++k) dmax = std::max(dmax, td_delay_steps(c, f, i, j, k));
-    }
-    // bins t + floor(delay + 1/2) + {0, 1, 2} (the rounding of the sum with t
-    // can add one)
-    c.td_span = static_cast<int>(std::floor(dmax + 0.5)) + 3;
+    compile_td(c, n.theta, n.phi);
   }
 
   // ---- monitors ------------------------------------------------------------

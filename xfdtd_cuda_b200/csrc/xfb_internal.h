@@ -60,6 +60,11 @@ struct Compiled {
   double ca[3] = {0, 0, 0}, cb[3] = {0, 0, 0};
   int aux_nl = 0;
   double aux_dl = 0, aux_ceih = 0, aux_chie = 0, aux_abc = 0;
+  // incident tables handed over by the caller (xfb_create_from_arrays)
+  // instead of the 1-D auxiliary grid's: rows of E (nl + 1) and H (nl)
+  bool inc_given = false;
+  long long inc_steps = 0;
+  std::vector<double> e_inc, h_inc;
   int wave_kind = XFB_WAVE_GAUSSIAN;
   double wave_tau = 0, wave_t0 = 0, wave_freq = 0;
   // NF2FF
@@ -87,6 +92,8 @@ struct Compiled {
 // Host scene compiler (scene_compile.cpp).  Returns XFB_OK or an error with
 // a message in *err.
 int compile_scene(const xfb_scene& s, Compiled& out, std::string* err);
+// The same from arrays XFDTD_CORE compiled (core_ingest.cpp).
+int compile_arrays(const xfb_core_arrays& a, Compiled& out, std::string* err);
 // Sizes the step-count dependent tables (TFSF source samples, NF2FF DFT
 // kernels) for a run of total_steps steps.
 void size_tables(Compiled& c, long long total_steps);
@@ -112,5 +119,6 @@ constexpr double kTdC0 = 299792458.0;
 // nf2ff_time_domain_data.cu:53-66) and its delay in steps,
 // (ref - r . dir) / (c dt).
 double td_delay_steps(const Compiled& c, int face, int i, int j, int k);
+void compile_td(Compiled& c, double theta, double phi);
 
 }  // namespace xfb

@@ -584,6 +584,21 @@ class Handle:
         L.check(self.lib.xfb_create(C.byref(scene), C.byref(h)))
         self.h = h
 
+    @classmethod
+    def from_core_arrays(cls, arrays: L.CoreArrays, keep=()):
+        """A handle from a scene XFDTD_CORE compiled (xfb_create_from_arrays);
+        `keep` holds the numpy arrays the struct points into."""
+        self = cls.__new__(cls)
+        self.lib = L.load()
+        self._keep = list(keep)
+        self.probe_desc = [(arrays.probes[q].field, *arrays.probes[q].index) for q in range(arrays.n_probes)]
+        self.movie_desc = [(arrays.movies[q].field, *arrays.movies[q].lo, *arrays.movies[q].hi, arrays.movies[q].interval)
+                           for q in range(arrays.n_movies)]
+        h = C.c_void_p()
+        L.check(self.lib.xfb_create_from_arrays(C.byref(arrays), C.byref(h)))
+        self.h = h
+        return self
+
     def close(self):
         if getattr(self, "h", None):
             self.lib.xfb_destroy(self.h)
