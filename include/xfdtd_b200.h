@@ -294,6 +294,19 @@ int xfb_get_grid_info(const xfb_handle* h, xfb_grid_info* out);
 
 /* One field component in its reference shape, converted to double. */
 int xfb_read_field(xfb_handle* h, int field, double* dst, size_t dst_len);
+/* Fault in the pages of a host range that results will be read into (a
+ * field or NF2FF destination), on background host threads, and return at
+ * once; contents are unchanged.  A read into fresh memory otherwise pays the
+ * page faults of every destination page (about 5x slower than into resident
+ * memory), so a caller that allocates its result arrays ahead of a run (as
+ * XFDTD_CORE allocates the host fields in Simulation::init) lets the faults
+ * run while the device initialises and steps.  The range must stay allocated
+ * until the handle's next read, far-field or get_state call,
+ * xfb_host_prefault_wait or xfb_destroy; each of these waits for the threads
+ * first. */
+int xfb_host_prefault(xfb_handle* h, void* ptr, size_t bytes);
+int xfb_host_prefault_wait(xfb_handle* h);
+
 /* Overwrite one field component (reference shape, double) - initial values. */
 int xfb_write_field(xfb_handle* h, int field, const double* src, size_t src_len);
 /* Time series of probe `id` (one value per step taken, double). */
@@ -308,6 +321,12 @@ int xfb_read_movie(xfb_handle* h, int id, double* dst, size_t dst_len);
  * (src/nf2ff/frequency_domain/nf2ff_frequency_domain.data.cu:80-194). */
 int xfb_nf2ff_face_shape(const xfb_handle* h, int face, int shape_out[3]);
 int xfb_read_nf2ff(xfb_handle* h, int freq, int face, int which, double* dst, size_t dst_len);
+/* All surface currents of frequency `freq` in one read: [which 0..3][points],
+ * complex interleaved, the six faces one after another in face order, each
+ * in its xfb_nf2ff_face_shape (so face f of current w starts at point
+ * w * points + the sizes of faces 0..f-1).  dst_len >= 8 * points doubles;
+ * *points (optional) receives the face points of all six faces. */
+int xfb_read_nf2ff_all(xfb_handle* h, int freq, double* dst, size_t dst_len, long long* points);
 /* Far field from the accumulated surface currents, computed on the device.
  * For each (theta[i], phi[i]) writes 4 doubles: Re/Im E_theta, Re/Im E_phi of
  * r*E (the e^{-jkr} factor removed), in the e^{+jwt} phasor convention of the

@@ -166,12 +166,15 @@ SIGNATURES = [
     ("xfb_set_temporal_block", C.c_int, [_H, C.c_int]),
     ("xfb_get_grid_info", C.c_int, [_H, C.POINTER(GridInfo)]),
     ("xfb_read_field", C.c_int, [_H, C.c_int, _dp, C.c_size_t]),
+    ("xfb_host_prefault", C.c_int, [_H, C.c_void_p, C.c_size_t]),
+    ("xfb_host_prefault_wait", C.c_int, [_H]),
     ("xfb_write_field", C.c_int, [_H, C.c_int, _dp, C.c_size_t]),
     ("xfb_read_probe", C.c_int, [_H, C.c_int, _dp, C.c_size_t, C.POINTER(C.c_longlong)]),
     ("xfb_movie_shape", C.c_int, [_H, C.c_int, C.c_int * 4]),
     ("xfb_read_movie", C.c_int, [_H, C.c_int, _dp, C.c_size_t]),
     ("xfb_nf2ff_face_shape", C.c_int, [_H, C.c_int, C.c_int * 3]),
     ("xfb_read_nf2ff", C.c_int, [_H, C.c_int, C.c_int, C.c_int, _dp, C.c_size_t]),
+    ("xfb_read_nf2ff_all", C.c_int, [_H, C.c_int, _dp, C.c_size_t, C.POINTER(C.c_longlong)]),
     ("xfb_far_field", C.c_int, [_H, C.c_int, C.c_int, _dp, _dp, _dp]),
     ("xfb_far_field_static", C.c_int, [_H, C.c_int, C.c_int, _dp, _dp, _dp]),
     ("xfb_nf2ff_td_bins", C.c_int, [_H, C.POINTER(C.c_longlong)]),

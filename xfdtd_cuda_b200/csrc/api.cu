@@ -8,6 +8,7 @@
 // in device memory (bumped once per captured chunk) so a captured chunk is
 // valid for any starting step.
 #include <cuda_runtime.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <cmath>
@@ -164,6 +165,69 @@ int not_batched(xfb_handle* h) {
   return XFB_OK;
 }
 
+// Join the handle's prefault threads (before any write into caller memory).
+void wait_prefault(xfb_handle* h) {
+  for (auto& t : h->prefault) t.join();
+  h->prefault.clear();
+  h->pf_queue.clear();
+  h->pf_active = 0;
+}
+
+// A prefault worker: takes queued parts until none is left and takes the
+// write fault of every page of each by an atomic add of zero to one byte of
+// the page inside the part (contents unchanged; one fault per huge page where
+// the range is madvised for them).
+void prefault_worker(xfb_handle* h) {
+  const uintptr_t page = static_cast<uintptr_t>(sysconf(_SC_PAGESIZE));
+  for (;;) {
+    std::pair<char*, char*> r;
+    {
+      std::lock_guard<std::mutex> lk(h->pf_mu);
+      if (h->pf_queue.empty()) {
+        --h->pf_active;
+        return;
+      }
+      r = h->pf_queue.back();
+      h->pf_queue.pop_back();
+    }
+    char* p = r.first;
+    while (p < r.second) {
+      __atomic_fetch_add(p, static_cast<char>(0), __ATOMIC_RELAXED);
+      p = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(p) / page + 1) * page);
+    }
+  }
+}
+
+// Queue [ptr, ptr + bytes) for the handle's prefault pool (64 MiB parts) and
+// start workers up to the pool size; false when that fails.
+bool queue_prefault(xfb_handle* h, void* ptr, size_t bytes) {
+  if (!bytes) return true;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const int max_threads = static_cast<int>(std::max(1u, std::min(12u, hw * 3 / 4)));
+  const size_t part = 64u << 20;
+  char* base = static_cast<char*>(ptr);
+  try {
+    std::lock_guard<std::mutex> lk(h->pf_mu);
+    for (size_t o = 0; o < bytes; o += part) h->pf_queue.emplace_back(base + o, base + std::min(bytes, o + part));
+    while (h->pf_active < max_threads) {
+      h->prefault.emplace_back(prefault_worker, h);
+      ++h->pf_active;
+    }
+  } catch (const std::exception&) {
+    wait_prefault(h);
+    return false;
+  }
+  return true;
+}
+
+// Fault in a large caller destination with the pool before a read-back writes
+// it: the pool takes fresh pages several times faster than the read-back's
+// own writes would.  A failure only leaves the faults to the read-back.
+void prefault_now(xfb_handle* h, void* ptr, size_t bytes) {
+  if (bytes >= (8u << 20)) queue_prefault(h, ptr, bytes);
+  wait_prefault(h);
+}
+
 int check_handle(xfb_handle* h, bool need_init) {
   if (!h) return set_err(nullptr, XFB_ERR_INVALID, "null handle");
   if (need_init && !h->inited) return set_err(h, XFB_ERR_STATE, "handle not initialised (call xfb_init or xfb_run)");
@@ -267,6 +331,7 @@ int xfb_create_from_arrays(const xfb_core_arrays* arrays, xfb_handle** out) {
 int xfb_destroy(xfb_handle* h) {
   if (!h) return XFB_OK;
   if (int rc = not_batched(h)) return rc;
+  wait_prefault(h);
   if (h->device >= 0) {
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
@@ -486,10 +551,19 @@ int xfb_get_grid_info(const xfb_handle* h, xfb_grid_info* o) {
   o->current_step = h->step;
   o->total_steps = c.total_steps;
   o->device_bytes = h->bytes;
-  long long nd = 0;
-  if (c.ade_kind != XFB_ADE_NONE)
-    for (uint8_t m : c.mat_id) nd += c.ade_mat[static_cast<size_t>(m) * kAdeMat] != 0;
-  o->n_dispersive_cells = nd;
+  if (h->n_disp_cells < 0) {  // counted once: the material ids do not change
+    long long nd = 0;
+    if (c.ade_kind != XFB_ADE_NONE) {
+      bool disp[256] = {};
+      for (int m = 0; m < c.n_mat; ++m) disp[m] = c.ade_mat[static_cast<size_t>(m) * kAdeMat] != 0;
+      const long long n = static_cast<long long>(c.mat_id.size());
+      const uint8_t* id = c.mat_id.data();
+#pragma omp parallel for reduction(+ : nd) schedule(static)
+      for (long long q = 0; q < n; ++q) nd += disp[id[q]];
+    }
+    h->n_disp_cells = nd;
+  }
+  o->n_dispersive_cells = h->n_disp_cells;
   o->launches_per_step = launches_per_step(h);
   o->kernel_path = h->path;
   o->h2d_bytes = h->h2d_bytes;
@@ -501,13 +575,28 @@ int xfb_get_grid_info(const xfb_handle* h, xfb_grid_info* o) {
 int xfb_read_field(xfb_handle* h, int f, double* dst, size_t len) {
   int rc = check_handle(h, true);
   if (rc) return rc;
+  wait_prefault(h);
   if (f < 0 || f > 5 || !dst) return set_err(h, XFB_ERR_INVALID, "bad field or buffer");
   if (!h->f[f]) return set_err(h, XFB_ERR_INVALID, "component not present in a 2-D (TMz) scene");
   int s[3];
   comp_shape(h->c, f, s);
-  if (len < static_cast<size_t>(s[0]) * s[1] * s[2]) return set_err(h, XFB_ERR_RANGE, "destination too small");
+  const size_t n = static_cast<size_t>(s[0]) * s[1] * s[2];
+  if (len < n) return set_err(h, XFB_ERR_RANGE, "destination too small");
   if (!h->batch && (rc = step_status(h))) return rc;
+  prefault_now(h, dst, n * sizeof(double));
   return h->c.prec == XFB_FP64 ? read_field_t<double>(h, f, dst) : read_field_t<float>(h, f, dst);
+}
+
+int xfb_host_prefault(xfb_handle* h, void* ptr, size_t bytes) {
+  if (!h || (!ptr && bytes)) return set_err(h, XFB_ERR_INVALID, "null handle or range");
+  if (!queue_prefault(h, ptr, bytes)) return set_err(h, XFB_ERR_OOM, "could not queue the range or start host threads");
+  return XFB_OK;
+}
+
+int xfb_host_prefault_wait(xfb_handle* h) {
+  if (!h) return set_err(nullptr, XFB_ERR_INVALID, "null handle");
+  wait_prefault(h);
+  return XFB_OK;
 }
 
 int xfb_write_field(xfb_handle* h, int f, const double* src, size_t len) {
@@ -524,6 +613,7 @@ int xfb_write_field(xfb_handle* h, int f, const double* src, size_t len) {
 int xfb_read_probe(xfb_handle* h, int id, double* dst, size_t len, long long* n_written) {
   int rc = check_handle(h, true);
   if (rc) return rc;
+  wait_prefault(h);
   if (id < 0 || id >= static_cast<int>(h->c.probes.size())) return set_err(h, XFB_ERR_RANGE, "probe id out of range");
   const long long n = h->step;
   if (len < static_cast<size_t>(n)) return set_err(h, XFB_ERR_RANGE, "destination too small");
@@ -545,6 +635,7 @@ int xfb_movie_shape(const xfb_handle* h, int id, int s[4]) {
 int xfb_read_movie(xfb_handle* h, int id, double* dst, size_t len) {
   int rc = check_handle(h, true);
   if (rc) return rc;
+  wait_prefault(h);
   int s[4];
   if ((rc = xfb_movie_shape(h, id, s))) return rc;
   const size_t n = static_cast<size_t>(s[0]) * s[1] * s[2] * s[3];
@@ -592,6 +683,7 @@ static int nf2ff_flush(xfb_handle* h) {
 int xfb_read_nf2ff(xfb_handle* h, int freq, int face, int which, double* dst, size_t len) {
   int rc = check_handle(h, true);
   if (rc) return rc;
+  wait_prefault(h);
   int s[3];
   if ((rc = xfb_nf2ff_face_shape(h, face, s))) return rc;
   if (freq < 0 || freq >= static_cast<int>(h->c.freqs.size()) || which < 0 || which > 3)
@@ -605,9 +697,28 @@ int xfb_read_nf2ff(xfb_handle* h, int freq, int face, int which, double* dst, si
   return XFB_OK;
 }
 
+int xfb_read_nf2ff_all(xfb_handle* h, int freq, double* dst, size_t len, long long* points) {
+  int rc = check_handle(h, true);
+  if (rc) return rc;
+  wait_prefault(h);
+  if (!h->c.nf_on) return set_err(h, XFB_ERR_STATE, "scene has no NF2FF box");
+  if (freq < 0 || freq >= static_cast<int>(h->c.freqs.size())) return set_err(h, XFB_ERR_RANGE, "frequency index out of range");
+  const size_t n = 4 * static_cast<size_t>(h->nf_npts);
+  if (points) *points = h->nf_npts;
+  if (!dst) return set_err(h, XFB_ERR_INVALID, "null destination");
+  if (len < 2 * n) return set_err(h, XFB_ERR_RANGE, "destination too small (complex interleaved)");
+  if ((rc = nf2ff_flush(h))) return rc;
+  if (!h->batch && (rc = step_status(h))) return rc;
+  prefault_now(h, dst, n * sizeof(double2));
+  const double2* src = h->nf_acc + static_cast<long long>(freq) * 4 * h->nf_npts;
+  return h->c.prec == XFB_FP64 ? read_bytes_t<double>(h, dst, src, n * sizeof(double2))
+                               : read_bytes_t<float>(h, dst, src, n * sizeof(double2));
+}
+
 int xfb_far_field(xfb_handle* h, int freq, int n, const double* theta, const double* phi, double* out) {
   int rc = check_handle(h, true);
   if (rc) return rc;
+  wait_prefault(h);
   if (!h->c.nf_on) return set_err(h, XFB_ERR_STATE, "scene has no NF2FF box");
   if (freq < 0 || freq >= static_cast<int>(h->c.freqs.size())) return set_err(h, XFB_ERR_RANGE, "frequency index out of range");
   if (n < 0 || (n > 0 && (!theta || !phi || !out))) return set_err(h, XFB_ERR_INVALID, "bad angle arrays");
@@ -650,6 +761,7 @@ int xfb_far_field(xfb_handle* h, int freq, int n, const double* theta, const dou
 int xfb_far_field_static(xfb_handle* h, int freq, int n, const double* theta, const double* phi, double* out) {
   int rc = check_handle(h, true);  // makes the handle's device current
   if (rc) return rc;
+  wait_prefault(h);
   if (!h->c.nf_on) return set_err(h, XFB_ERR_STATE, "scene has no NF2FF box");
   if (freq < 0 || freq >= static_cast<int>(h->c.freqs.size())) return set_err(h, XFB_ERR_RANGE, "frequency index out of range");
   if (n < 0 || (n > 0 && (!theta || !phi || !out))) return set_err(h, XFB_ERR_INVALID, "bad angle arrays");
@@ -694,6 +806,7 @@ int xfb_nf2ff_td_bins(const xfb_handle* h, long long* n_bins) {
 int xfb_read_nf2ff_td(xfb_handle* h, int which, double* dst, size_t len) {
   int rc = check_handle(h, true);
   if (rc) return rc;
+  wait_prefault(h);
   if (!h->c.td_on) return set_err(h, XFB_ERR_STATE, "scene has no time-domain NF2FF box");
   if (which < 0 || which > 5 || !dst) return set_err(h, XFB_ERR_INVALID, "potential index must be 0..5 (W_x..U_z)");
   const size_t n = static_cast<size_t>(h->c.td_bins);
@@ -706,6 +819,7 @@ int xfb_read_nf2ff_td(xfb_handle* h, int which, double* dst, size_t len) {
 int xfb_far_field_td(xfb_handle* h, double* e_theta, double* e_phi, size_t len) {
   int rc = check_handle(h, true);
   if (rc) return rc;
+  wait_prefault(h);
   if (!h->c.td_on) return set_err(h, XFB_ERR_STATE, "scene has no time-domain NF2FF box");
   const size_t n = static_cast<size_t>(h->c.td_bins);
   if (!e_theta || !e_phi || len < n) return set_err(h, XFB_ERR_RANGE, "destination too small");
@@ -852,6 +966,7 @@ int xfb_state_size(const xfb_handle* h, size_t* bytes) {
 int xfb_get_state(xfb_handle* h, void* dst, size_t len) {
   int rc = check_handle(h, true);
   if (rc) return rc;
+  wait_prefault(h);
   size_t need;
   if ((rc = xfb_state_size(h, &need))) return rc;
   if (!dst || len < need) return set_err(h, XFB_ERR_RANGE, "state buffer too small");

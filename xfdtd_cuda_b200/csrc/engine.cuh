@@ -1235,6 +1235,51 @@ int read_field_t(xfb_handle* h, int f, double* dst) {
   return XFB_OK;
 }
 
+// dst <- src (device), bytes long, through the pinned read-back buffers:
+// chunk c is copied into host buffer c & 1 while host threads copy chunk c - 1
+// into dst.  Falls back to one pageable copy when the buffers cannot be had.
+template <typename T>
+int read_bytes_t(xfb_handle* h, void* dst, const void* src, size_t bytes) {
+  if (bytes == 0) return XFB_OK;
+  if (!readback_buffers<T>(h)) {
+    h->err.clear();
+    XFB_CUDA(h, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream));
+    XFB_CUDA(h, cudaStreamSynchronize(h->stream));
+    h->d2h_bytes += static_cast<long long>(bytes);
+    return XFB_OK;
+  }
+  const size_t chunk = static_cast<size_t>(kReadChunk) * sizeof(T);
+  const size_t nch = (bytes + chunk - 1) / chunk;
+  auto enqueue = [&](size_t c) -> cudaError_t {
+    const size_t o = c * chunk, n = std::min(chunk, bytes - o);
+    cudaError_t e = cudaMemcpyAsync(h->rb_host[c & 1], static_cast<const char*>(src) + o, n, cudaMemcpyDeviceToHost,
+                                    h->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(h->rb_ev[c & 1], h->stream);
+    return e;
+  };
+  cudaError_t e = enqueue(0);
+  const int threads = std::max(1, std::min(16, omp_get_max_threads()));
+  for (size_t c = 0; c < nch && e == cudaSuccess; ++c) {
+    if (c + 1 < nch) e = enqueue(c + 1);
+    if (e == cudaSuccess) e = cudaEventSynchronize(h->rb_ev[c & 1]);
+    if (e != cudaSuccess) break;
+    const size_t o = c * chunk, n = std::min(chunk, bytes - o), per = (n + threads - 1) / threads;
+    const char* from = static_cast<const char*>(h->rb_host[c & 1]);
+    char* to = static_cast<char*>(dst) + o;
+#pragma omp parallel for schedule(static) num_threads(threads)
+    for (int t = 0; t < threads; ++t) {
+      const size_t a = static_cast<size_t>(t) * per;
+      if (a < n) std::memcpy(to + a, from + a, std::min(per, n - a));
+    }
+    h->d2h_bytes += static_cast<long long>(n);
+  }
+  if (e != cudaSuccess) {
+    cudaStreamSynchronize(h->stream);
+    return cuda_err(h, e, "read-back");
+  }
+  return XFB_OK;
+}
+
 template <typename T>
 int write_field_t(xfb_handle* h, int f, const double* src) {
   std::vector<T> tmp(static_cast<size_t>(h->elems));
@@ -1530,6 +1575,7 @@ int batch_run(xfb_batch* b, long long n) {
   template int slab_record<T>(xfb_handle*);                                                \
   template int profile_steps<T>(xfb_handle*, long long, double*, long long*);              \
   template int read_field_t<T>(xfb_handle*, int, double*);                                 \
+  template int read_bytes_t<T>(xfb_handle*, void*, const void*, size_t);                   \
   template int write_field_t<T>(xfb_handle*, int, const double*);                          \
   template void launch_nonfinite<T>(xfb_handle*);                                          \
   template int batch_init<T>(xfb_batch*);                                                  \

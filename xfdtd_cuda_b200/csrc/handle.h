@@ -6,7 +6,9 @@
 #include <cuda_runtime.h>
 
 #include <map>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "xfb_internal.h"
@@ -25,6 +27,14 @@ struct xfb_handle {
   using Buf = xfb::Buf;
   xfb::Compiled c;
   std::string err;
+  // xfb_host_prefault: ranges (64 MiB parts) queued for a pool of host
+  // threads (three quarters of the cores, at most 12) that fault them in;
+  // every call that writes caller memory joins the pool first
+  std::vector<std::thread> prefault;
+  mutable long long n_disp_cells = -1;  // cells of dispersive materials (grid info), once counted
+  std::vector<std::pair<char*, char*>> pf_queue;
+  std::mutex pf_mu;
+  int pf_active = 0;
   int device = -1;
   cudaStream_t stream = nullptr;
   bool inited = false;
@@ -227,6 +237,7 @@ template <typename T> int slab_update(xfb_handle* h);
 template <typename T> int slab_record(xfb_handle* h);
 template <typename T> int profile_steps(xfb_handle* h, long long n, double* ms, long long* launches);
 template <typename T> int read_field_t(xfb_handle* h, int f, double* dst);
+template <typename T> int read_bytes_t(xfb_handle* h, void* dst, const void* src, size_t bytes);
 template <typename T> int write_field_t(xfb_handle* h, int f, const double* src);
 template <typename T> void launch_nonfinite(xfb_handle* h);
 template <typename T> int batch_init(xfb_batch* b);

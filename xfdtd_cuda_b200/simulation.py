@@ -22,6 +22,7 @@ from __future__ import annotations
 import ctypes as C
 import math
 import os
+import time
 from dataclasses import dataclass, field
 from pathlib import Path
 from typing import Sequence
@@ -56,8 +57,21 @@ class Axis:
 
 
 class EMF:
+    """XFDTD_CORE's EMF: the component enum and, after a SimulationHD run,
+    the host field arrays ex ... hz in their Yee shapes (float64), filled by
+    SimulationHD.copyDeviceToHost."""
+
     class Field:
         EX, EY, EZ, HX, HY, HZ = range(6)
+
+    names = ("ex", "ey", "ez", "hx", "hy", "hz")
+
+    def __init__(self):
+        for n in self.names:
+            setattr(self, n, None)
+
+    def field(self, f: int):
+        return getattr(self, self.names[f])
 
 
 # ---- shapes ---------------------------------------------------------------
@@ -406,6 +420,7 @@ class Simulation:
         self.monitor_list: list = []
         self.nf2ff_list: list[NFFFTFrequencyDomain] = []
         self.dimension = 3
+        self.emf = None  # host field arrays of the last SimulationHD run (EMF)
 
     def addObject(self, o: Object):
         self.objects.append(o)
@@ -674,11 +689,29 @@ class Handle:
         self._c(self.lib.xfb_profile_kernels(self.h, int(n), ms, cnt))
         return list(ms), list(cnt)
 
-    def read_field(self, f) -> np.ndarray:
+    def read_field(self, f, out: np.ndarray | None = None) -> np.ndarray:
+        """Component f (reference shape, float64); into `out` when given."""
         s = self.shape(f)
-        out = np.empty(s, dtype=np.float64)
+        if out is None:
+            out = np.empty(s, dtype=np.float64)
+        elif out.shape != s or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous float64 array of shape {s}")
         self._c(self.lib.xfb_read_field(self.h, f, out.ctypes.data_as(L._dp), out.size))
+        self._prefault_keep = []
         return out
+
+    def prefault(self, arr: np.ndarray):
+        """Fault in the pages of a result array on background host threads
+        (xfb_host_prefault) while the device works; the array is kept alive
+        until the next read."""
+        if not hasattr(self, "_prefault_keep"):
+            self._prefault_keep = []
+        self._prefault_keep.append(arr)
+        self._c(self.lib.xfb_host_prefault(self.h, arr.ctypes.data, arr.nbytes))
+
+    def prefault_wait(self):
+        self._c(self.lib.xfb_host_prefault_wait(self.h))
+        self._prefault_keep = []
 
     def write_field(self, f, arr):
         arr = np.ascontiguousarray(arr, dtype=np.float64)
@@ -700,12 +733,47 @@ class Handle:
         self._c(self.lib.xfb_read_movie(self.h, m, out.ctypes.data_as(L._dp), out.size))
         return out
 
-    def read_nf2ff(self, freq, face, which) -> np.ndarray:
+    def nf2ff_face_shape(self, face) -> tuple:
         s = (C.c_int * 3)()
         self._c(self.lib.xfb_nf2ff_face_shape(self.h, face, s))
-        out = np.empty(tuple(s) + (2,), dtype=np.float64)
-        self._c(self.lib.xfb_read_nf2ff(self.h, freq, face, which, out.ctypes.data_as(L._dp), out.size))
-        return out[..., 0] + 1j * out[..., 1]
+        return tuple(s)
+
+    def read_nf2ff(self, freq, face, which, out: np.ndarray | None = None) -> np.ndarray:
+        """Surface current `which` (J_a, J_b, M_a, M_b) of one face and
+        frequency, complex128 (the library's interleaved re/im pairs are
+        numpy's complex layout); into `out` when given."""
+        s = self.nf2ff_face_shape(face)
+        if out is None:
+            out = np.empty(s, dtype=np.complex128)
+        elif out.shape != s or out.dtype != np.complex128 or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous complex128 array of shape {s}")
+        self._c(self.lib.xfb_read_nf2ff(self.h, freq, face, which, out.ctypes.data_as(L._dp), 2 * out.size))
+        self._prefault_keep = []
+        return out
+
+    def read_nf2ff_all(self, freq, out: np.ndarray | None = None) -> np.ndarray:
+        """All surface currents of one frequency in one read: complex128
+        [4 (J_a, J_b, M_a, M_b), points], the six faces one after another
+        (nf2ff_split cuts them into per-face arrays); into `out` when given."""
+        pts = C.c_longlong()
+        n = sum(int(np.prod(self.nf2ff_face_shape(f))) for f in range(6))
+        if out is None:
+            out = np.empty((4, n), dtype=np.complex128)
+        elif out.shape != (4, n) or out.dtype != np.complex128 or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous complex128 array of shape {(4, n)}")
+        self._c(self.lib.xfb_read_nf2ff_all(self.h, freq, out.ctypes.data_as(L._dp), 2 * out.size, C.byref(pts)))
+        self._prefault_keep = []
+        return out
+
+    def nf2ff_split(self, cur: np.ndarray):
+        """[face][which] views (face shapes) into a read_nf2ff_all array."""
+        res, o = [], 0
+        for face in range(6):
+            s = self.nf2ff_face_shape(face)
+            m = int(np.prod(s))
+            res.append([cur[w, o:o + m].reshape(s) for w in range(4)])
+            o += m
+        return res
 
     def far_field(self, freq, theta, phi):
         th = np.ascontiguousarray(theta, dtype=np.float64)
@@ -834,13 +902,26 @@ class Batch:
 
 
 class SimulationHD:
-    """Drop-in for ``xfdtd::cuda::SimulationHD`` (simulation_hd.cuh:37-88)."""
+    """Drop-in for ``xfdtd::cuda::SimulationHD`` (simulation_hd.cuh:37-88).
+
+    init(n) compiles the host scene, uploads the device state and allocates
+    the host result arrays (the fields in ``host().emf``, the NF2FF surface
+    currents), as XFDTD_CORE's Simulation::init does; run(n) has their pages
+    faulted in on background host threads while the device steps.
+    copyDeviceToHost() fills them, as the reference copies results back into
+    the host objects (simulation_hd.cu:228-247)."""
 
     def __init__(self, host: Simulation):
         self._host = host
         self._grid = (1, 1, 1)
         self._block = (1, 1, 1)
         self.handle: Handle | None = None
+        self.device = None        # CUDA ordinal (None: the current device)
+        self.kernel_path = None   # xfb_set_kernel_path value (None: automatic)
+        self.timings = {}
+
+    def setDevice(self, ordinal: int):
+        self.device = int(ordinal)
 
     def host(self):
         return self._host
@@ -852,29 +933,69 @@ class SimulationHD:
         self._block = tuple(int(v) for v in b)
 
     def init(self, time_step: int):
+        t0 = time.perf_counter()
         sc, keep = self._host.lower()
         if self.handle is not None:
             self.handle.close()
         self.handle = Handle(sc, keep)
+        t1 = time.perf_counter()
+        if self.device is not None:
+            self.handle.set_device(self.device)
+        if self.kernel_path is not None:
+            self.handle.set_kernel_path(self.kernel_path)
         self.handle.set_launch_hint(self._grid, self._block)
         self.handle.init(time_step)
+        # after the device init: large untouched host mappings made it slower
+        self._alloc_host_results()
+        self.timings = {"compile": t1 - t0, "init": time.perf_counter() - t1}
         gi = self.handle.info()
         for w in self._host.sources:
             if isinstance(w, TFSF3D):
                 w.waveform()._time = (np.arange(time_step) + 1) * gi.dt
 
     def run(self, time_step: int):
-        """Reference run(n): initialise, advance n steps, copy results back into the host objects."""
+        """Reference run(n): initialise, advance n steps, copy results back
+        into the host objects.  The pages of the host result arrays are
+        faulted in on host threads while the device steps."""
         self.init(time_step)
+        self.prefaultHostResults()
         self.handle.step(time_step)
         self.handle.sync()
         self.copyDeviceToHost()
+
+    def prefaultHostResults(self):
+        """Start faulting in the host result arrays on background host threads
+        (xfb_host_prefault); the next read joins them."""
+        emf = self._host.emf
+        for f in range(6):
+            a = emf.field(f) if emf is not None else None
+            if a is not None:
+                self.handle.prefault(a)
+        for a in self._nf_out or ():
+            self.handle.prefault(a)
+
+    def _alloc_host_results(self):
+        h = self.handle
+        gi = h.info()
+        emf = EMF()
+        for f in ((L.EZ, L.HX, L.HY) if gi.dim == 2 else range(6)):
+            setattr(emf, EMF.names[f], np.empty(h.shape(f), dtype=np.float64))
+        self._host.emf = emf
+        self._nf_out = None
+        if gi.n_freqs:
+            n = sum(int(np.prod(h.nf2ff_face_shape(face))) for face in range(6))
+            self._nf_out = [np.empty((4, n), dtype=np.complex128) for _ in range(gi.n_freqs)]
 
     def copyHostToDevice(self):
         pass  # buffers are uploaded by init()
 
     def copyDeviceToHost(self):
         h = self.handle
+        emf = self._host.emf
+        for f in range(6):
+            a = emf.field(f)
+            if a is not None:
+                h.read_field(f, out=a)
         pi = mi = 0
         for m in self._host.monitor_list:
             if isinstance(m, PointMonitor):
@@ -889,7 +1010,7 @@ class SimulationHD:
             if isinstance(nf, NFFFTTimeDomain):
                 nf.potentials = [h.read_nf2ff_td(w) for w in range(6)]
                 continue
-            nf.currents = [[[h.read_nf2ff(f, face, w) for w in range(4)] for face in range(6)]
+            nf.currents = [h.nf2ff_split(h.read_nf2ff_all(f, out=self._nf_out[f] if self._nf_out else None))
                            for f in range(nf.freqCount())]
 
     def releaseDevice(self):
