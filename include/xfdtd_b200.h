@@ -417,6 +417,21 @@ typedef struct xfb_batch xfb_batch;
 int xfb_batch_create(xfb_handle* const* handles, int n, xfb_batch** out);
 /* Tile rows of the one-sweep kernel: 0 = autotune on the first steps (default), 8, 14 or 16. */
 int xfb_batch_set_tile(xfb_batch* b, int rows);
+/* How the steps are launched.  XFB_BATCH_PER_STEP: one launch of the
+ * one-sweep kernel per step.  XFB_BATCH_PERSISTENT: one launch per chunk of
+ * steps (up to the graph chunk), whose resident CTAs take the work items of
+ * all steps from a device queue; an item of step s starts once every item of
+ * step s - 1 of its scene is done (bounded waits, XFB_ERR_TIMEOUT as for the
+ * staging waits), so a scene's next step overlaps the end of the current
+ * step of the others.  Only for batches whose scenes record no monitors (NF2FF,
+ * probes, movies) and run no separate ADE pass, which the per-step form
+ * launches between steps; otherwise XFB_ERR_INVALID.  XFB_BATCH_AUTO (default)
+ * times both on the first steps, together with the tile rows, and keeps the
+ * faster. */
+enum xfb_batch_launch { XFB_BATCH_AUTO = 0, XFB_BATCH_PER_STEP = 1, XFB_BATCH_PERSISTENT = 2 };
+int xfb_batch_set_launch(xfb_batch* b, int launch);
+/* The launch form in use (0 before the first step). */
+int xfb_batch_launch_form(const xfb_batch* b, int* launch);
 /* xfb_init every scene for total_steps steps (one-sweep path) and build the batch's work list. */
 int xfb_batch_init(xfb_batch* b, long long total_steps);
 /* Advance every scene n steps (asynchronous). */

@@ -10,6 +10,7 @@ import numpy as np
 import pytest
 
 import xfdtd_cuda_b200 as X
+from xfdtd_cuda_b200 import _lib as L
 from xfdtd_cuda_b200 import configs
 from conftest import max_rel
 from helpers import bit_equal, compare_fields, fields_of, oracle_of
@@ -110,11 +111,71 @@ def test_autotune_cache_reused(tmp_path, monkeypatch):
     b.step(20)
     b.sync()
     rows = b.info()["tile_rows"]
+    form = b.info()["launch"]
     b.close()
     lines = cache.read_text().splitlines()
-    assert len(lines) == 1 and lines[0].split()[-1] in ("0", "1", "2")
+    # one line per autotune: key, then tile index + 3 * launch form (1 per step, 2 persistent)
+    assert len(lines) == 1 and int(lines[0].split()[-1]) in range(3, 9)
     b2, hs2 = batch()
     b2.step(1)  # too few steps to autotune: without the cache it would take 16-row tiles
     b2.sync()
-    assert b2.info()["tile_rows"] == rows
+    assert b2.info()["tile_rows"] == rows and b2.info()["launch"] == form
     b2.close()
+
+
+def _sweep(precision, n=5, seed=21):
+    # scenes without monitors or a separate ADE pass: the persistent form applies
+    return configs.batched_sweep(n=n, seed=seed, lo=18, hi=46, pml=5, dl=2e-3, precision=precision)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+@pytest.mark.parametrize("tile", [8, 16])
+def test_persistent_batch_matches_per_step_and_alone(precision, tile):
+    # several persistent launches (chunks of at most 64 steps, odd chunk
+    # lengths so launches start on both field sets) against the per-step
+    # form and against every scene stepped alone
+    n = 150
+    sims = _sweep(precision)
+    runs = {}
+    for form in (L.BATCH_PERSISTENT, L.BATCH_PER_STEP):
+        hs = [X.Handle(*s.lower()) for s in sims]
+        b = X.Batch(hs, tile_rows=tile, launch=form)
+        b.init(n)
+        for chunk in (1, 37, 64, 48):
+            b.step(chunk)
+        b.sync()
+        assert b.info()["launch"] == ("persistent" if form == L.BATCH_PERSISTENT else "per_step")
+        runs[form] = [fields_of(h, 3) for h in hs]
+        b.close()
+        for h in hs:
+            h.close()
+    for q, s in enumerate(sims):
+        a = _handle(s, n)
+        a.step(n)
+        a.sync()
+        alone = fields_of(a, 3)
+        a.close()
+        if precision == "fp64":
+            assert bit_equal(runs[L.BATCH_PERSISTENT][q], runs[L.BATCH_PER_STEP][q])
+            assert bit_equal(runs[L.BATCH_PERSISTENT][q], alone)
+        else:
+            assert compare_fields(runs[L.BATCH_PERSISTENT][q], runs[L.BATCH_PER_STEP][q]) <= FP32_TOL
+            assert compare_fields(runs[L.BATCH_PERSISTENT][q], alone) <= FP32_TOL
+
+
+def test_persistent_batch_refused_with_monitors():
+    sims = _scenes("fp64")[:1]  # records probes and NF2FF between steps
+    hs = [X.Handle(*s.lower()) for s in sims]
+    b = X.Batch(hs, launch=L.BATCH_PERSISTENT)
+    with pytest.raises(X.XfbError) as e:
+        b.init(10)
+    assert e.value.status == L.XFB_ERR_INVALID
+    b.close()
+    b = X.Batch(hs)  # the automatic choice keeps the per-step form
+    b.init(30)
+    b.step(30)
+    b.sync()
+    assert b.info()["launch"] == "per_step"
+    b.close()
+    for h in hs:
+        h.close()

@@ -76,6 +76,29 @@ def test_batch_wait_runs_out_reports_timeout():
         h.close()
 
 
+def test_persistent_batch_wait_runs_out_reports_timeout():
+    # the persistent launch's staging waits and its waits on the previous
+    # step of a scene share the batch's poll limit: with 0 they run out, the
+    # CTAs stop at their next ticket and the host reports the timeout
+    sims = configs.batched_sweep(n=3, seed=21, lo=18, hi=30, pml=5, dl=2e-3, precision="fp64")
+    hs = [X.Handle(*s.lower()) for s in sims]
+    b = X.Batch(hs, tile_rows=16, launch=L.BATCH_PERSISTENT)
+    b.init(20)
+    b.step(2)
+    b.sync()
+    b.set_wait_limit(0)
+    b.step(5)
+    with pytest.raises(L.XfbError) as e:
+        b.sync()
+    assert e.value.status == L.XFB_ERR_TIMEOUT
+    b.init(20)  # the limit and the flag start over
+    b.step(4)
+    b.sync()
+    b.close()
+    for h in hs:
+        h.close()
+
+
 def test_wait_limit_rejects_negative_and_paths_without_waits():
     h = _handle(_scene(), 4)
     with pytest.raises(L.XfbError) as e:

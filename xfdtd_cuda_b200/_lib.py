@@ -26,6 +26,7 @@ JA, JB, MA, MB = 0, 1, 2, 3
 ADE_NONE, ADE_DEBYE, ADE_DRUDE, ADE_MLORENTZ = 0, 1, 2, 3
 MAX_POLES = 4
 FAR_FIELD_STATIC_MAX_ANGLES = 4096  # XFB_FAR_FIELD_STATIC_MAX_ANGLES
+BATCH_AUTO, BATCH_PER_STEP, BATCH_PERSISTENT = 0, 1, 2  # xfb_batch_set_launch
 K_UPDATE_H, K_AUX, K_UPDATE_E, K_NF2FF, K_PROBE, K_MOVIE, K_STEP, K_CORRECT, K_COUNT = range(9)
 KERNEL_NAMES = ("k_h3/k_h2 (H half-step)", "k_aux (TFSF aux grid)", "k_e3/k_e2 (E half-step)", "k_nf2ff",
                 "k_probe", "k_movie", "k_step3 (one-sweep H+E step)",
@@ -190,6 +191,8 @@ SIGNATURES = [
     ("xfb_labc_wall_cells", C.c_int, [_H, C.POINTER(C.c_longlong)]),
     ("xfb_batch_create", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]),
     ("xfb_batch_set_tile", C.c_int, [C.c_void_p, C.c_int]),
+    ("xfb_batch_set_launch", C.c_int, [C.c_void_p, C.c_int]),
+    ("xfb_batch_launch_form", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     ("xfb_batch_init", C.c_int, [C.c_void_p, C.c_longlong]),
     ("xfb_batch_step", C.c_int, [C.c_void_p, C.c_longlong]),
     ("xfb_batch_sync", C.c_int, [C.c_void_p]),

@@ -147,13 +147,18 @@ int batch_err(xfb_batch* b, int code, const std::string& m) {
 void batch_free(xfb_batch* b) {
   for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
   b->graphs.clear();
-  void* ps[7] = {b->scenes, b->maps, b->items[0], b->items[1], b->items[2], b->t_dev, b->err_dev};
+  void* ps[14] = {b->scenes,       b->maps,           b->items[0],       b->items[1],       b->items[2],
+                  b->t_dev,        b->err_dev,        b->pitems[0],      b->pitems[1],      b->pitems[2],
+                  b->pscene_items[0], b->pscene_items[1], b->pscene_items[2], b->queue};
   for (void* p : ps) cudaFree(p);
   b->scenes = b->maps = nullptr;
   for (int t = 0; t < kStepTileCount; ++t) {
     b->items[t] = nullptr;
     b->n_items[t] = 0;
+    b->pitems[t] = nullptr;
+    b->pscene_items[t] = nullptr;
   }
+  b->queue = nullptr;
   b->t_dev = nullptr;
   b->err_dev = nullptr;
   b->inited = false;
@@ -1137,6 +1142,24 @@ int xfb_batch_set_tile(xfb_batch* b, int rows) {
   return XFB_OK;
 }
 
+int xfb_batch_set_launch(xfb_batch* b, int launch) {
+  if (!b) return set_err(nullptr, XFB_ERR_INVALID, "null batch");
+  if (launch != XFB_BATCH_AUTO && launch != XFB_BATCH_PER_STEP && launch != XFB_BATCH_PERSISTENT)
+    return batch_err(b, XFB_ERR_INVALID, "launch form must be XFB_BATCH_AUTO, XFB_BATCH_PER_STEP or XFB_BATCH_PERSISTENT");
+  if (b->inited && launch == XFB_BATCH_PERSISTENT && !b->persist_ok)
+    return batch_err(b, XFB_ERR_INVALID, "persistent batch launches need scenes without monitors or a separate ADE pass");
+  b->launch_req = launch;
+  b->launch = -1;
+  b->tile = -1;
+  return XFB_OK;
+}
+
+int xfb_batch_launch_form(const xfb_batch* b, int* launch) {
+  if (!b || !launch) return set_err(nullptr, XFB_ERR_INVALID, "null batch or output");
+  *launch = b->launch < 0 ? 0 : b->launch;
+  return XFB_OK;
+}
+
 int xfb_batch_init(xfb_batch* b, long long total_steps) {
   if (!b) return set_err(nullptr, XFB_ERR_INVALID, "null batch");
   if (b->inited) {
@@ -1178,6 +1201,7 @@ int xfb_batch_init(xfb_batch* b, long long total_steps) {
   b->step = 0;
   b->total = total_steps;
   b->tile = -1;
+  b->launch = -1;
   b->inited = true;
   return XFB_OK;
 }

@@ -1382,7 +1382,40 @@ int batch_init(xfb_batch* b) {
     }
     b->n_items[t] = static_cast<int>(all.size());
     if (!all.empty() && (rc = batch_upload(b, &b->items[t], all.data(), all.size() * sizeof(int4)))) return rc;
+    // the persistent form's list: the same items scene by scene (scenes with
+    // more work first), within a scene in the order above, so a scene's
+    // items of one step finish close together and its next step can start
+    // while later scenes finish theirs
+    std::vector<long long> work(b->hs.size(), 0);
+    std::vector<int> count(b->hs.size(), 0);
+    for (const int4& v : all) {
+      const int q = static_cast<int>(static_cast<unsigned>(v.x) >> 16);
+      work[q] += v.w - v.z;
+      ++count[q];
+    }
+    std::vector<int> order(b->hs.size());
+    for (size_t q = 0; q < order.size(); ++q) order[q] = static_cast<int>(q);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return work[a] > work[c]; });
+    std::vector<int> rank(order.size());
+    for (size_t r = 0; r < order.size(); ++r) rank[order[r]] = static_cast<int>(r);
+    std::vector<int4> per = all;
+    std::stable_sort(per.begin(), per.end(), [&](const int4& a, const int4& c) {
+      return rank[static_cast<unsigned>(a.x) >> 16] < rank[static_cast<unsigned>(c.x) >> 16];
+    });
+    if (!per.empty() && (rc = batch_upload(b, &b->pitems[t], per.data(), per.size() * sizeof(int4)))) return rc;
+    if ((rc = batch_upload(b, &b->pscene_items[t], count.data(), count.size() * sizeof(int)))) return rc;
   }
+  {
+    std::vector<unsigned> zero(1 + b->hs.size(), 0u);
+    if ((rc = batch_upload(b, reinterpret_cast<void**>(&b->queue), zero.data(), zero.size() * sizeof(unsigned)))) return rc;
+  }
+  b->persist_ok = true;
+  for (xfb_handle* h : b->hs) {
+    const Compiled& c = h->c;
+    if (h->ade_deferred || c.nf_on || c.td_on || !c.probes.empty() || !c.movies.empty()) b->persist_ok = false;
+  }
+  if (b->launch_req == XFB_BATCH_PERSISTENT && !b->persist_ok)
+    return batch_err(b, XFB_ERR_INVALID, "persistent batch launches need scenes without monitors or a separate ADE pass");
   cudaError_t e = cudaMalloc(&b->t_dev, sizeof(long long));
   if (e != cudaSuccess) return batch_err(b, XFB_ERR_OOM, "cudaMalloc (batch step counter)");
   e = cudaMemsetAsync(b->t_dev, 0, sizeof(long long), b->stream);
@@ -1406,6 +1439,34 @@ void batch_step3(xfb_batch* b, int t, TimeP tp, int parity) {
       static_cast<const int4*>(b->items[t]), tp, parity, t, b->err_dev);
 }
 
+// n steps of every scene in one persistent launch (k_step3_persist): as many
+// CTAs as fit on the device at once, each taking items from the queue.
+template <typename T, int R, int NWM>
+void batch_persist3(xfb_batch* b, int t, TimeP tp, int parity, int n) {
+  constexpr int NS = 4;
+  using S = StepCfg<T, R, NWM, NS>;
+  static bool attr_set[64] = {};
+  static int per_sm[64] = {};
+  const int dev = b->device & 63;
+  if (!attr_set[dev]) {
+    cudaFuncSetAttribute(k_step3_persist<T, R, NWM, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(S::bytes));
+    int blocks = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_step3_persist<T, R, NWM, NS>, S::NT, S::bytes);
+    per_sm[dev] = std::max(1, blocks);
+    attr_set[dev] = true;
+  }
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+  const long long tickets = static_cast<long long>(n) * b->n_items[t];
+  const int grid = static_cast<int>(std::min<long long>(tickets, static_cast<long long>(sms) * per_sm[dev]));
+  cudaMemsetAsync(b->queue, 0, (1 + b->hs.size()) * sizeof(unsigned), b->stream);
+  k_step3_persist<T, R, NWM, NS><<<grid, S::NT, S::bytes, b->stream>>>(
+      static_cast<const BatchScene<T>*>(b->scenes), static_cast<const BatchMaps*>(b->maps),
+      static_cast<const int4*>(b->pitems[t]), b->n_items[t], static_cast<const int*>(b->pscene_items[t]), tp, parity, n,
+      t, b->queue, b->err_dev);
+}
+
 // One step of every scene: the one-sweep kernel over all work items,
 // deferred ADE passes, monitors (the TFSF incident tables were computed when
 // each handle was initialised).
@@ -1426,14 +1487,24 @@ void batch_enqueue_step(xfb_batch* b, int off, int t) {
 }
 
 template <typename T>
-int batch_chunk(xfb_batch* b, int n, int t, bool graph) {
+int batch_chunk(xfb_batch* b, int n, int t, bool graph, int launch) {
   auto enqueue = [&]() {
-    for (int q = 0; q < n; ++q) batch_enqueue_step<T>(b, q, t);
+    if (launch == XFB_BATCH_PERSISTENT) {
+      if (b->n_items[t]) {
+        TimeP tp{b->t_dev, 0};
+        const int parity = static_cast<int>(b->step & 1);
+        if (t == 0) batch_persist3<T, kStepTiles[0].r, kStepTiles[0].nwm>(b, 0, tp, parity, n);
+        else if (t == 1) batch_persist3<T, kStepTiles[1].r, kStepTiles[1].nwm>(b, 1, tp, parity, n);
+        else batch_persist3<T, kStepTiles[2].r, kStepTiles[2].nwm>(b, 2, tp, parity, n);
+      }
+    } else {
+      for (int q = 0; q < n; ++q) batch_enqueue_step<T>(b, q, t);
+    }
     k_bump<<<1, 1, 0, b->stream>>>(b->t_dev, n);
   };
   cudaError_t e = cudaSuccess;
   if (graph) {
-    const int key = (n * 2 + static_cast<int>(b->step & 1)) * kStepTileCount + t;
+    const int key = ((n * 2 + static_cast<int>(b->step & 1)) * 3 + launch) * kStepTileCount + t;
     auto it = b->graphs.find(key);
     if (it == b->graphs.end()) {
       cudaGraph_t g;
@@ -1520,46 +1591,68 @@ inline void tile_cache_put(const std::string& key, int tile) {
 template <typename T>
 int batch_run(xfb_batch* b, long long n) {
   int rc;
-  if (b->tile < 0 && b->tile_req == 0) {  // an earlier autotune of the same scenes on this GPU
-    const int t = tile_cache_get(tile_cache_key(b));
-    if (t >= 0 && t < kStepTileCount) b->tile = t;
+  // candidate launch forms: per step always, persistent when the scenes allow
+  std::vector<int> forms;
+  if (b->launch_req != XFB_BATCH_PERSISTENT) forms.push_back(XFB_BATCH_PER_STEP);
+  if (b->launch_req != XFB_BATCH_PER_STEP && b->persist_ok) forms.push_back(XFB_BATCH_PERSISTENT);
+  if (b->tile < 0 && b->tile_req == 0 && b->launch_req == XFB_BATCH_AUTO) {  // an earlier autotune of the same scenes
+    const int v = tile_cache_get(tile_cache_key(b));
+    const int t = v % kStepTileCount, f = v / kStepTileCount;
+    if (v >= 0 && (f == XFB_BATCH_PER_STEP || (f == XFB_BATCH_PERSISTENT && b->persist_ok))) {
+      b->tile = t;
+      b->launch = f;
+    }
   }
   if (b->tile < 0) {
-    if (b->tile_req != 0 || n < 2 * kStepTileCount) {
-      b->tile = 1;
-      for (int t = 0; t < kStepTileCount; ++t)
-        if (kStepTileRows[t] == b->tile_req) b->tile = t;
+    std::vector<int> tiles;
+    for (int t = 0; t < kStepTileCount; ++t)
+      if (b->tile_req == 0 || kStepTileRows[t] == b->tile_req) tiles.push_back(t);
+    const long long cands = static_cast<long long>(tiles.size() * forms.size());
+    if (cands == 1 || n < 2 * cands) {  // nothing to choose, or too few steps to time: 16-row tiles, first form
+      b->tile = tiles.size() == 1 ? tiles[0] : 1;
+      b->launch = forms[0];
     } else {
-      for (int t = 0; t < kStepTileCount; ++t)
-        if ((rc = batch_chunk<T>(b, 1, t, false))) return rc;
-      n -= kStepTileCount;
-      const int probe = static_cast<int>(std::min<long long>(4, n / kStepTileCount));
-      float ms[kStepTileCount] = {};
+      // one untimed step per (tile, form) (the first launch of a kernel
+      // loads its module), then a few timed steps per (tile, form); keep the
+      // fastest
+      for (int f : forms)
+        for (int t : tiles)
+          if ((rc = batch_chunk<T>(b, 1, t, false, f))) return rc;
+      n -= cands;
+      const int probe = static_cast<int>(std::min<long long>(4, n / cands));
       cudaEvent_t ev[2];
       cudaEventCreate(&ev[0]);
       cudaEventCreate(&ev[1]);
       rc = XFB_OK;
-      for (int t = 0; t < kStepTileCount && !rc; ++t) {
-        cudaEventRecord(ev[0], b->stream);
-        if ((rc = batch_chunk<T>(b, probe, t, false))) break;
-        cudaEventRecord(ev[1], b->stream);
-        cudaError_t e = cudaEventSynchronize(ev[1]);
-        if (e != cudaSuccess) rc = batch_err(b, XFB_ERR_CUDA, cudaGetErrorString(e));
-        else cudaEventElapsedTime(&ms[t], ev[0], ev[1]);
-      }
+      float best = 0.0f;
+      for (int f : forms)
+        for (int t : tiles) {
+          if (rc) break;
+          float ms = 0.0f;
+          cudaEventRecord(ev[0], b->stream);
+          if ((rc = batch_chunk<T>(b, probe, t, false, f))) break;
+          cudaEventRecord(ev[1], b->stream);
+          cudaError_t e = cudaEventSynchronize(ev[1]);
+          if (e != cudaSuccess) rc = batch_err(b, XFB_ERR_CUDA, cudaGetErrorString(e));
+          else cudaEventElapsedTime(&ms, ev[0], ev[1]);
+          n -= probe;
+          if (!rc && (b->tile < 0 || ms < best)) {
+            best = ms;
+            b->tile = t;
+            b->launch = f;
+          }
+        }
       cudaEventDestroy(ev[0]);
       cudaEventDestroy(ev[1]);
       if (rc) return rc;
-      b->tile = 0;
-      for (int t = 1; t < kStepTileCount; ++t)
-        if (ms[t] < ms[b->tile]) b->tile = t;
-      tile_cache_put(tile_cache_key(b), b->tile);
-      n -= kStepTileCount * probe;
+      if (b->launch_req == XFB_BATCH_AUTO && b->tile_req == 0)
+        tile_cache_put(tile_cache_key(b), b->tile + kStepTileCount * b->launch);
     }
   }
+  if (b->launch < 0) b->launch = forms[0];
   while (n > 0) {
     const int chunk = static_cast<int>(std::min<long long>(n, b->graph_steps));
-    if ((rc = batch_chunk<T>(b, chunk, b->tile, true))) return rc;
+    if ((rc = batch_chunk<T>(b, chunk, b->tile, true, b->launch))) return rc;
     n -= chunk;
   }
   return XFB_OK;

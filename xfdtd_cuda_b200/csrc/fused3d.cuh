@@ -296,10 +296,13 @@ struct StepCfg {
   static constexpr int PL = (RH * RW + PLA - 1) / PLA * PLA;
   static constexpr int NT = (NWM + 1) * 32;  // row warps + halo warp
   // shared memory, from a 128-byte aligned base: field ring [NS][6][PL],
-  // material ring [NS][RH][MW], NS staging barriers, H planes, E planes of
+  // material ring [NS][MPL], NS staging barriers, H planes, E planes of
   // the lean interior body, LUT [LUTM][8], dispersive flags [LUTM]
   static constexpr size_t f_bytes = static_cast<size_t>(NS) * 6 * PL * sizeof(T);
-  static constexpr size_t m_bytes = static_cast<size_t>(NS) * RH * MW;
+  // material plane of the ring, rounded up so every plane starts on a
+  // 128-byte boundary (bulk-copy destinations)
+  static constexpr int MPL = (RH * MW + 127) / 128 * 128;
+  static constexpr size_t m_bytes = static_cast<size_t>(NS) * MPL;
   static constexpr size_t h_bytes = (2ull * 3 * HPL * sizeof(T) + 15) / 16 * 16;
   static constexpr size_t l_bytes = LUTM * 8 * sizeof(T);
   static constexpr size_t d_bytes = LUTM;
@@ -323,7 +326,6 @@ struct StepCfg {
   static_assert(NC >= RH && NC >= TK + 1, "coefficient table covers the tile with its halo");
   // bytes one staged plane brings (six field boxes and the material box)
   static constexpr unsigned tx_bytes = static_cast<unsigned>(6 * RH * RW * sizeof(T) + RH * MW);
-  static_assert((RH * MW) % 128 == 0, "material planes stay 128-byte aligned");
   // CTAs per SM that the 228 KB of shared memory per SM admits (1 KB reserved
   // per CTA), at most 4; the register budget is sized for that residency
   static constexpr int fit = static_cast<int>((228u * 1024u) / (bytes + 1024u));
@@ -566,7 +568,7 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* base = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
   T* sF = reinterpret_cast<T*>(base);                               // [NS][6][PL]
-  uint8_t* sM = base + L::off_m;                                    // [NS][RH][MW]
+  uint8_t* sM = base + L::off_m;                                    // [NS][MPL]: RH rows of MW
   uint64_t* bar = reinterpret_cast<uint64_t*>(base + L::off_b);     // [NS]
   T* sH = reinterpret_cast<T*>(base + L::off_h);                    // [2][3][HH][HW]
   T* sL = reinterpret_cast<T*>(base + L::off_l);                    // [LUTM][8]
@@ -623,7 +625,7 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
         T* dst = sF + st * 6 * PL;
 #pragma unroll
         for (int f = 0; f < 6; ++f) tma_load_3d(dst + f * PL, &maps->f[f], k0 - HP, j0 - 1, plane, bar + st);
-        tma_load_3d(sM + st * RH * MW, &maps->mid, k0 - 16, j0 - 1, plane, bar + st);
+        tma_load_3d(sM + st * L::MPL, &maps->mid, k0 - 16, j0 - 1, plane, bar + st);
       }
       return;
     }
@@ -646,7 +648,7 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
       const uint8_t* gm = s.mid + pb;
 #pragma unroll
       for (int c = 0; c < NMC; ++c)
-        if (mok[c]) cp_async16(sM + st * RH * MW + mso[c], gm + mgo[c]);
+        if (mok[c]) cp_async16(sM + st * L::MPL + mso[c], gm + mgo[c]);
     }
     cp_async_commit();
   };
@@ -743,7 +745,7 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
     stage(i + NS - 1, slot_p);  // whose last readers finished iteration i-1
     const T* Fc = sF + slot * 6 * PL;
     const T* Fn = sF + slot_n * 6 * PL;
-    const uint8_t* Mc = sM + slot * RH * MW;
+    const uint8_t* Mc = sM + slot * L::MPL;
     slot = slot_n;
     T* Hc = sH + (i & 1) * 3 * HPL;              // H plane i (written here)
     const T* Hq = sH + ((i + 1) & 1) * 3 * HPL;  // H plane i-1
@@ -905,7 +907,7 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* base = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
   T* sF = reinterpret_cast<T*>(base);                            // [NS][6][PL]
-  uint8_t* sM = base + L::off_m;                                 // [NS][RH][MW]
+  uint8_t* sM = base + L::off_m;                                 // [NS][MPL]: RH rows of MW
   uint64_t* bar = reinterpret_cast<uint64_t*>(base + L::off_b);  // [NS]
   T* sH = reinterpret_cast<T*>(base + L::off_h);                 // [2][3][CS]
   T* sE = reinterpret_cast<T*>(base + L::off_e);                 // [2][3][TJ * 32]
@@ -951,7 +953,7 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
       T* dst = sF + st * 6 * PL;
 #pragma unroll
       for (int f = 0; f < 6; ++f) tma_load_3d(dst + f * PL, &maps->f[f], k0 - HP, j0 - 1, plane, bar + st);
-      tma_load_3d(sM + st * RH * MW, &maps->mid, k0 - 16, j0 - 1, plane, bar + st);
+      tma_load_3d(sM + st * L::MPL, &maps->mid, k0 - 16, j0 - 1, plane, bar + st);
     }
   };
   for (int q = 0; q < NS - 1; ++q) stage(i_first + q, (i_first + q) % NS);
@@ -1098,7 +1100,7 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
     }
     const T* Fc = sF + slot * 6 * PL;
     const T* Fn = sF + slot_n * 6 * PL;
-    const uint8_t* Mc = sM + slot * RH * MW;
+    const uint8_t* Mc = sM + slot * L::MPL;
     slot = slot_n;
     T* Hc = sH + (i & 1) * 3 * CS;              // H plane i (written here)
     const T* Hq = sH + ((i + 1) & 1) * 3 * CS;  // H plane i-1
@@ -1403,6 +1405,107 @@ __global__ void __launch_bounds__(StepCfg<T, R, NWM, NS_>::NT, StepCfg<T, R, NWM
   step_dispatch<T, R, NWM, NS_, true>(sp.g[parity], sp.g[1 - parity], sp.pm, sp.psh[parity], sp.psh[1 - parity],
                                       sp.tf, sp.ad, item, sp.lut8, sp.disp, sp.n_mat, &bm.stage[tile][parity],
                                       &bm.store[tile][1 - parity], err);
+}
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void red_release_gpu_add(unsigned* p, unsigned v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+// orders generic-proxy accesses to global memory with later (or, on the
+// writing side, earlier) async-proxy accesses: bulk tensor copies of data
+// other CTAs wrote with plain stores, and plain reads of data bulk stores wrote
+__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_inval(uint64_t* b) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smem_u32(b)) : "memory");
+}
+
+// Persistent form of the batch step: n_steps steps of every scene in one
+// launch.  A grid of resident CTAs draws tickets from a device queue
+// (queue[0]); ticket q is item q % n_items of step q / n_items, so all items
+// of a step are handed out before any of the next.  An item of step s > 0
+// starts once every item of step s - 1 of its scene has finished: each CTA
+// counts its finished items per scene (queue[1 + scene], release), the
+// next step's items of that scene wait for the count s * scene_items[scene]
+// (acquire).  That is the whole step-to-step dependency of a scene: the step
+// reads the field set its previous step wrote and writes the set that step
+// read.  Items are listed scene by scene, so a scene's next step can start
+// while later scenes still finish the current one; no CTA ever waits for an
+// item that has not been handed out, so the queue cannot deadlock.  The
+// waits are bounded (err[1] polls, as the staging waits); a wait that runs
+// out, or any earlier error, sets err[0] and every CTA stops at its next
+// ticket.  queue[] is zeroed before each launch.
+template <typename T, int R, int NWM, int NS_>
+__global__ void __launch_bounds__(StepCfg<T, R, NWM, NS_>::NT, StepCfg<T, R, NWM, NS_>::min_blocks)
+    k_step3_persist(const BatchScene<T>* scenes, const BatchMaps* maps, const int4* items, int n_items,
+                    const int* scene_items, TimeP tp, int parity0, int n_steps, int tile, unsigned* queue, int* err) {
+  using L = StepCfg<T, R, NWM, NS_>;
+  __shared__ BatchScene<T> sp;
+  __shared__ TfsfP s_tf;
+  __shared__ unsigned s_ticket;
+  __shared__ int s_go;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u) + L::off_b);
+  unsigned* done = queue + 1;
+  const unsigned tickets = static_cast<unsigned>(n_steps) * static_cast<unsigned>(n_items);
+  const long long t0 = cur_step(tp);
+  int cur = -1;  // scene whose parameters sit in sp
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const unsigned q = atomicAdd(queue, 1u);
+      int go = q < tickets && *reinterpret_cast<volatile int*>(err) == 0;
+      if (go && q >= static_cast<unsigned>(n_items)) {
+        const unsigned s = q / static_cast<unsigned>(n_items);
+        const int scene = static_cast<int>(static_cast<unsigned>(items[q - s * n_items].x) >> 16);
+        const unsigned need = s * static_cast<unsigned>(scene_items[scene]);
+        const int polls = err[1];
+        int n = 0;
+        while (ld_acquire_gpu(done + scene) < need) {
+          if (*reinterpret_cast<volatile int*>(err) != 0) { go = 0; break; }
+          if (++n > polls) {
+            atomicExch(err, 1);
+            go = 0;
+            break;
+          }
+          __nanosleep(128);
+        }
+        fence_proxy_async_global();  // the previous step's writes, before this CTA's bulk copies read them
+      }
+      s_ticket = q;
+      s_go = go;
+    }
+    __syncthreads();
+    if (!s_go) break;
+    const unsigned q = s_ticket;
+    const unsigned s = q / static_cast<unsigned>(n_items);
+    const int4 it = items[q - s * n_items];
+    const int scene = static_cast<int>(static_cast<unsigned>(it.x) >> 16);
+    if (scene != cur) {
+      const int* src = reinterpret_cast<const int*>(scenes + scene);
+      int* dst = reinterpret_cast<int*>(&sp);
+      for (int w = threadIdx.x; w < static_cast<int>(sizeof(BatchScene<T>) / 4); w += blockDim.x) dst[w] = src[w];
+      cur = scene;
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) s_tf = tfsf_at_step(sp.tf, t0 + s);  // incident-table rows of this item's step
+    __syncthreads();
+    const int parity = (parity0 + static_cast<int>(s)) & 1;
+    const int4 item = make_int4((it.x & 0x7ff) | (((it.x >> 11) & 0x1f) << 16), it.y, it.z, it.w);
+    const BatchMaps& bm = maps[scene];
+    step_dispatch<T, R, NWM, NS_, true>(sp.g[parity], sp.g[1 - parity], sp.pm, sp.psh[parity], sp.psh[1 - parity],
+                                        s_tf, sp.ad, item, sp.lut8, sp.disp, sp.n_mat, &bm.stage[tile][parity],
+                                        &bm.store[tile][1 - parity], err);
+    __threadfence();  // this thread's plain stores of the item, before the count below
+    __syncthreads();  // every thread is done with the item and its shared memory
+    if (threadIdx.x == 0) {
+      for (int b = 0; b < NS_; ++b) mbar_inval(bar + b);  // the next item initialises them again
+      fence_proxy_async_global();  // the item's bulk stores (completed by this thread), before the count
+      red_release_gpu_add(done + scene, 1u);
+    }
+  }
 }
 
 }  // namespace xfb

@@ -151,8 +151,9 @@ struct xfb_handle {
 };
 
 // A batch of scenes stepped together: one launch of the one-sweep kernel per
-// step over the work items of every scene.  The handles stay owned by the
-// caller; the batch owns only its tables, stream, counter and graphs.
+// step over the work items of every scene, or one persistent launch for a
+// chunk of steps (k_step3_persist).  The handles stay owned by the caller;
+// the batch owns only its tables, stream, counters and graphs.
 struct xfb_batch {
   std::vector<xfb_handle*> hs;
   std::string err;
@@ -171,6 +172,15 @@ struct xfb_batch {
   int n_items[3] = {};
   long long* t_dev = nullptr;
   std::map<int, cudaGraphExec_t> graphs;
+  // persistent launches (XFB_BATCH_PERSISTENT): work lists scene by scene,
+  // items per scene, and the queue (ticket counter, then one finished-item
+  // counter per scene), per tile configuration
+  int launch_req = XFB_BATCH_AUTO;  // xfb_batch_set_launch
+  int launch = -1;                  // XFB_BATCH_PER_STEP or XFB_BATCH_PERSISTENT (-1 until chosen)
+  bool persist_ok = false;          // no scene records monitors or runs a separate ADE pass
+  void* pitems[3] = {};
+  void* pscene_items[3] = {};
+  unsigned* queue = nullptr;
 };
 
 namespace xfb {

@@ -849,9 +849,11 @@ class Handle:
 class Batch:
     """Steps many 3-D scenes of one precision together (xfb_batch_*): one
     launch of the one-sweep kernel per step over the work items of every
-    scene.  The Handles stay usable for read-back after ``sync()``."""
+    scene, or one persistent launch per chunk of steps (``launch``:
+    L.BATCH_AUTO picks the faster on the first steps).  The Handles stay
+    usable for read-back after ``sync()``."""
 
-    def __init__(self, handles, tile_rows: int = 0):
+    def __init__(self, handles, tile_rows: int = 0, launch: int = L.BATCH_AUTO):
         self.lib = L.load()
         self.handles = list(handles)
         arr = (C.c_void_p * len(self.handles))(*[h.h for h in self.handles])
@@ -861,6 +863,7 @@ class Batch:
             raise L.XfbError(st, self.lib.xfb_last_error(None).decode())
         self.b = b
         self._c(self.lib.xfb_batch_set_tile(self.b, tile_rows))
+        self._c(self.lib.xfb_batch_set_launch(self.b, launch))
 
     def _c(self, status):
         if status != L.XFB_OK:
@@ -887,7 +890,10 @@ class Batch:
     def info(self):
         cells, rows, items = C.c_longlong(), C.c_int(), C.c_int()
         self._c(self.lib.xfb_batch_info(self.b, C.byref(cells), C.byref(rows), C.byref(items)))
-        return {"cells": cells.value, "tile_rows": rows.value, "work_items": items.value}
+        form = C.c_int()
+        self._c(self.lib.xfb_batch_launch_form(self.b, C.byref(form)))
+        return {"cells": cells.value, "tile_rows": rows.value, "work_items": items.value,
+                "launch": {0: "unchosen", 1: "per_step", 2: "persistent"}[form.value]}
 
     def close(self):
         if getattr(self, "b", None):
