@@ -147,9 +147,8 @@ int batch_err(xfb_batch* b, int code, const std::string& m) {
 void batch_free(xfb_batch* b) {
   for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
   b->graphs.clear();
-  void* ps[14] = {b->scenes,       b->maps,           b->items[0],       b->items[1],       b->items[2],
-                  b->t_dev,        b->err_dev,        b->pitems[0],      b->pitems[1],      b->pitems[2],
-                  b->pscene_items[0], b->pscene_items[1], b->pscene_items[2], b->queue};
+  void* ps[11] = {b->scenes,  b->maps,           b->items[0],       b->items[1],       b->items[2],     b->t_dev,
+                  b->err_dev, b->pscene_items[0], b->pscene_items[1], b->pscene_items[2], b->queue};  // pitems alias items
   for (void* p : ps) cudaFree(p);
   b->scenes = b->maps = nullptr;
   for (int t = 0; t < kStepTileCount; ++t) {
@@ -1183,7 +1182,9 @@ int xfb_batch_init(xfb_batch* b, long long total_steps) {
     h->batch = nullptr;  // xfb_init is refused for batched handles
     if (h->device < 0) cudaSetDevice(dev);  // xfb_init adopts the current device
     h->path = XFB_PATH_FUSED;
+    h->no_lines = true;  // the batch kernels compute the TFSF incident values in place
     int rc = xfb_init(h, total_steps);
+    h->no_lines = false;
     h->batch = b;
     if (rc) return batch_err(b, rc, "scene init failed: " + h->err);
     b->cells += static_cast<long long>(h->c.nx) * h->c.ny * h->c.nz;

@@ -121,6 +121,14 @@ int init_device(xfb_handle* h) {
     if ((rc = upload<T>(h, &h->lut, round_coefficients(c.coeff, h->coeff_storage)))) return rc;
     if ((rc = upload<T>(h, &h->lut8, round_coefficients(c.coeff8, h->coeff_storage)))) return rc;
   }
+  h->lines_on = fused(h) && c.dim == 3 && c.tfsf_on && !h->no_lines;
+  if (h->lines_on) {  // TFSF line tables: [face][plane][component][k or j]
+    h->line_ykp = h->nzp;
+    h->line_zjp = roundup(c.ny, 2);
+    const size_t ny_el = 2ull * (c.nx + 1) * 2 * h->line_ykp, nz_el = 2ull * (c.nx + 1) * 2 * h->line_zjp;
+    for (int q = 0; q < 4; ++q)
+      if ((rc = alloc(h, &h->line_tab[q], (q < 2 ? ny_el : nz_el) * sizeof(double), false))) return rc;
+  }
   if (fused(h) && c.dim == 3 && (rc = upload_step_items(h))) return rc;
   if (fused(h) && c.dim == 3 && h->ade_deferred && (rc = upload_ade_runs(h))) return rc;
   if (fused(h) && c.dim == 3) {
@@ -435,7 +443,8 @@ inline bool tfsf_touch(const Compiled& c, int p, int q, int j0, int TJ, int k0) 
 // below the range and the halo row and column of the tile) need no more than
 // the range's kind handles.  Ranges are at most `ich` planes long.
 inline void build_step_items(const Compiled& c, int TJ, int NT, bool ade_deferred, std::vector<int4> (&out)[kStepKindCount],
-                             int plane_chunk = 0, bool lean_interior = false, int p0 = 0, int p1 = -1) {
+                             int plane_chunk = 0, bool lean_interior = false, int p0 = 0, int p1 = -1,
+                             bool lines = false) {
   const int nx = c.nx, ny = c.ny, nz = c.nz;
   if (p1 < 0) p1 = nx;  // planes [p0, p1): the whole grid, or an x slab
   const int* L = c.pml;
@@ -486,6 +495,12 @@ inline void build_step_items(const Compiled& c, int TJ, int NT, bool ade_deferre
         if (lean_interior && (kind == 3 || kind == 4 || kind == 5)) kind = kind == 3 ? kFastY : kind == 4 ? kFastZ : kFastYZ;
         if (lean_interior && (kind == 11 || kind == 12 || kind == 13))
           kind = kind == 11 ? kFastYTf : kind == 12 ? kFastZTf : kFastYZTf;
+        // with staged TFSF lines the bulk-copy TFSF bodies hold one face of
+        // the box per axis; a tile that meets both (a box thinner than a
+        // tile) runs the general body, which computes every incident value
+        if (lines && (kind == kLeanInteriorTf || kind == kFastYTf || kind == kFastZTf || kind == kFastYZTf) &&
+            (tfsf_line_face(c.tf[2], c.tf[3], j0, TJ) == 2 || tfsf_line_face(c.tf[4], c.tf[5], k0, 32) == 2))
+          kind = kind == kLeanInteriorTf ? 7 : kind == kFastYTf ? 11 : kind == kFastZTf ? 12 : 13;
         out[kind].push_back(make_int4(bx, by, p, q));
         p = q;
       }
@@ -568,8 +583,41 @@ int encode_stage_maps(xfb_handle* h) {
                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
       if (r != CUDA_SUCCESS) return set_err(h, XFB_ERR_CUDA, "cuTensorMapEncodeTiled (ids) failed: " + std::to_string(r));
     }
+    if (h->lines_on) {  // TFSF line tables as (k or j, component, plane, face), boxes of one plane's line pair
+      for (int q = 0; q < 4; ++q) {
+        const cuuint64_t w = static_cast<cuuint64_t>(q < 2 ? h->line_ykp : h->line_zjp);
+        const cuuint64_t ldims[4] = {w, 2, static_cast<cuuint64_t>(c.nx + 1), 2};
+        const cuuint64_t lstr[3] = {w * 8, 2 * w * 8, static_cast<cuuint64_t>(c.nx + 1) * 2 * w * 8};
+        const cuuint32_t lbox[4] = {static_cast<cuuint32_t>(q < 2 ? 34 : TJ + 2), 2, 1, 1};
+        const cuuint32_t lestr[4] = {1, 1, 1, 1};
+        CUresult r = enc(&h->line_maps[t][q], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, h->line_tab[q], ldims, lstr, lbox,
+                         lestr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return set_err(h, XFB_ERR_CUDA, "cuTensorMapEncodeTiled (TFSF lines) failed: " + std::to_string(r));
+      }
+    }
   }
   return XFB_OK;
+}
+
+inline LineP line_params(const xfb_handle* h) {
+  LineP lp{};
+  lp.yh = static_cast<double*>(h->line_tab[0]); lp.ye = static_cast<double*>(h->line_tab[1]);
+  lp.zh = static_cast<double*>(h->line_tab[2]); lp.ze = static_cast<double*>(h->line_tab[3]);
+  lp.ykp = h->line_ykp; lp.zjp = h->line_zjp;
+  lp.ysl = 2 * h->line_ykp; lp.zsl = 2 * h->line_zjp;
+  lp.yfs = static_cast<long long>(h->c.nx + 1) * lp.ysl; lp.zfs = static_cast<long long>(h->c.nx + 1) * lp.zsl;
+  return lp;
+}
+
+// The TFSF line values of one step (before the step kernel that reads them).
+template <typename T>
+void launch_lines(xfb_handle* h, TimeP tp, cudaStream_t st) {
+  const Compiled& c = h->c;
+  const long long ni = c.tf[1] - c.tf[0] + 1, nj = c.tf[3] - c.tf[2] + 1, nk = c.tf[5] - c.tf[4] + 1;
+  const long long work = 2 * ni * (nj + nk);
+  const int blocks = static_cast<int>(std::min<long long>((work + 255) / 256, 148LL * 8));
+  k_tfsf_lines<T><<<blocks, 256, 0, st>>>(tfsf_params(h), tp, line_params(h));
 }
 
 // Tables of the time-domain NF2FF: the sample points of every (face, field
@@ -679,7 +727,7 @@ inline int upload_step_items(xfb_handle* h) {
     std::vector<int4> items[kStepKindCount];
     const int nt = (kStepTiles[t].nwm + 1) * 32;
     build_step_items(h->c, kStepTiles[t].r * kStepTiles[t].nwm, nt, h->ade_deferred, items, 0, true,
-                     is_slab(h) ? h->slab_i0 : 0, is_slab(h) ? h->slab_i1 : -1);
+                     is_slab(h) ? h->slab_i0 : 0, is_slab(h) ? h->slab_i1 : -1, h->lines_on);
     // one list, the kind in the high half of .x: first the costly kinds (y/z
     // CPML columns, in-kernel ADE), costliest first, so the long items start
     // early; then the lean and x-slab items ordered by first plane, then row
@@ -779,10 +827,13 @@ void launch_step3(xfb_handle* h, int t, int parity, TimeP tp, cudaStream_t st) {
   maps.mid = h->stage_maps[t][parity][6];
   StoreMaps outs;
   std::memcpy(outs.f, h->store_maps[t][1 - parity], sizeof(outs.f));
+  LineMaps lines;
+  if (h->lines_on) std::memcpy(&lines, h->line_maps[t], sizeof(lines));
+  else std::memset(&lines, 0, sizeof(lines));
   k_step3<T, R, NWM, NS><<<h->n_step_items[t], S::NT, S::bytes, st>>>(
       grid_params<T>(h, parity), grid_params<T>(h, 1 - parity), pml_params<T>(h), psi_h_set<T>(h, parity),
       psi_h_set<T>(h, 1 - parity), tfsf_params(h), step_ade, tp, static_cast<const int4*>(h->step_items[t]),
-      as<const T>(h->lut8), h->mat_disp, h->c.n_mat, maps, outs, h->step_err);
+      as<const T>(h->lut8), h->mat_disp, h->c.n_mat, maps, outs, lines, h->step_err);
 }
 
 // One-sweep step: one launch over all work items, for the tile the launch
@@ -983,6 +1034,13 @@ void enqueue_update(xfb_handle* h, int off, Prof* pf) {
           grid_params<T>(h, parity), grid_params<T>(h, 1 - parity), pml_params<T>(h), psi_h_set<T>(h, parity),
           psi_h_set<T>(h, 1 - parity), tfsf_params(h), tp, ich, h->c.n_mat);
     } else {
+      if (h->lines_on) {
+        prof_end(h, pf);
+        prof_begin(h, pf, XFB_K_AUX);
+        launch_lines<T>(h, tp, s);
+        prof_end(h, pf);
+        prof_begin(h, pf, XFB_K_STEP);
+      }
       launch_fused<T>(h, parity, tp, s);
     }
     if (h->ade_deferred) launch_ade<T>(h, parity, s);
@@ -1382,28 +1440,14 @@ int batch_init(xfb_batch* b) {
     }
     b->n_items[t] = static_cast<int>(all.size());
     if (!all.empty() && (rc = batch_upload(b, &b->items[t], all.data(), all.size() * sizeof(int4)))) return rc;
-    // the persistent form's list: the same items scene by scene (scenes with
-    // more work first), within a scene in the order above, so a scene's
-    // items of one step finish close together and its next step can start
-    // while later scenes finish theirs
-    std::vector<long long> work(b->hs.size(), 0);
+    // the persistent form takes the same list (costliest kinds of all scenes
+    // first): listing the items scene by scene, which would let a scene's
+    // next step start early, measured 1.6x slower on the 64-scene sweep even
+    // for a single step; and the number of items of every scene
     std::vector<int> count(b->hs.size(), 0);
-    for (const int4& v : all) {
-      const int q = static_cast<int>(static_cast<unsigned>(v.x) >> 16);
-      work[q] += v.w - v.z;
-      ++count[q];
-    }
-    std::vector<int> order(b->hs.size());
-    for (size_t q = 0; q < order.size(); ++q) order[q] = static_cast<int>(q);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return work[a] > work[c]; });
-    std::vector<int> rank(order.size());
-    for (size_t r = 0; r < order.size(); ++r) rank[order[r]] = static_cast<int>(r);
-    std::vector<int4> per = all;
-    std::stable_sort(per.begin(), per.end(), [&](const int4& a, const int4& c) {
-      return rank[static_cast<unsigned>(a.x) >> 16] < rank[static_cast<unsigned>(c.x) >> 16];
-    });
-    if (!per.empty() && (rc = batch_upload(b, &b->pitems[t], per.data(), per.size() * sizeof(int4)))) return rc;
+    for (const int4& v : all) ++count[static_cast<unsigned>(v.x) >> 16];
     if ((rc = batch_upload(b, &b->pscene_items[t], count.data(), count.size() * sizeof(int)))) return rc;
+    b->pitems[t] = b->items[t];  // shared, freed once
   }
   {
     std::vector<unsigned> zero(1 + b->hs.size(), 0u);

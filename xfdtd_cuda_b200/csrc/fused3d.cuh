@@ -57,6 +57,13 @@ struct StoreMaps {
   CUtensorMap f[6];
 };
 
+// Tensor maps of the TFSF line tables (k_tfsf_lines): yh, ye as 4-D tensors
+// (k, component, i, face), box (34 x 2 x 1 x 1) from k0 - 2; zh, ze as
+// (j, component, i, face), box (TJ + 2) x 2 x 1 x 1 from j0 - 2.
+struct LineMaps {
+  CUtensorMap yh, ye, zh, ze;
+};
+
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
 }
@@ -99,6 +106,14 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
       "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
       "[%5];\n" ::"r"(smem_u32(dst)),
       "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int x, int y, int z, int w,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];\n" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(w), "r"(smem_u32(bar))
       : "memory");
 }
 // Tiled bulk store of one box from shared memory (bulk-group completion).
@@ -322,7 +337,17 @@ struct StepCfg {
   static constexpr int NC = 40;
   static constexpr size_t off_c = (off_d + d_bytes + 15) / 16 * 16;
   static constexpr size_t c_bytes = 8 * NC * sizeof(T);  // column axis, and z of a corner tile
-  static constexpr size_t bytes = off_c + c_bytes + 128;  // + alignment slack of the base
+  // TFSF line values of the items on the TFSF surface, a ring of NS slots
+  // filled with the planes: per slot the y-line box (2 components x YW
+  // doubles from k0 - 2) of the H pass at the slot's plane i and of the E pass
+  // at plane i - 1, then the z-line boxes (2 x ZW from j0 - 2) likewise, each
+  // box 128-byte aligned
+  static constexpr int YW = TK + 2, ZW = TJ + 2;
+  static constexpr int YB = (2 * YW * 8 + 127) / 128 * 128, ZB = (2 * ZW * 8 + 127) / 128 * 128;
+  static constexpr int LSLOT = 2 * YB + 2 * ZB;
+  static constexpr size_t off_t = (off_c + c_bytes + 127) / 128 * 128;
+  static constexpr size_t bytes = off_t + static_cast<size_t>(NS) * LSLOT + 128;  // + alignment slack of the base
+  static_assert((ZW * 8) % 16 == 0, "z-line boxes span whole 16-byte granules");
   static_assert(NC >= RH && NC >= TK + 1, "coefficient table covers the tile with its halo");
   // bytes one staged plane brings (six field boxes and the material box)
   static constexpr unsigned tx_bytes = static_cast<unsigned>(6 * RH * RW * sizeof(T) + RH * MW);
@@ -419,6 +444,91 @@ __device__ __forceinline__ void tfsf_e(const TfsfP& tf, const Inc& in, int i, in
     if (i == tf.is) add_inc(eyv, in.hz(tf.is - 1, j, k), tf.ca[0]);
     if (i == tf.ie) add_inc(eyv, in.hz(tf.ie, j, k), -tf.ca[0]);
   }
+}
+
+// TFSF line values of one plane, staged in shared memory from the line
+// tables: the two components of the tile's y line (from k0 - 2, pitch yw)
+// and of its z line (from j0 - 2, pitch zw).
+struct LineVals {
+  const double* y;
+  const double* z;
+  int yw, zw, k0m2, j0m2;
+};
+
+// tfsf_h with the incident values of the y- and z-face lines taken from the
+// staged lines (the x-face planes still from `in`): the same terms in the
+// same order, so the result is unchanged.  yh holds (ex, ez) at the face row
+// (js for the row js-1, je for je), zh (ey, ex) at the face column.
+template <typename T, class Inc>
+__device__ __forceinline__ void tfsf_h_lines(const TfsfP& tf, const Inc& in, const LineVals& lv, int i, int jj, int kk,
+                                             T& hxv, T& hyv, T& hzv) {
+  const bool iin = i >= tf.is && i <= tf.ie, jin = jj >= tf.js && jj <= tf.je, kin = kk >= tf.ks && kk <= tf.ke;
+  if (jin && jj < tf.je && kin) {
+    if (i == tf.is - 1) add_inc(hzv, in.ey(tf.is, jj, kk), tf.cb[0]);
+    if (i == tf.ie) add_inc(hzv, in.ey(tf.ie, jj, kk), -tf.cb[0]);
+  }
+  if (iin && i < tf.ie && kin) {
+    if (jj == tf.js - 1) add_inc(hzv, lv.y[kk - lv.k0m2], -tf.cb[1]);
+    if (jj == tf.je) add_inc(hzv, lv.y[kk - lv.k0m2], tf.cb[1]);
+  }
+  if (iin && jin && jj < tf.je) {
+    if (kk == tf.ks - 1) add_inc(hxv, lv.z[jj - lv.j0m2], -tf.cb[2]);
+    if (kk == tf.ke) add_inc(hxv, lv.z[jj - lv.j0m2], tf.cb[2]);
+  }
+  if (iin && kin && kk < tf.ke) {
+    if (jj == tf.js - 1) add_inc(hxv, lv.y[lv.yw + kk - lv.k0m2], tf.cb[1]);
+    if (jj == tf.je) add_inc(hxv, lv.y[lv.yw + kk - lv.k0m2], -tf.cb[1]);
+  }
+  if (iin && i < tf.ie && jin) {
+    if (kk == tf.ks - 1) add_inc(hyv, lv.z[lv.zw + jj - lv.j0m2], tf.cb[2]);
+    if (kk == tf.ke) add_inc(hyv, lv.z[lv.zw + jj - lv.j0m2], -tf.cb[2]);
+  }
+  if (jin && kin && kk < tf.ke) {
+    if (i == tf.is - 1) add_inc(hyv, in.ez(tf.is, jj, kk), -tf.cb[0]);
+    if (i == tf.ie) add_inc(hyv, in.ez(tf.ie, jj, kk), tf.cb[0]);
+  }
+}
+
+// tfsf_e likewise: ye holds (hx, hz) at the row js-1 (for the row js) or je,
+// ze (hy, hx) at the column ks-1 (for ks) or ke.
+template <typename T, class Inc>
+__device__ __forceinline__ void tfsf_e_lines(const TfsfP& tf, const Inc& in, const LineVals& lv, int i, int j, int k,
+                                             T& exv, T& eyv, T& ezv) {
+  const bool iin = i >= tf.is && i <= tf.ie, jin = j >= tf.js && j <= tf.je, kin = k >= tf.ks && k <= tf.ke;
+  if (jin && kin && k < tf.ke) {
+    if (i == tf.is) add_inc(ezv, in.hy(tf.is - 1, j, k), -tf.ca[0]);
+    if (i == tf.ie) add_inc(ezv, in.hy(tf.ie, j, k), tf.ca[0]);
+  }
+  if (iin && kin && k < tf.ke) {
+    if (j == tf.js) add_inc(ezv, lv.y[k - lv.k0m2], tf.ca[1]);
+    if (j == tf.je) add_inc(ezv, lv.y[k - lv.k0m2], -tf.ca[1]);
+  }
+  if (iin && i < tf.ie && jin) {
+    if (k == tf.ks) add_inc(exv, lv.z[j - lv.j0m2], tf.ca[2]);
+    if (k == tf.ke) add_inc(exv, lv.z[j - lv.j0m2], -tf.ca[2]);
+  }
+  if (iin && i < tf.ie && kin) {
+    if (j == tf.js) add_inc(exv, lv.y[lv.yw + k - lv.k0m2], -tf.ca[1]);
+    if (j == tf.je) add_inc(exv, lv.y[lv.yw + k - lv.k0m2], tf.ca[1]);
+  }
+  if (iin && jin && j < tf.je) {
+    if (k == tf.ks) add_inc(eyv, lv.z[lv.zw + j - lv.j0m2], -tf.ca[2]);
+    if (k == tf.ke) add_inc(eyv, lv.z[lv.zw + j - lv.j0m2], tf.ca[2]);
+  }
+  if (jin && j < tf.je && kin) {
+    if (i == tf.is) add_inc(eyv, in.hz(tf.is - 1, j, k), tf.ca[0]);
+    if (i == tf.ie) add_inc(eyv, in.hz(tf.ie, j, k), -tf.ca[0]);
+  }
+}
+
+// Face of the TFSF box whose y (z) line a tile meets: 0 the low face (the H
+// row js-1 among the tile's H rows j0-1 .. j0+TJ-1, or the E row js among its
+// rows j0 .. j0+TJ-1), 1 the high face (je), -1 none; 2 both (tiles of boxes
+// thinner than a tile, which the host gives the general body).
+__device__ __host__ __forceinline__ int tfsf_line_face(int lo, int hi, int c0, int n) {
+  const bool f0 = (lo - 1 >= c0 - 1 && lo - 1 <= c0 + n - 1) || (lo >= c0 && lo <= c0 + n - 1);
+  const bool f1 = hi >= c0 - 1 && hi <= c0 + n - 1;
+  return f0 && f1 ? 2 : f0 ? 0 : f1 ? 1 : -1;
 }
 
 // H^{n+1/2} of cell c at plane i: hNext from the staged E^n planes i and i+1
@@ -892,18 +1002,18 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
 // each cell (H of the next plane, E of the current one) is loaded a plane
 // ahead; x-slab psi (planes near the x faces) inline.  TF: with the TFSF
 // corrections of the cells on the TFSF surface.
-template <typename T, int R, int NWM, int NS_, bool TF, int PK>
+template <typename T, int R, int NWM, int NS_, bool TF, int PK, bool LN>
 __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>& pm, const PsiH<T>& ps,
                                                const PsiH<T>& pd, int4 item, const T* lut8, int n_mat,
                                                const TfsfP& tf, const StageMaps* maps, const StoreMaps* outs,
-                                               int* err) {
+                                               const LineMaps* lines, int* err) {
   using L = StepCfg<T, R, NWM, NS_>;
-  constexpr int NS = L::NS, HP = L::HP, RW = L::RW, MW = L::MW, TJ = L::TJ, PL = L::PL, NT = L::NT, RH = L::RH;
+  constexpr int NS = L::NS, HP = L::HP, RW = L::RW, MW = L::MW, TJ = L::TJ, PL = L::PL, NT = L::NT;
   constexpr int CS = L::LCS, ET = TJ * 32;
   constexpr bool PX = (PK & 1) != 0, PY = (PK & 2) != 0, PZ = (PK & 8) != 0, PML = PK != 0;
   // column axis whose psi pair is loaded a plane ahead (y when both are
   // present), and z as a second column axis (corner columns, loaded inline)
-  constexpr bool CY = PY, CZ = PZ && !PY, Z2 = PY && PZ;
+  constexpr bool CZ = PZ && !PY, Z2 = PY && PZ;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* base = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
   T* sF = reinterpret_cast<T*>(base);                            // [NS][6][PL]
@@ -944,16 +1054,34 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
     fence_mbar_init();
   }
   __syncthreads();
+  // TFSF line values (LN): the face of the y and z lines the tile meets (the
+  // host gives tiles that meet both faces of an axis the general body)
+  const int fy = TF && LN && tf.on ? tfsf_line_face(tf.js, tf.je, j0, TJ) : -1;
+  const int fz = TF && LN && tf.on ? tfsf_line_face(tf.ks, tf.ke, k0, 32) : -1;
+  unsigned char* sT = base + L::off_t;  // [NS][LSLOT]: y boxes (H, E), z boxes (H, E)
+  const unsigned line_tx = (fy >= 0 ? 2u * 2u * L::YW * 8u : 0u) + (fz >= 0 ? 2u * 2u * L::ZW * 8u : 0u);
   int staged = -1;  // last plane whose copies were issued (thread 0)
   auto stage = [&](int plane, int st) {
     if (tid == 0 && plane <= i_end) {
       staged = plane;
       fence_proxy_async();
-      mbar_expect_tx(bar + st, L::tx_bytes);
+      mbar_expect_tx(bar + st, L::tx_bytes + line_tx);
       T* dst = sF + st * 6 * PL;
 #pragma unroll
       for (int f = 0; f < 6; ++f) tma_load_3d(dst + f * PL, &maps->f[f], k0 - HP, j0 - 1, plane, bar + st);
       tma_load_3d(sM + st * L::MPL, &maps->mid, k0 - 16, j0 - 1, plane, bar + st);
+      if (LN) {
+        // the H-pass lines of this plane, the E-pass lines of the plane before
+        unsigned char* t = sT + st * L::LSLOT;
+        if (fy >= 0) {
+          tma_load_4d(t, &lines->yh, k0 - 2, 0, plane, fy, bar + st);
+          tma_load_4d(t + L::YB, &lines->ye, k0 - 2, 0, plane - 1, fy, bar + st);
+        }
+        if (fz >= 0) {
+          tma_load_4d(t + 2 * L::YB, &lines->zh, j0 - 2, 0, plane, fz, bar + st);
+          tma_load_4d(t + 2 * L::YB + L::ZB, &lines->ze, j0 - 2, 0, plane - 1, fz, bar + st);
+        }
+      }
     }
   };
   for (int q = 0; q < NS - 1; ++q) stage(i_first + q, (i_first + q) % NS);
@@ -1101,6 +1229,12 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
     const T* Fc = sF + slot * 6 * PL;
     const T* Fn = sF + slot_n * 6 * PL;
     const uint8_t* Mc = sM + slot * L::MPL;
+    // staged TFSF lines of this slot: H pass of plane i, E pass of plane i-1
+    const unsigned char* tl = sT + slot * L::LSLOT;
+    const LineVals lvh{reinterpret_cast<const double*>(tl), reinterpret_cast<const double*>(tl + 2 * L::YB), L::YW,
+                       L::ZW, k0 - 2, j0 - 2};
+    const LineVals lve{reinterpret_cast<const double*>(tl + L::YB),
+                       reinterpret_cast<const double*>(tl + 2 * L::YB + L::ZB), L::YW, L::ZW, k0 - 2, j0 - 2};
     slot = slot_n;
     T* Hc = sH + (i & 1) * 3 * CS;              // H plane i (written here)
     const T* Hq = sH + ((i + 1) & 1) * 3 * CS;  // H plane i-1
@@ -1128,7 +1262,10 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
         T hxv = cf.c * f[3 * PL] + cf.z * d_hx_a - cf.y * d_hx_b;
         T hyv = cf.c * f[4 * PL] + cf.x * d_hy_a - cf.z * d_hy_b;
         T hzv = cf.c * f[5 * PL] + cf.y * d_hz_a - cf.x * d_hz_b;
-        if (TF && (tf_hplane || (tfl[u] & 1))) tfsf_h(tf, IncTables{tf}, i, cj[u], ck[u], hxv, hyv, hzv);
+        if (TF && (tf_hplane || (tfl[u] & 1))) {
+          if (LN) tfsf_h_lines(tf, IncTables{tf}, lvh, i, cj[u], ck[u], hxv, hyv, hzv);
+          else tfsf_h(tf, IncTables{tf}, i, cj[u], ck[u], hxv, hyv, hzv);
+        }
         if (PX && sxp >= 0 && in_grid[u]) {
           const long long p = static_cast<long long>(sxp) * s.sx + go[u];
           const T a = pm.ah[0][i], b = pm.bh[0][i];
@@ -1206,7 +1343,10 @@ __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>&
         T exv = cf.c * eox[u] - cf.z * d_ex_a + cf.y * d_ex_b;
         T eyv = cf.c * eoy[u] - cf.x * d_ey_a + cf.z * d_ey_b;
         T ezv = cf.c * eoz[u] - cf.y * d_ez_a + cf.x * d_ez_b;
-        if (TF && (tf_eplane || (tfl[u] & 2))) tfsf_e(tf, IncTables{tf}, ie, cj[u], ck[u], exv, eyv, ezv);
+        if (TF && (tf_eplane || (tfl[u] & 2))) {
+          if (LN) tfsf_e_lines(tf, IncTables{tf}, lve, ie, cj[u], ck[u], exv, eyv, ezv);
+          else tfsf_e(tf, IncTables{tf}, ie, cj[u], ck[u], exv, eyv, ezv);
+        }
         if (PML) {
           const bool jpos = cj[u] > 0, kpos = ck[u] > 0;
           const bool upd_x = jpos && kpos, upd_y = ipos && kpos, upd_z = ipos && jpos;
@@ -1304,23 +1444,29 @@ constexpr int kFastYZ = 18;
 // column whose 32 columns or TJ rows hold both CPML cells and a TFSF face)
 constexpr int kFastYTf = 19, kFastZTf = 20, kFastYZTf = 21;
 
-template <typename T, int R, int NWM, int NS_, bool TMA>
+// LN: the TFSF bodies take the y- and z-line incident values from the line
+// tables (single scenes, which compute them every step); batches compute
+// them from the projections and the auxiliary rows.
+template <typename T, int R, int NWM, int NS_, bool TMA, bool LN = false>
 __device__ __forceinline__ void step_dispatch(const GridP<T>& s, const GridP<T>& d, const PmlP<T>& pm,
                                               const PsiH<T>& ps, const PsiH<T>& pd, const TfsfP& tf,
                                               const AdeP<T>& ad, int4 item, const T* lut8, const uint8_t* disp,
-                                              int n_mat, const StageMaps* maps, const StoreMaps* outs, int* err) {
+                                              int n_mat, const StageMaps* maps, const StoreMaps* outs, int* err,
+                                              const LineMaps* lines = nullptr) {
   if (TMA) {
+#define XFB_FAST(tfc, pk) step_item_fast<T, R, NWM, NS_, tfc, pk, LN>(s, pm, ps, pd, item, lut8, n_mat, tf, maps, outs, lines, err)
     switch (item.x >> 16) {
-      case kLeanInterior: step_item_fast<T, R, NWM, NS_, false, 0>(s, pm, ps, pd, item, lut8, n_mat, tf, maps, outs, err); return;
-      case kLeanInteriorTf: step_item_fast<T, R, NWM, NS_, true, 0>(s, pm, ps, pd, item, lut8, n_mat, tf, maps, outs, err); return;
-      case kFastY: step_item_fast<T, R, NWM, NS_, false, 3>(s, pm, ps, pd, item, lut8, n_mat, tf, maps, outs, err); return;
-      case kFastZ: step_item_fast<T, R, NWM, NS_, false, 9>(s, pm, ps, pd, item, lut8, n_mat, tf, maps, outs, err); return;
-      case kFastYZ: step_item_fast<T, R, NWM, NS_, false, 11>(s, pm, ps, pd, item, lut8, n_mat, tf, maps, outs, err); return;
-      case kFastYTf: step_item_fast<T, R, NWM, NS_, true, 3>(s, pm, ps, pd, item, lut8, n_mat, tf, maps, outs, err); return;
-      case kFastZTf: step_item_fast<T, R, NWM, NS_, true, 9>(s, pm, ps, pd, item, lut8, n_mat, tf, maps, outs, err); return;
-      case kFastYZTf: step_item_fast<T, R, NWM, NS_, true, 11>(s, pm, ps, pd, item, lut8, n_mat, tf, maps, outs, err); return;
+      case kLeanInterior: XFB_FAST(false, 0); return;
+      case kLeanInteriorTf: XFB_FAST(true, 0); return;
+      case kFastY: XFB_FAST(false, 3); return;
+      case kFastZ: XFB_FAST(false, 9); return;
+      case kFastYZ: XFB_FAST(false, 11); return;
+      case kFastYTf: XFB_FAST(true, 3); return;
+      case kFastZTf: XFB_FAST(true, 9); return;
+      case kFastYZTf: XFB_FAST(true, 11); return;
       default: break;
     }
+#undef XFB_FAST
   }
 #define XFB_ITEM(q) step_item<T, R, NWM, NS_, kStepKinds[q], TMA>(s, d, pm, ps, pd, tf, ad, item, lut8, disp, n_mat, maps, err)
   switch (item.x >> 16) {
@@ -1343,17 +1489,18 @@ __device__ __forceinline__ void step_dispatch(const GridP<T>& s, const GridP<T>&
 }
 
 // The single-scene step stages with tiled bulk copies from the tensor maps of
-// its read set (`maps`, a grid constant) and its lean interior items store
-// through the maps of the write set (`outs`); a staging wait that runs out
-// sets *err.
+// its read set (`maps`, a grid constant), together with the TFSF line values
+// of the items on the TFSF surface (`lines`, tables k_tfsf_lines filled for
+// this step); its lean interior and CPML column items store through the maps
+// of the write set (`outs`); a staging wait that runs out sets *err.
 template <typename T, int R, int NWM, int NS_>
 __global__ void __launch_bounds__(StepCfg<T, R, NWM, NS_>::NT, StepCfg<T, R, NWM, NS_>::min_blocks)
     k_step3(GridP<T> s, GridP<T> d, PmlP<T> pm, PsiH<T> ps, PsiH<T> pd, TfsfP tf_in, AdeP<T> ad, TimeP tp,
             const int4* items, const T* lut8, const uint8_t* disp, int n_mat, const __grid_constant__ StageMaps maps,
-            const __grid_constant__ StoreMaps outs, int* err) {
+            const __grid_constant__ StoreMaps outs, const __grid_constant__ LineMaps lines, int* err) {
   const TfsfP tf = tfsf_at_step(tf_in, cur_step(tp));
-  step_dispatch<T, R, NWM, NS_, true>(s, d, pm, ps, pd, tf, ad, items[blockIdx.x], lut8, disp, n_mat, &maps, &outs,
-                                      err);
+  step_dispatch<T, R, NWM, NS_, true, true>(s, d, pm, ps, pd, tf, ad, items[blockIdx.x], lut8, disp, n_mat, &maps,
+                                            &outs, err, &lines);
 }
 
 // Everything the one-sweep step reads of one scene of a batch.  Both field
@@ -1423,6 +1570,20 @@ __device__ __forceinline__ void mbar_inval(uint64_t* b) {
   asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smem_u32(b)) : "memory");
 }
 
+// One work item of the persistent batch step.  Kept out of line: the item
+// bodies get the kernel's whole register budget, and the queue loop around
+// them keeps (almost) nothing live across the call.
+template <typename T, int R, int NWM, int NS_>
+__device__ __noinline__ void persist_item(const BatchScene<T>& sp, const TfsfP& tf, const BatchMaps* maps, int4 it,
+                                          int parity, int tile, int* err) {
+  const int scene = static_cast<int>(static_cast<unsigned>(it.x) >> 16);
+  const int4 item = make_int4((it.x & 0x7ff) | (((it.x >> 11) & 0x1f) << 16), it.y, it.z, it.w);
+  const BatchMaps& bm = maps[scene];
+  step_dispatch<T, R, NWM, NS_, true>(sp.g[parity], sp.g[1 - parity], sp.pm, sp.psh[parity], sp.psh[1 - parity], tf,
+                                      sp.ad, item, sp.lut8, sp.disp, sp.n_mat, &bm.stage[tile][parity],
+                                      &bm.store[tile][1 - parity], err);
+}
+
 // Persistent form of the batch step: n_steps steps of every scene in one
 // launch.  A grid of resident CTAs draws tickets from a device queue
 // (queue[0]); ticket q is item q % n_items of step q / n_items, so all items
@@ -1432,12 +1593,11 @@ __device__ __forceinline__ void mbar_inval(uint64_t* b) {
 // next step's items of that scene wait for the count s * scene_items[scene]
 // (acquire).  That is the whole step-to-step dependency of a scene: the step
 // reads the field set its previous step wrote and writes the set that step
-// read.  Items are listed scene by scene, so a scene's next step can start
-// while later scenes still finish the current one; no CTA ever waits for an
-// item that has not been handed out, so the queue cannot deadlock.  The
-// waits are bounded (err[1] polls, as the staging waits); a wait that runs
-// out, or any earlier error, sets err[0] and every CTA stops at its next
-// ticket.  queue[] is zeroed before each launch.
+// read.  A scene's next step can start while other scenes still finish the
+// current one; no CTA ever waits for an item that has not been handed out,
+// so the queue cannot deadlock.  The waits are bounded (err[1] polls, as the
+// staging waits); a wait that runs out, or any earlier error, sets err[0] and
+// every CTA stops at its next ticket.  queue[] is zeroed before each launch.
 template <typename T, int R, int NWM, int NS_>
 __global__ void __launch_bounds__(StepCfg<T, R, NWM, NS_>::NT, StepCfg<T, R, NWM, NS_>::min_blocks)
     k_step3_persist(const BatchScene<T>* scenes, const BatchMaps* maps, const int4* items, int n_items,
@@ -1446,24 +1606,21 @@ __global__ void __launch_bounds__(StepCfg<T, R, NWM, NS_>::NT, StepCfg<T, R, NWM
   __shared__ BatchScene<T> sp;
   __shared__ TfsfP s_tf;
   __shared__ unsigned s_ticket;
-  __shared__ int s_go;
+  __shared__ int s_go, s_cur;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u) + L::off_b);
-  unsigned* done = queue + 1;
-  const unsigned tickets = static_cast<unsigned>(n_steps) * static_cast<unsigned>(n_items);
-  const long long t0 = cur_step(tp);
-  int cur = -1;  // scene whose parameters sit in sp
+  if (threadIdx.x == 0) s_cur = -1;  // scene whose parameters sit in sp
   for (;;) {
     if (threadIdx.x == 0) {
       const unsigned q = atomicAdd(queue, 1u);
-      int go = q < tickets && *reinterpret_cast<volatile int*>(err) == 0;
+      int go = q < static_cast<unsigned>(n_steps) * static_cast<unsigned>(n_items) &&
+               *reinterpret_cast<volatile int*>(err) == 0;
       if (go && q >= static_cast<unsigned>(n_items)) {
         const unsigned s = q / static_cast<unsigned>(n_items);
         const int scene = static_cast<int>(static_cast<unsigned>(items[q - s * n_items].x) >> 16);
         const unsigned need = s * static_cast<unsigned>(scene_items[scene]);
         const int polls = err[1];
         int n = 0;
-        while (ld_acquire_gpu(done + scene) < need) {
+        while (ld_acquire_gpu(queue + 1 + scene) < need) {
           if (*reinterpret_cast<volatile int*>(err) != 0) { go = 0; break; }
           if (++n > polls) {
             atomicExch(err, 1);
@@ -1479,31 +1636,26 @@ __global__ void __launch_bounds__(StepCfg<T, R, NWM, NS_>::NT, StepCfg<T, R, NWM
     }
     __syncthreads();
     if (!s_go) break;
-    const unsigned q = s_ticket;
-    const unsigned s = q / static_cast<unsigned>(n_items);
-    const int4 it = items[q - s * n_items];
+    const unsigned s = s_ticket / static_cast<unsigned>(n_items);
+    const int4 it = items[s_ticket - s * n_items];
     const int scene = static_cast<int>(static_cast<unsigned>(it.x) >> 16);
-    if (scene != cur) {
+    if (scene != s_cur) {
       const int* src = reinterpret_cast<const int*>(scenes + scene);
       int* dst = reinterpret_cast<int*>(&sp);
       for (int w = threadIdx.x; w < static_cast<int>(sizeof(BatchScene<T>) / 4); w += blockDim.x) dst[w] = src[w];
-      cur = scene;
       __syncthreads();
+      if (threadIdx.x == 0) s_cur = scene;
     }
-    if (threadIdx.x == 0) s_tf = tfsf_at_step(sp.tf, t0 + s);  // incident-table rows of this item's step
+    if (threadIdx.x == 0) s_tf = tfsf_at_step(sp.tf, cur_step(tp) + s);  // incident-table rows of this item's step
     __syncthreads();
-    const int parity = (parity0 + static_cast<int>(s)) & 1;
-    const int4 item = make_int4((it.x & 0x7ff) | (((it.x >> 11) & 0x1f) << 16), it.y, it.z, it.w);
-    const BatchMaps& bm = maps[scene];
-    step_dispatch<T, R, NWM, NS_, true>(sp.g[parity], sp.g[1 - parity], sp.pm, sp.psh[parity], sp.psh[1 - parity],
-                                        s_tf, sp.ad, item, sp.lut8, sp.disp, sp.n_mat, &bm.stage[tile][parity],
-                                        &bm.store[tile][1 - parity], err);
+    persist_item<T, R, NWM, NS_>(sp, s_tf, maps, it, (parity0 + static_cast<int>(s)) & 1, tile, err);
     __threadfence();  // this thread's plain stores of the item, before the count below
     __syncthreads();  // every thread is done with the item and its shared memory
     if (threadIdx.x == 0) {
+      uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u) + L::off_b);
       for (int b = 0; b < NS_; ++b) mbar_inval(bar + b);  // the next item initialises them again
       fence_proxy_async_global();  // the item's bulk stores (completed by this thread), before the count
-      red_release_gpu_add(done + scene, 1u);
+      red_release_gpu_add(queue + 1 + scene, 1u);
     }
   }
 }

@@ -120,6 +120,15 @@ struct xfb_handle {
   CUtensorMap stage_maps[3][2][7];
   CUtensorMap store_maps[3][2][6];
   int* step_err = nullptr;
+  // TFSF line tables of the one-sweep step, filled every step by
+  // k_tfsf_lines (yh, ye: rows of pitch line_ykp; zh, ze: rows of pitch
+  // line_zjp), and their tensor maps per tile configuration.  Off without a
+  // TFSF source and for the scenes of a batch (no_lines), whose step kernels
+  // compute the incident values in place.
+  bool lines_on = false, no_lines = false;
+  void* line_tab[4] = {};
+  long long line_ykp = 0, line_zjp = 0;
+  CUtensorMap line_maps[3][4];
   // ADE applied by k_ade_box after the one-sweep step (no dispersive cell
   // takes a TFSF or CPML correction)
   bool ade_deferred = false;
@@ -172,9 +181,9 @@ struct xfb_batch {
   int n_items[3] = {};
   long long* t_dev = nullptr;
   std::map<int, cudaGraphExec_t> graphs;
-  // persistent launches (XFB_BATCH_PERSISTENT): work lists scene by scene,
-  // items per scene, and the queue (ticket counter, then one finished-item
-  // counter per scene), per tile configuration
+  // persistent launches (XFB_BATCH_PERSISTENT): work lists (the per-step
+  // lists, aliased), items per scene, and the queue (ticket counter, then one
+  // finished-item counter per scene)
   int launch_req = XFB_BATCH_AUTO;  // xfb_batch_set_launch
   int launch = -1;                  // XFB_BATCH_PER_STEP or XFB_BATCH_PERSISTENT (-1 until chosen)
   bool persist_ok = false;          // no scene records monitors or runs a separate ADE pass

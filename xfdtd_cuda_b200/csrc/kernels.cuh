@@ -660,6 +660,67 @@ static __global__ void k_aux_table(double* e_tab, double* h_tab, int nl, double 
 static __global__ void k_bump(long long* t, int n) { *t += n; }
 
 // ---------------------------------------------------------------------------
+// TFSF line tables of one step.  Every cell on a y or z face line of the TFSF
+// surface (the rows js-1, js, je; the columns ks-1, ks, ke) takes its
+// corrections from two incident-field components at a fixed node of the line;
+// the step kernel stages those values per plane with its bulk copies, next to
+// the fields, instead of computing each from the projections and the
+// auxiliary row (two dependent loads per corrected cell).  Tables, all FP64:
+//   yh[f][i][c][k]: H pass, row js-1 (f = 0: values at j = js) or je (f = 1):
+//                   c = 0 ex_inc, c = 1 ez_inc
+//   ye[f][i][c][k]: E pass, row js (f = 0: values at j = js-1) or je:
+//                   c = 0 hx_inc, c = 1 hz_inc
+//   zh[f][i][c][j]: H pass, column ks-1 (f = 0: values at k = ks) or ke:
+//                   c = 0 ey_inc, c = 1 ex_inc
+//   ze[f][i][c][j]: E pass, column ks (f = 0: values at k = ks-1) or ke:
+//                   c = 0 hy_inc, c = 1 hx_inc
+// over i in [is, ie] and k (j) in [ks, ke] ([js, je]), each entry only where
+// a correction reads it (the others stay zero); rows of k pitch ykp, rows of
+// j pitch zjp.  The values are those ex_inc .. hz_inc return, so the
+// corrections are unchanged bit for bit.
+struct LineP {
+  double* yh; double* ye; double* zh; double* ze;
+  long long ykp, zjp;  // row pitch (elements) of the y and z tables
+  long long ysl, zsl;  // elements per plane i (2 components)
+  long long yfs, zfs;  // elements per face
+};
+
+// (instantiated per engine precision, so the FP64 engine's copy is compiled
+// with that engine's no-contraction rule)
+template <typename T>
+__global__ void k_tfsf_lines(TfsfP tf_in, TimeP tp, LineP lp) {
+  const TfsfP tf = tfsf_at_step(tf_in, cur_step(tp));
+  const int ni = tf.ie - tf.is + 1, nk = tf.ke - tf.ks + 1, nj = tf.je - tf.js + 1;
+  const long long ny_work = 2LL * ni * nk, nz_work = 2LL * ni * nj;
+  for (long long w = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; w < ny_work + nz_work;
+       w += static_cast<long long>(gridDim.x) * blockDim.x) {
+    if (w < ny_work) {
+      const int f = static_cast<int>(w / (static_cast<long long>(ni) * nk));
+      const long long r = w - static_cast<long long>(f) * ni * nk;
+      const int i = tf.is + static_cast<int>(r / nk), k = tf.ks + static_cast<int>(r % nk);
+      const long long o = f * lp.yfs + i * lp.ysl + k;
+      const int jh = f ? tf.je : tf.js, je = f ? tf.je : tf.js - 1;
+      // only the entries a correction reads (the others stay zero)
+      if (i < tf.ie) lp.yh[o] = ex_inc(tf, i, jh, k);
+      if (k < tf.ke) lp.yh[o + lp.ykp] = ez_inc(tf, i, jh, k);
+      if (k < tf.ke) lp.ye[o] = hx_inc(tf, i, je, k);
+      if (i < tf.ie) lp.ye[o + lp.ykp] = hz_inc(tf, i, je, k);
+    } else {
+      const long long v = w - ny_work;
+      const int f = static_cast<int>(v / (static_cast<long long>(ni) * nj));
+      const long long r = v - static_cast<long long>(f) * ni * nj;
+      const int i = tf.is + static_cast<int>(r / nj), j = tf.js + static_cast<int>(r % nj);
+      const long long o = f * lp.zfs + i * lp.zsl + j;
+      const int kh = f ? tf.ke : tf.ks, ke = f ? tf.ke : tf.ks - 1;
+      if (j < tf.je) lp.zh[o] = ey_inc(tf, i, j, kh);
+      if (i < tf.ie) lp.zh[o + lp.zjp] = ex_inc(tf, i, j, kh);
+      if (i < tf.ie) lp.ze[o] = hy_inc(tf, i, j, ke);
+      if (j < tf.je) lp.ze[o + lp.zjp] = hx_inc(tf, i, j, ke);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // NF2FF frequency-domain accumulation: one thread per face point, all faces and
 // frequencies in one launch.  The four surface samples of a point (the
 // interpolated tangential H and E with the current signs) are kept for
