@@ -253,7 +253,8 @@ int xfb_set_wait_limit(xfb_handle* h, int polls);
  * synchronize); *ms = elapsed device time of the n steps. */
 int xfb_timed_step(xfb_handle* h, long long n, double* ms);
 
-/* Kernel classes of one time step, for xfb_profile_kernels. */
+/* Kernel classes of one time step, for xfb_profile_kernels (XFB_K_AUX: the
+ * per-step TFSF line values of the one-sweep 3-D step). */
 enum xfb_kernel_class {
   XFB_K_UPDATE_H = 0, XFB_K_AUX = 1, XFB_K_UPDATE_E = 2, XFB_K_NF2FF = 3, XFB_K_PROBE = 4,
   XFB_K_MOVIE = 5, XFB_K_STEP = 6, XFB_K_CORRECT = 7, XFB_K_COUNT = 8

@@ -28,7 +28,7 @@ MAX_POLES = 4
 FAR_FIELD_STATIC_MAX_ANGLES = 4096  # XFB_FAR_FIELD_STATIC_MAX_ANGLES
 BATCH_AUTO, BATCH_PER_STEP, BATCH_PERSISTENT = 0, 1, 2  # xfb_batch_set_launch
 K_UPDATE_H, K_AUX, K_UPDATE_E, K_NF2FF, K_PROBE, K_MOVIE, K_STEP, K_CORRECT, K_COUNT = range(9)
-KERNEL_NAMES = ("k_h3/k_h2 (H half-step)", "k_aux (TFSF aux grid)", "k_e3/k_e2 (E half-step)", "k_nf2ff",
+KERNEL_NAMES = ("k_h3/k_h2 (H half-step)", "k_tfsf_lines (TFSF line values of the step)", "k_e3/k_e2 (E half-step)", "k_nf2ff",
                 "k_probe", "k_movie", "k_step3 (one-sweep H+E step)",
                 "boundary corrections (plain CPML/TFSF launches; k_labc_apply of the learned boundary)")
 PATH_AUTO, PATH_SPLIT, PATH_FUSED, PATH_PLAIN = 0, 1, 2, 3

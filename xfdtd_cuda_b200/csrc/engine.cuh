@@ -1022,6 +1022,11 @@ void enqueue_update(xfb_handle* h, int off, Prof* pf) {
     plain_pml<T, true>(h, g);
     prof_end(h, pf);
   } else if (fused(h)) {
+    if (c.dim == 3 && h->lines_on) {  // the TFSF line values this step's kernel stages
+      prof_begin(h, pf, XFB_K_AUX);
+      launch_lines<T>(h, tp, s);
+      prof_end(h, pf);
+    }
     prof_begin(h, pf, XFB_K_STEP);
     if (c.dim == 2 && h->tb_on) {
       launch_tb2d<T>(h, off, 1);  // a single step (profiling): the blocked kernel with S = 1
@@ -1034,13 +1039,6 @@ void enqueue_update(xfb_handle* h, int off, Prof* pf) {
           grid_params<T>(h, parity), grid_params<T>(h, 1 - parity), pml_params<T>(h), psi_h_set<T>(h, parity),
           psi_h_set<T>(h, 1 - parity), tfsf_params(h), tp, ich, h->c.n_mat);
     } else {
-      if (h->lines_on) {
-        prof_end(h, pf);
-        prof_begin(h, pf, XFB_K_AUX);
-        launch_lines<T>(h, tp, s);
-        prof_end(h, pf);
-        prof_begin(h, pf, XFB_K_STEP);
-      }
       launch_fused<T>(h, parity, tp, s);
     }
     if (h->ade_deferred) launch_ade<T>(h, parity, s);
