@@ -1182,9 +1182,7 @@ int xfb_batch_init(xfb_batch* b, long long total_steps) {
     h->batch = nullptr;  // xfb_init is refused for batched handles
     if (h->device < 0) cudaSetDevice(dev);  // xfb_init adopts the current device
     h->path = XFB_PATH_FUSED;
-    h->no_lines = true;  // the batch kernels compute the TFSF incident values in place
     int rc = xfb_init(h, total_steps);
-    h->no_lines = false;
     h->batch = b;
     if (rc) return batch_err(b, rc, "scene init failed: " + h->err);
     b->cells += static_cast<long long>(h->c.nx) * h->c.ny * h->c.nz;

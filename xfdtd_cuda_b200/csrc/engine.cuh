@@ -121,7 +121,7 @@ int init_device(xfb_handle* h) {
     if ((rc = upload<T>(h, &h->lut, round_coefficients(c.coeff, h->coeff_storage)))) return rc;
     if ((rc = upload<T>(h, &h->lut8, round_coefficients(c.coeff8, h->coeff_storage)))) return rc;
   }
-  h->lines_on = fused(h) && c.dim == 3 && c.tfsf_on && !h->no_lines;
+  h->lines_on = fused(h) && c.dim == 3 && c.tfsf_on;
   if (h->lines_on) {  // TFSF line tables: [face][plane][component][k or j]
     h->line_ykp = h->nzp;
     h->line_zjp = roundup(c.ny, 2);
@@ -1378,6 +1378,7 @@ BatchScene<T> batch_scene(xfb_handle* h) {
   b.lut8 = as<const T>(h->lut8);
   b.disp = h->mat_disp;
   b.n_mat = h->c.n_mat;
+  if (h->lines_on) b.lines = line_params(h);
   return b;
 }
 
@@ -1409,8 +1410,17 @@ int batch_init(xfb_batch* b) {
         mp[q].stage[t][set].mid = h->stage_maps[t][set][6];
         std::memcpy(mp[q].store[t][set].f, h->store_maps[t][set], sizeof(mp[q].store[t][set].f));
       }
+    for (int t = 0; t < kStepTileCount; ++t)
+      if (h->lines_on) std::memcpy(&mp[q].line[t], h->line_maps[t], sizeof(mp[q].line[t]));
   }
   int rc;
+  b->lines_work = 0;  // largest line-table work of a scene (k_tfsf_lines_batch)
+  for (xfb_handle* h : b->hs)
+    if (h->lines_on) {
+      const Compiled& c = h->c;
+      const long long ni = c.tf[1] - c.tf[0] + 1, nj = c.tf[3] - c.tf[2] + 1, nk = c.tf[5] - c.tf[4] + 1;
+      b->lines_work = std::max(b->lines_work, 2 * ni * (nj + nk));
+    }
   if ((rc = batch_upload(b, &b->scenes, sc.data(), sc.size() * sizeof(BatchScene<T>)))) return rc;
   if ((rc = batch_upload(b, &b->maps, mp.data(), mp.size() * sizeof(BatchMaps)))) return rc;
   {  // error word pair: flag, poll limit of the staging waits
@@ -1426,7 +1436,7 @@ int batch_init(xfb_batch* b) {
     for (size_t q = 0; q < b->hs.size(); ++q) {
       const xfb_handle* h = b->hs[q];
       std::vector<int4> items[kStepKindCount];
-      build_step_items(h->c, TJ, NT, h->ade_deferred, items, whole ? h->c.nx : 0, true);
+      build_step_items(h->c, TJ, NT, h->ade_deferred, items, whole ? h->c.nx : 0, true, 0, -1, h->lines_on);
       for (int k = 0; k < kStepKindCount; ++k)
         for (int4 v : items[k]) per_kind[k].push_back(make_int4(v.x | (k << 11) | (static_cast<int>(q) << 16), v.y, v.z, v.w));
     }
@@ -1516,6 +1526,11 @@ template <typename T>
 void batch_enqueue_step(xfb_batch* b, int off, int t) {
   TimeP tp{b->t_dev, off};
   const int parity = static_cast<int>((b->step + off) & 1);
+  if (b->lines_work > 0) {  // the TFSF line values of every scene for this step
+    const int bx = static_cast<int>(std::min<long long>((b->lines_work + 255) / 256, 64));
+    k_tfsf_lines_batch<T><<<dim3(bx, static_cast<unsigned>(b->hs.size())), 256, 0, b->stream>>>(
+        static_cast<const BatchScene<T>*>(b->scenes), tp);
+  }
   if (b->n_items[t]) {
     if (t == 0) batch_step3<T, kStepTiles[0].r, kStepTiles[0].nwm>(b, 0, tp, parity);
     else if (t == 1) batch_step3<T, kStepTiles[1].r, kStepTiles[1].nwm>(b, 1, tp, parity);
@@ -1649,6 +1664,8 @@ int batch_run(xfb_batch* b, long long n) {
     std::vector<int> tiles;
     for (int t = 0; t < kStepTileCount; ++t)
       if (b->tile_req == 0 || kStepTileRows[t] == b->tile_req) tiles.push_back(t);
+    // too few steps to time every (tile, form): the tiles alone in the first form
+    if (forms.size() > 1 && n < 2 * static_cast<long long>(tiles.size() * forms.size())) forms.resize(1);
     const long long cands = static_cast<long long>(tiles.size() * forms.size());
     if (cands == 1 || n < 2 * cands) {  // nothing to choose, or too few steps to time: 16-row tiles, first form
       b->tile = tiles.size() == 1 ? tiles[0] : 1;

@@ -1516,21 +1516,35 @@ struct BatchScene {
   const uint8_t* disp;
   int n_mat;
   int pad;
+  LineP lines;  // TFSF line tables (per-step form)
 };
 
 // Tensor maps of one scene of a batch, in global memory: staging maps per tile
 // configuration and read set, bulk-store maps per tile configuration and
-// write set.
+// write set, TFSF line maps per tile configuration.
 struct BatchMaps {
   StageMaps stage[3][2];
   StoreMaps store[3][2];
+  LineMaps line[3];
 };
+
+// The TFSF line tables of one step of every scene of a batch (blockIdx.y:
+// the scene), ahead of the batch's step kernel.
+template <typename T>
+__global__ void k_tfsf_lines_batch(const BatchScene<T>* scenes, TimeP tp) {
+  const BatchScene<T>& sc = scenes[blockIdx.y];
+  if (!sc.tf.on) return;
+  tfsf_lines_fill(tfsf_at_step(sc.tf, cur_step(tp)), sc.lines,
+                  blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x,
+                  static_cast<long long>(gridDim.x) * blockDim.x);
+}
 
 // The one-sweep step of a batch of scenes in one launch: one CTA per work
 // item (x: k tile | kind << 11 | scene << 16, y: j tile, z/w: plane range).
 // The CTA copies its scene's parameters into shared memory and runs the same
 // region-specialised bodies as k_step3 (bulk copies through the scene's
-// tensor maps in `maps`, tile configuration `tile`); a staging wait that runs
+// tensor maps in `maps`, tile configuration `tile`, TFSF line values from the
+// tables k_tfsf_lines_batch filled for this step); a staging wait that runs
 // out sets *err.
 template <typename T, int R, int NWM, int NS_>
 __global__ void __launch_bounds__(StepCfg<T, R, NWM, NS_>::NT, StepCfg<T, R, NWM, NS_>::min_blocks)
@@ -1549,9 +1563,9 @@ __global__ void __launch_bounds__(StepCfg<T, R, NWM, NS_>::NT, StepCfg<T, R, NWM
   __syncthreads();
   const int4 item = make_int4((it.x & 0x7ff) | (((it.x >> 11) & 0x1f) << 16), it.y, it.z, it.w);
   const BatchMaps& bm = maps[scene];
-  step_dispatch<T, R, NWM, NS_, true>(sp.g[parity], sp.g[1 - parity], sp.pm, sp.psh[parity], sp.psh[1 - parity],
-                                      sp.tf, sp.ad, item, sp.lut8, sp.disp, sp.n_mat, &bm.stage[tile][parity],
-                                      &bm.store[tile][1 - parity], err);
+  step_dispatch<T, R, NWM, NS_, true, true>(sp.g[parity], sp.g[1 - parity], sp.pm, sp.psh[parity],
+                                            sp.psh[1 - parity], sp.tf, sp.ad, item, sp.lut8, sp.disp, sp.n_mat,
+                                            &bm.stage[tile][parity], &bm.store[tile][1 - parity], err, &bm.line[tile]);
 }
 
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {

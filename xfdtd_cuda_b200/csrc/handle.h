@@ -121,11 +121,10 @@ struct xfb_handle {
   CUtensorMap store_maps[3][2][6];
   int* step_err = nullptr;
   // TFSF line tables of the one-sweep step, filled every step by
-  // k_tfsf_lines (yh, ye: rows of pitch line_ykp; zh, ze: rows of pitch
-  // line_zjp), and their tensor maps per tile configuration.  Off without a
-  // TFSF source and for the scenes of a batch (no_lines), whose step kernels
-  // compute the incident values in place.
-  bool lines_on = false, no_lines = false;
+  // k_tfsf_lines (or, in a batch, k_tfsf_lines_batch; yh, ye: rows of pitch
+  // line_ykp; zh, ze: rows of pitch line_zjp), and their tensor maps per tile
+  // configuration.  Off without a TFSF source.
+  bool lines_on = false;
   void* line_tab[4] = {};
   long long line_ykp = 0, line_zjp = 0;
   CUtensorMap line_maps[3][4];
@@ -190,6 +189,7 @@ struct xfb_batch {
   void* pitems[3] = {};
   void* pscene_items[3] = {};
   unsigned* queue = nullptr;
+  long long lines_work = 0;  // TFSF line entries of the largest scene (0: no scene has a TFSF source)
 };
 
 namespace xfb {

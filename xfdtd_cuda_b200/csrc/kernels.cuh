@@ -685,15 +685,12 @@ struct LineP {
   long long yfs, zfs;  // elements per face
 };
 
-// (instantiated per engine precision, so the FP64 engine's copy is compiled
-// with that engine's no-contraction rule)
-template <typename T>
-__global__ void k_tfsf_lines(TfsfP tf_in, TimeP tp, LineP lp) {
-  const TfsfP tf = tfsf_at_step(tf_in, cur_step(tp));
+// Entries w0, w0 + stride, ... of the line tables of the step whose rows tf
+// holds (the y tables first, then the z tables).
+__device__ __forceinline__ void tfsf_lines_fill(const TfsfP& tf, const LineP& lp, long long w0, long long stride) {
   const int ni = tf.ie - tf.is + 1, nk = tf.ke - tf.ks + 1, nj = tf.je - tf.js + 1;
   const long long ny_work = 2LL * ni * nk, nz_work = 2LL * ni * nj;
-  for (long long w = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; w < ny_work + nz_work;
-       w += static_cast<long long>(gridDim.x) * blockDim.x) {
+  for (long long w = w0; w < ny_work + nz_work; w += stride) {
     if (w < ny_work) {
       const int f = static_cast<int>(w / (static_cast<long long>(ni) * nk));
       const long long r = w - static_cast<long long>(f) * ni * nk;
@@ -718,6 +715,14 @@ __global__ void k_tfsf_lines(TfsfP tf_in, TimeP tp, LineP lp) {
       if (j < tf.je) lp.ze[o + lp.zjp] = hx_inc(tf, i, j, ke);
     }
   }
+}
+
+// (kernels instantiated per engine precision, so the FP64 engine's copies are
+// compiled with that engine's no-contraction rule)
+template <typename T>
+__global__ void k_tfsf_lines(TfsfP tf_in, TimeP tp, LineP lp) {
+  tfsf_lines_fill(tfsf_at_step(tf_in, cur_step(tp)), lp, blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x,
+                  static_cast<long long>(gridDim.x) * blockDim.x);
 }
 
 // ---------------------------------------------------------------------------
