@@ -239,7 +239,7 @@ def run_reference(args, rank, world):
 
 
 def plain_compare(local: int, steps: int, warmup: int):
-    """Mcell-updates/s of the C1 workload (dielectric sphere 140^3 + 8-cell CPML
+    """Mcell-updates/s of the dielectric-sphere workload (dielectric sphere 140^3 + 8-cell CPML
     = 156^3, TFSF, NF2FF at 1 GHz) in the FP64 plain form (the reference's
     kernel structure: per-cell coefficient arrays, one launch per component,
     separate CPML/TFSF corrector launches) next to the FP32 and FP64 fused
@@ -267,7 +267,7 @@ def plain_compare(local: int, steps: int, warmup: int):
 
 
 def batched_compare(local: int, steps: int, warmup: int, solo_steps: int = 8):
-    """C4: 64 seeded 3-D scenes (64^3..256^3 inner cells + 8-cell CPML, random
+    """The batched sweep: 64 seeded 3-D scenes (64^3..256^3 inner cells + 8-cell CPML, random
     sphere/cube scatterer, TFSF Gaussian, FP32) stepped as one batch (tile
     rows and launch form -- one launch of the one-sweep kernel per step, or
     one persistent launch per chunk of steps -- autotuned on the warm-up
@@ -314,7 +314,7 @@ def batched_compare(local: int, steps: int, warmup: int, solo_steps: int = 8):
 
 
 def cylinder2d_compare(local: int, steps: int = 4000):
-    """C2: 2-D TMz PEC cylinder (r = 50 cells) in 1024^2 cells + 10-cell CPML
+    """The 2-D cylinder: TMz PEC cylinder (r = 50 cells) in 1024^2 cells + 10-cell CPML
     (1044^2), TFSF Gaussian, 4000 steps, in FP32 and FP64 on the temporally
     blocked kernel (9 steps per launch), and FP32 with one launch per step;
     device-timed Mcell-updates/s of each and the relative L2 error of the
@@ -346,7 +346,7 @@ def cylinder2d_compare(local: int, steps: int = 4000):
 
 
 def learned_abc_compare(local: int, steps: int, warmup: int, side: int = 768):
-    """C5: a side^3 FP32 scattering domain whose walls use the learned
+    """The learned boundary: a side^3 FP32 scattering domain whose walls use the learned
     absorbing boundary (shipped weights) against the same interior wrapped in
     a 12-cell CPML ((side+24)^3) and in a 3-cell CPML ((side+6)^3, the depth
     of the learned stencil), device-timed, with k_labc_apply's share of the
@@ -544,7 +544,7 @@ def main():
                         "dielectric_sphere_156cube_2400_steps": A.fp32_vs_fp64("dielectric", 2400, local),
                         "dispersive_sphere_408cube_6000_steps": A.fp32_vs_fp64("dispersive", 6000, local),
                         "coefficient_storage_trial": {
-                            "what": "C1 (156^3, 2400 steps) with the FP32 engine's coefficient LUT rounded to 16 bits",
+                            "what": "dielectric sphere (156^3, 2400 steps) with the FP32 engine's coefficient LUT rounded to 16 bits",
                             "fp16": A.fp32_vs_fp64("dielectric", 2400, local, fields=False, coeff_storage=1),
                             "bf16": A.fp32_vs_fp64("dielectric", 2400, local, fields=False, coeff_storage=2)}}
         except Exception as exc:

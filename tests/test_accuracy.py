@@ -1,11 +1,12 @@
 """FP32 accuracy at the full-size workloads, and the FP64 engine against the
 CPU restatement at full size.
 
-The north-star bar is a relative L2 error of at most 1e-4 on the far-field
-and probe outputs of the FP32 engine against the FP64 oracle.  At full size
-(C1: 156^3 x 2400 steps; C3: 408^3 x 6000 steps) the FP64 reference run is
+The FP32 engine's accuracy bar is a relative L2 error of at most 1e-4 on the
+far-field and probe outputs against the FP64 oracle.  At full size (the
+dielectric sphere, 156^3 x 2400 steps; the dispersive sphere, 408^3 x 6000
+steps) the FP64 reference run is
 the FP64 engine, which is bit-identical to the CPU restatement: the last test
-shows that on the whole C1 run (about two minutes of CPU on the host).
+shows that on the whole dielectric-sphere run (about two minutes of CPU on the host).
 """
 import numpy as np
 import pytest
@@ -15,7 +16,7 @@ from xfdtd_cuda_b200 import accuracy
 
 pytestmark = pytest.mark.gpu
 
-BAR = 1e-4  # relative L2, far field and probes (north-star bar)
+BAR = 1e-4  # relative L2, far field and probes
 
 
 def test_fp32_dielectric_sphere_full_size():
@@ -55,7 +56,7 @@ def test_fp64_dielectric_sphere_full_size_bit_identical_to_oracle():
 
 
 def test_coefficient_storage_trial_reports_its_error():
-    # 16-bit storage of the coefficient LUT (the north star's trial): the
+    # 16-bit storage of the coefficient LUT (FP16 / BF16 trial): the
     # rounding changes every coefficient by up to 2^-11 (FP16) / 2^-8 (BF16)
     # relative, far above FP32's; measured here, not assumed
     nat = accuracy.fp32_vs_fp64("dielectric", 600, cells=60, fields=False)

@@ -355,7 +355,7 @@ def test_plain_path_rejects_dispersive_and_2d():
 
 
 def test_fp32_2d_cylinder_against_fp64():
-    # C2 at reduced size: the FP32 engine against the FP64 engine (which is
+    # the 2-D cylinder at reduced size: the FP32 engine against the FP64 engine (which is
     # bit-identical to the CPU restatement) on all probe series
     n = 900
     series = {}

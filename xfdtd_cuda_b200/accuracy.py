@@ -45,8 +45,8 @@ def seeded_probes(half_side: float, n: int = 8, seed: int = 3):
 
 
 def scene(name: str, precision: str, cells: int | None = None):
-    """The C1 (dielectric sphere 140^3 + 8-cell CPML, 1 GHz) or C3 (dispersive
-    sphere 384^3 + 12-cell CPML, 1/3/5 GHz) workload with seeded probes."""
+    """The dielectric sphere (140^3 + 8-cell CPML, 1 GHz) or the dispersive
+    sphere (384^3 + 12-cell CPML, 1/3/5 GHz) workload with seeded probes."""
     if name == "dielectric":
         c = cells or 140
         return configs.dielectric_sphere(cells=c, precision=precision, probes=seeded_probes(c * 2.5e-3 / 2))

@@ -96,7 +96,7 @@ def dispersive_sphere(cells: int = 384, dl: float = 1e-3, pml: int = 12, precisi
 
 def batched_sweep(n: int = 64, seed: int = 4, lo: int = 64, hi: int = 256, pml: int = 8, dl: float = 1e-3,
                   precision: str = "fp32"):
-    """C4: `n` 3-D scenes with inner sides drawn uniformly from [lo, hi] cells
+    """Batched sweep: `n` 3-D scenes with inner sides drawn uniformly from [lo, hi] cells
     (seeded), each holding one random sphere or cube scatterer (eps_r in
     [1, 10], sigma in [0, 0.1] S/m) inside an 8-cell CPML, lit by a TFSF
     Gaussian pulse.  Returns the list of Simulation objects."""
