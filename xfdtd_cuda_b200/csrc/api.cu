@@ -131,7 +131,9 @@ int launches_per_step(const xfb_handle* h) {
   }
   int bulk = 2;
   if (fused(h)) {
-    bulk = c.dim == 2 ? 1 : (h->n_step_items[step_tile_index(h->tj)] > 0 ? 1 : 0) + (h->ade_deferred ? 1 : 0);
+    bulk = c.dim == 2 ? 1
+                      : (h->n_step_items[step_tile_index(h->tj)] > 0 ? 1 : 0) + (h->ade_deferred ? 1 : 0) +
+                            (h->lines_on ? 1 : 0);  // k_tfsf_lines
   }
   if (h->tb_on) return 1;  // one blocked launch per tb_steps steps, probes recorded inside
   return bulk + (c.nf_on ? 1 : 0) + (c.td_on ? 2 : 0) + (c.probes.empty() ? 0 : 1) +
