@@ -8,6 +8,11 @@ mie_sphere.npz   analytic bistatic radar cross-section sigma / lambda^2 of a
                  H-plane (S1) against the scattering angle: an independent
                  anchor for the whole engine path (scene compilation, TFSF,
                  Yee/CPML update, NF2FF accumulation, far field).
+mie_dispersive.npz the same cross-section for the dispersive sphere of the
+                 benchmark workload (radius 0.1 m; eps_inf = 1, a Drude pole
+                 and a Lorentz pole) at 1, 3 and 5 GHz, with the complex
+                 permittivity of the material model: an anchor for the ADE
+                 path and the multi-frequency NF2FF.
 oracle_small.npz probe series and field checksums of the CPU restatement on a
                  small FP64 dielectric sphere: pins the oracle against drift.
 """
@@ -69,6 +74,26 @@ def make_mie():
              radius=A, eps_r=EPS, mu_r=MU, freq=FREQ)
 
 
+def make_mie_dispersive():
+    sys.path.insert(0, str(ROOT))
+    from xfdtd_cuda_b200 import configs
+    mat = configs.dispersive_material()
+    radius, freqs = 0.1, (1e9, 3e9, 5e9)
+    theta = np.linspace(0.0, np.pi, 37)
+    se, sh = [], []
+    for f in freqs:
+        k = 2 * np.pi * f / C0
+        # the model's permittivity is in the exp(+j w t) convention; the
+        # series (Bohren & Huffman) uses exp(-i w t): the conjugate
+        m = np.sqrt(np.conj(complex(mat.relativePermittivity(f))))
+        s1, s2 = mie_s1_s2(k * radius, m, 1.0, theta)
+        norm = 4 * np.pi / k ** 2 / (2 * np.pi / k) ** 2
+        se.append(norm * np.abs(s2) ** 2)
+        sh.append(norm * np.abs(s1) ** 2)
+    np.savez(OUT / "mie_dispersive.npz", theta=theta, sigma_e=np.array(se), sigma_h=np.array(sh), radius=radius,
+             freqs=np.array(freqs))
+
+
 def make_oracle_small():
     sys.path.insert(0, str(ROOT))
     sys.path.insert(0, str(ROOT / "oracle"))
@@ -90,5 +115,6 @@ def make_oracle_small():
 
 if __name__ == "__main__":
     make_mie()
+    make_mie_dispersive()
     make_oracle_small()
     print("wrote", sorted(p.name for p in OUT.glob("*.npz")))
