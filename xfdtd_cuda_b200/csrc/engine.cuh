@@ -123,8 +123,9 @@ int init_device(xfb_handle* h) {
   }
   h->lines_on = fused(h) && c.dim == 3 && c.tfsf_on;
   if (h->lines_on) {  // TFSF line tables: [face][plane][component][k or j]
-    h->line_ykp = h->nzp;
-    h->line_zjp = roundup(c.ny, 2);
+    // (rows at least as long as the widest box: 34 k values, TJ + 2 <= 18 j values)
+    h->line_ykp = std::max<long long>(h->nzp, 64);
+    h->line_zjp = std::max<long long>(roundup(c.ny, 2), 32);
     const size_t ny_el = 2ull * (c.nx + 1) * 2 * h->line_ykp, nz_el = 2ull * (c.nx + 1) * 2 * h->line_zjp;
     for (int q = 0; q < 4; ++q)
       if ((rc = alloc(h, &h->line_tab[q], (q < 2 ? ny_el : nz_el) * sizeof(double), false))) return rc;
