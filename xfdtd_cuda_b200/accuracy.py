@@ -12,7 +12,8 @@ run against the FP64 run:
   360 angles from -pi to pi, per NF2FF frequency, as the reference's sphere
   tests request them (test/dielectric_sphere_scatter.cu:85-91,
   test/dispersive_sphere_scatter/dispersive_sphere_scatter.cuh:113-124);
-* final fields: each of the six components after the last step.
+* final fields: each of the six components after the last step, relative
+  and (largest difference, largest value) absolute.
 """
 from __future__ import annotations
 
@@ -92,6 +93,13 @@ def fp32_vs_fp64(name: str, steps: int, device: int = 0, cells: int | None = Non
         "far_field": {f"{k[1]}@f{k[0]}": rel_l2(r32["far"][k], r64["far"][k]) for k in r64["far"]},
     }
     if fields:
-        res["fields"] = {"exeyezhxhyhz"[2 * q:2 * q + 2]: rel_l2(r32["fields"][q], r64["fields"][q]) for q in range(6)}
+        names = ["exeyezhxhyhz"[2 * q:2 * q + 2] for q in range(6)]
+        res["fields"] = {names[q]: rel_l2(r32["fields"][q], r64["fields"][q]) for q in range(6)}
+        # the same differences on an absolute scale: largest |FP32 - FP64| and
+        # largest |FP64| of each final component (the incident pulse has
+        # amplitude 1 in E, 1 / 377 in H)
+        res["fields_max_abs_error"] = {names[q]: float(np.abs(r32["fields"][q].astype(np.float64) - r64["fields"][q]).max())
+                                       for q in range(6)}
+        res["fields_max_abs"] = {names[q]: float(np.abs(r64["fields"][q]).max()) for q in range(6)}
     res["far_field_worst"] = max(res["far_field"].values()) if res["far_field"] else None
     return res
