@@ -1001,7 +1001,10 @@ __device__ __forceinline__ void step_item(const GridP<T>& s, const GridP<T>& d, 
 // coefficients are computed once per item; the psi pair of the slab axis of
 // each cell (H of the next plane, E of the current one) is loaded a plane
 // ahead; x-slab psi (planes near the x faces) inline.  TF: with the TFSF
-// corrections of the cells on the TFSF surface.
+// corrections of the cells on the TFSF surface; LN: the incident values of
+// the tile's y and z face lines arrive with each staged plane (one bulk copy
+// per line window and pass from the tables of k_tfsf_lines, on the plane's
+// barrier), the x-face planes compute theirs in place.
 template <typename T, int R, int NWM, int NS_, bool TF, int PK, bool LN>
 __device__ __forceinline__ void step_item_fast(const GridP<T>& s, const PmlP<T>& pm, const PsiH<T>& ps,
                                                const PsiH<T>& pd, int4 item, const T* lut8, int n_mat,
