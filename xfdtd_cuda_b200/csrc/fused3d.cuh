@@ -100,7 +100,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity, int poll
   return false;
 }
 // Tiled bulk copy of one box of a 3-D tensor into shared memory, completing
-// on barrier `bar` (no multicast).
+// on barrier `bar`, into this CTA's shared memory only.
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
   asm volatile(
       "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
