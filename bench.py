@@ -490,9 +490,8 @@ def main():
         hd.kernel_path = path
         hd.setGridDim((1, 1, 1))
         hd.setBlockDim((32, args.tile_rows, 1))
-        hd.init(args.steps)  # host scene compile, host result arrays, device state and uploads
+        hd.init(args.steps)  # host scene compile, host result arrays (faulted in by host threads), device state
         t1 = time.perf_counter()
-        hd.prefaultHostResults()  # host threads fault in the result arrays while the device steps
         hd.handle.step(args.steps)
         hd.handle.sync()
         t2 = time.perf_counter()
@@ -506,9 +505,9 @@ def main():
                "h2d_bytes_per_step": gi2.h2d_bytes / args.steps, "d2h_bytes_per_step": gi2.d2h_bytes / args.steps,
                "seconds": {**parts, "wall": t3 - t0},
                "path": "SimulationHD(sim).run(n) flow: init (host compile, host result arrays, device state and "
-                       "uploads) + n steps (host threads fault in the result arrays meanwhile) + copyDeviceToHost "
-                       "(six fields as float64 into sim.emf, NF2FF currents), wall clock; bytes counted by the "
-                       "library"}
+                       "uploads) + n steps (host threads fault in the result arrays during init and steps) + "
+                       "copyDeviceToHost (six fields as float64 into sim.emf, NF2FF currents), wall clock; bytes "
+                       "counted by the library"}
         hd.releaseDevice()
         sim.emf = None
 

@@ -32,7 +32,7 @@ def nvcc() -> str:
 
 # (source, fmad) pairs
 UNITS = [("api.cu", False), ("engine_f64.cu", False), ("engine_f32.cu", True), ("labc_train.cu", True),
-         ("scene_compile.cpp", False), ("core_ingest.cpp", False)]
+         ("scene_compile.cpp", False), ("core_ingest.cpp", False), ("host_copy.cpp", False)]
 
 
 def sources() -> list[Path]:

@@ -49,9 +49,12 @@ int cuda_err(xfb_handle* h, cudaError_t e, const char* what) {
 void free_device(xfb_handle* h) {
   for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
   h->graphs.clear();
-  for (auto& b : h->bufs) cudaFree(b.p);
+  for (auto& b : h->bufs)
+    if (b.owner) cudaFree(b.p);
   h->bufs.clear();
   h->bytes = 0;
+  h->arena = nullptr;
+  h->arena_left = 0;
   h->movie_out.clear();
   h->movie_frames.clear();
   h->labc_on = false;
@@ -70,20 +73,68 @@ void free_device(xfb_handle* h) {
   h->inited = false;
 }
 
-int alloc(xfb_handle* h, void** out, size_t bytes, bool state) {
-  *out = nullptr;
-  if (bytes == 0) return XFB_OK;
+namespace {
+constexpr size_t kArenaMax = 32u << 20;     // larger buffers get their own cudaMalloc
+constexpr size_t kArenaChunk = 256u << 20;  // chunk the smaller ones are carved from
+constexpr size_t kAlign = 256;
+
+// One cudaMalloc of `bytes`, listed as an owner buffer (freed with the device
+// state; not part of the checkpoint state, whose parts are listed separately).
+int device_malloc(xfb_handle* h, void** out, size_t bytes) {
   void* p = nullptr;
-  cudaError_t e = cudaMalloc(&p, bytes);
+  const cudaError_t e = cudaMalloc(&p, bytes);
   if (e != cudaSuccess) {
     cudaGetLastError();
     return set_err(h, XFB_ERR_OOM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
   }
-  e = cudaMemsetAsync(p, 0, bytes, h->stream);
-  if (e != cudaSuccess) { cudaFree(p); return cuda_err(h, e, "cudaMemsetAsync"); }
-  h->bufs.push_back({p, bytes, state});
+  h->bufs.push_back({p, 0, false, true});
   h->bytes += bytes;
   *out = p;
+  return XFB_OK;
+}
+}  // namespace
+
+// A zeroed device buffer of `bytes`, listed (with `state`) for the checkpoint.
+// Buffers up to kArenaMax come out of the handle's current chunk.  While host
+// threads fault in large result arrays (xfb_host_prefault), every cudaMalloc
+// waits on the process's memory map, so init keeps their number small.
+int alloc(xfb_handle* h, void** out, size_t bytes, bool state) {
+  *out = nullptr;
+  if (bytes == 0) return XFB_OK;
+  void* p = nullptr;
+  if (bytes <= kArenaMax) {
+    const size_t need = (bytes + kAlign - 1) / kAlign * kAlign;
+    if (h->arena_left < need) {
+      void* chunk;
+      if (int rc = device_malloc(h, &chunk, kArenaChunk)) return rc;
+      h->arena = static_cast<char*>(chunk);
+      h->arena_left = kArenaChunk;
+    }
+    p = h->arena;
+    h->arena += need;
+    h->arena_left -= need;
+  } else if (int rc = device_malloc(h, &p, bytes)) {
+    return rc;
+  }
+  const cudaError_t e = cudaMemsetAsync(p, 0, bytes, h->stream);
+  if (e != cudaSuccess) return cuda_err(h, e, "cudaMemsetAsync");
+  h->bufs.push_back({p, bytes, state, false});
+  *out = p;
+  return XFB_OK;
+}
+
+int alloc_block(xfb_handle* h, void** out, int n, size_t bytes, bool state) {
+  for (int q = 0; q < n; ++q) out[q] = nullptr;
+  if (n <= 0 || bytes == 0) return XFB_OK;
+  const size_t each = (bytes + kAlign - 1) / kAlign * kAlign;
+  void* base;
+  if (int rc = device_malloc(h, &base, each * n)) return rc;
+  const cudaError_t e = cudaMemsetAsync(base, 0, each * n, h->stream);
+  if (e != cudaSuccess) return cuda_err(h, e, "cudaMemsetAsync");
+  for (int q = 0; q < n; ++q) {
+    out[q] = static_cast<char*>(base) + q * each;
+    h->bufs.push_back({out[q], bytes, state, false});
+  }
   return XFB_OK;
 }
 

@@ -75,6 +75,23 @@ inline std::vector<double> round_coefficients(const std::vector<double>& v, int 
   return out;
 }
 
+// Material ids, dense [nx][ny][nz] -> padded (plane stride sx, row stride
+// sy); a warp per (i, j) row.  (A template, like every kernel of this
+// header, so that each engine unit keeps its own instance.)
+template <typename U>
+__global__ void k_spread_ids(const U* __restrict__ src, U* __restrict__ dst, int ny, int nz, long long sx,
+                             long long sy, long long rows) {
+  const int lane = threadIdx.x & 31;
+  const long long w0 = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const long long nw = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
+  for (long long r = w0; r < rows; r += nw) {
+    const long long i = r / ny, j = r - i * ny;
+    const U* s = src + r * nz;
+    U* d = dst + i * sx + j * sy;
+    for (int k = lane; k < nz; k += 32) d[k] = s[k];
+  }
+}
+
 template <typename T>
 int init_device(xfb_handle* h) {
   Compiled& c = h->c;
@@ -92,27 +109,42 @@ int init_device(xfb_handle* h) {
   h->guard = roundup(h->sx + 40 * h->sy + 256, 64);
   const size_t fbytes = (h->elems + 2 * h->guard) * sizeof(T);
   int rc;
-  for (int q = 0; q < 6; ++q) {
-    if (c.dim == 2 && !(q == XFB_EZ || q == XFB_HX || q == XFB_HY)) continue;
-    void* p;
-    if ((rc = alloc(h, &p, fbytes, true))) return rc;
-    h->f[q] = as<T>(p) + h->guard;
-    if (fused(h)) {
-      if ((rc = alloc(h, &p, fbytes, true))) return rc;
-      h->f1[q] = as<T>(p) + h->guard;
+  {  // every component of both field sets in one block, in checkpoint order
+    int comps[6], nc = 0;
+    for (int q = 0; q < 6; ++q)
+      if (c.dim == 3 || q == XFB_EZ || q == XFB_HX || q == XFB_HY) comps[nc++] = q;
+    const int per = fused(h) ? 2 : 1;
+    void* ps[12];
+    if ((rc = alloc_block(h, ps, nc * per, fbytes, true))) return rc;
+    for (int u = 0; u < nc; ++u) {
+      h->f[comps[u]] = as<T>(ps[u * per]) + h->guard;
+      if (fused(h)) h->f1[comps[u]] = as<T>(ps[u * per + 1]) + h->guard;
     }
   }
-  // material ids in the padded layout
+  // material ids in the padded layout: the dense array is copied as it is and
+  // spread into the (zeroed) padded one on the device
   {
-    std::vector<uint8_t> m(static_cast<size_t>(h->elems), 0);
-#pragma omp parallel for schedule(static)
-    for (int i = 0; i < nx; ++i)
-      for (int j = 0; j < ny; ++j)
-        std::memcpy(m.data() + i * h->sx + j * h->sy, c.mat_id.data() + (static_cast<size_t>(i) * ny + j) * nz, nz);
     void* p;  // same guard as the fields (the one-sweep kernel stages halo windows)
-    if ((rc = alloc(h, &p, m.size() + 2 * h->guard, false))) return rc;
-    if ((rc = copy(h, static_cast<uint8_t*>(p) + h->guard, m.data(), m.size(), cudaMemcpyHostToDevice))) return rc;
+    if ((rc = alloc(h, &p, static_cast<size_t>(h->elems) + 2 * h->guard, false))) return rc;
     h->mid = static_cast<uint8_t*>(p) + h->guard;
+    const size_t dense = c.mat_id.size();
+    void* tmp = nullptr;
+    if (cudaMalloc(&tmp, dense) != cudaSuccess) {
+      cudaGetLastError();
+      return set_err(h, XFB_ERR_OOM, "cudaMalloc of the material-id staging buffer failed");
+    }
+    rc = copy(h, tmp, c.mat_id.data(), dense, cudaMemcpyHostToDevice);
+    if (rc == XFB_OK) {
+      const long long rows = static_cast<long long>(nx) * ny;
+      k_spread_ids<uint8_t><<<static_cast<unsigned>(std::min<long long>((rows + 7) / 8, 148LL * 64)), 256, 0, h->stream>>>(
+          static_cast<const uint8_t*>(tmp), h->mid, ny, nz, h->sx, h->sy, rows);
+      const cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) rc = cuda_err(h, e, "material-id spread");
+      const cudaError_t e2 = cudaStreamSynchronize(h->stream);  // before the staging buffer is freed
+      if (rc == XFB_OK && e2 != cudaSuccess) rc = cuda_err(h, e2, "material-id spread");
+    }
+    cudaFree(tmp);
+    if (rc) return rc;
   }
   if (h->coeff_storage == XFB_COEFF_NATIVE) {
     if ((rc = upload<T>(h, &h->lut, c.coeff))) return rc;
@@ -764,7 +796,13 @@ inline bool build_ade_runs(const Compiled& c, std::vector<int2>& runs, int p0 = 
   runs.clear();
   if (c.nx >= 65536 || c.ny >= 65536 || c.nz >= 65536) return false;
   if (p1 < 0) p1 = c.nx;  // planes [p0, p1) (an x slab)
-  for (int i = std::max(b[0], p0); i < std::min(b[1], p1); ++i)
+  const int i0 = std::max(b[0], p0), i1 = std::min(b[1], p1);
+  if (i1 <= i0) return true;
+  // the planes' runs are listed by plane-parallel threads, then joined in plane order
+  std::vector<std::vector<int2>> per(static_cast<size_t>(i1 - i0));
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int i = i0; i < i1; ++i) {
+    std::vector<int2>& out = per[static_cast<size_t>(i - i0)];
     for (int j = b[2]; j < b[3]; ++j) {
       const uint8_t* row = c.mat_id.data() + (static_cast<size_t>(i) * c.ny + j) * c.nz;
       int k = b[4];
@@ -773,11 +811,16 @@ inline bool build_ade_runs(const Compiled& c, std::vector<int2>& runs, int p0 = 
         const int kb = k & ~31;
         int e = k;
         while (e < b[5] && e < kb + 32 && c.mat_disp[row[e]]) ++e;
-        runs.push_back(make_int2(static_cast<int>(static_cast<unsigned>(i) | (static_cast<unsigned>(j) << 16)),
-                                 kb | ((k - kb) << 16) | ((e - kb) << 24)));
+        out.push_back(make_int2(static_cast<int>(static_cast<unsigned>(i) | (static_cast<unsigned>(j) << 16)),
+                                kb | ((k - kb) << 16) | ((e - kb) << 24)));
         k = e;
       }
     }
+  }
+  size_t n = 0;
+  for (const auto& v : per) n += v.size();
+  runs.reserve(n);
+  for (const auto& v : per) runs.insert(runs.end(), v.begin(), v.end());
   return true;
 }
 
@@ -1134,6 +1177,9 @@ void enqueue_chunk(xfb_handle* h, int n) {
 }
 
 template <typename T>
+bool readback_buffers(xfb_handle* h);
+
+template <typename T>
 int run_steps(xfb_handle* h, long long n) {
   long long left = n;
   while (left > 0) {
@@ -1160,6 +1206,9 @@ int run_steps(xfb_handle* h, long long n) {
     left -= chunk;
     h->step += chunk;
   }
+  // the read-back's staging buffers, allocated while the device steps (a
+  // failure leaves the read-back to its unstaged form)
+  if (n > 0 && !h->rb_host[1] && !readback_buffers<T>(h)) h->err.clear();
   return XFB_OK;
 }
 
@@ -1210,13 +1259,6 @@ __global__ void k_gather_field(const T* src, T* dst, long long sx, long long sy,
 // buffer hold this many elements of the compute type).
 constexpr long long kReadChunk = 4LL << 20;
 
-// dst[q] = double(src[q]) for q < n, split over the host threads.
-template <typename T>
-void widen_to_double(const T* src, double* dst, long long n) {
-  const int threads = std::max(1, std::min(16, omp_get_max_threads()));
-#pragma omp parallel for schedule(static) num_threads(threads)
-  for (long long q = 0; q < n; ++q) dst[q] = static_cast<double>(src[q]);
-}
 
 // Read-back buffers of the handle (device gather buffer, two pinned host
 // buffers, their events), allocated on first use and kept until the next
@@ -1272,7 +1314,7 @@ int read_field_t(xfb_handle* h, int f, double* dst) {
       if (e == cudaSuccess) e = cudaEventSynchronize(h->rb_ev[c & 1]);
       if (e != cudaSuccess) break;
       const long long q0 = c * kReadChunk, n = std::min(kReadChunk, total - q0);
-      widen_to_double(static_cast<const T*>(h->rb_host[c & 1]), dst + q0, n);
+      host_widen(static_cast<const T*>(h->rb_host[c & 1]), dst + q0, n);
       h->d2h_bytes += n * static_cast<long long>(sizeof(T));
     }
     if (e != cudaSuccess) {
@@ -1315,19 +1357,12 @@ int read_bytes_t(xfb_handle* h, void* dst, const void* src, size_t bytes) {
     return e;
   };
   cudaError_t e = enqueue(0);
-  const int threads = std::max(1, std::min(16, omp_get_max_threads()));
   for (size_t c = 0; c < nch && e == cudaSuccess; ++c) {
     if (c + 1 < nch) e = enqueue(c + 1);
     if (e == cudaSuccess) e = cudaEventSynchronize(h->rb_ev[c & 1]);
     if (e != cudaSuccess) break;
-    const size_t o = c * chunk, n = std::min(chunk, bytes - o), per = (n + threads - 1) / threads;
-    const char* from = static_cast<const char*>(h->rb_host[c & 1]);
-    char* to = static_cast<char*>(dst) + o;
-#pragma omp parallel for schedule(static) num_threads(threads)
-    for (int t = 0; t < threads; ++t) {
-      const size_t a = static_cast<size_t>(t) * per;
-      if (a < n) std::memcpy(to + a, from + a, std::min(per, n - a));
-    }
+    const size_t o = c * chunk, n = std::min(chunk, bytes - o);
+    host_copy(h->rb_host[c & 1], static_cast<char*>(dst) + o, n);
     h->d2h_bytes += static_cast<long long>(n);
   }
   if (e != cudaSuccess) {

@@ -18,6 +18,7 @@ struct Buf {
   void* p = nullptr;
   size_t bytes = 0;
   bool state = false;  // part of the checkpoint state
+  bool owner = true;   // p is a cudaMalloc base (freed with the handle's device state)
 };
 
 }  // namespace xfb
@@ -54,6 +55,10 @@ struct xfb_handle {
   std::map<int, cudaGraphExec_t> graphs;
   std::vector<Buf> bufs;
   size_t bytes = 0;
+  // device buffers up to kArenaMax bytes are carved from chunks of one
+  // cudaMalloc each (fewer driver calls at init): the free part of the last chunk
+  char* arena = nullptr;
+  size_t arena_left = 0;
   int esize = 4;
   // field layout
   long long sx = 0, sy = 0, nzp = 0, elems = 0, guard = 0;
@@ -209,6 +214,8 @@ T* as(void* p) { return static_cast<T*>(p); }
 
 void free_device(xfb_handle* h);
 int alloc(xfb_handle* h, void** out, size_t bytes, bool state);
+// n zeroed buffers of `bytes` each (256-byte aligned) from one cudaMalloc.
+int alloc_block(xfb_handle* h, void** out, int n, size_t bytes, bool state);
 // Every host<->device copy of the library goes through this: it is issued on
 // the handle's stream (a non-blocking stream, which the legacy default stream
 // does not order against) and waited for, so it lands after the zero-fill of

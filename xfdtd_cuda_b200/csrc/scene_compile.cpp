@@ -331,7 +331,19 @@ int compile_scene(const xfb_scene& s, Compiled& c, std::string* err) {
 
   // ---- voxelisation: material of the last object holding the cell centre --
   const size_t ncell = static_cast<size_t>(c.nx) * c.ny * c.nz;
-  c.mat_id.assign(ncell, 0);
+  c.mat_id.resize(ncell);  // zeroed plane by plane below (first touch spread over the threads)
+  {
+    const size_t plane = static_cast<size_t>(c.ny) * c.nz;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < c.nx; ++i) std::memset(c.mat_id.data() + i * plane, 0, plane);
+  }
+  // union of the cell boxes of the objects with a dispersive material: the
+  // only cells that can hold one (unless material 0, the fill, is dispersive)
+  int dlo[3] = {c.nx, c.ny, c.nz}, dhi[3] = {0, 0, 0};
+  if (c.n_mat > 0 && c.mat_disp[0]) {
+    dlo[0] = dlo[1] = dlo[2] = 0;
+    dhi[0] = c.nx; dhi[1] = c.ny; dhi[2] = c.nz;
+  }
   for (int o = 0; o < s.n_objects; ++o) {
     const xfb_object& ob = s.objects[o];
     if (ob.material < 0 || ob.material >= c.n_mat) return fail("object material index out of range");
@@ -348,6 +360,11 @@ int compile_scene(const xfb_scene& s, Compiled& c, std::string* err) {
         hi[a] = std::min(n[a], static_cast<int>(std::ceil((ob.p[a] + ob.p[3] - c.origin[a]) / d[a])) + 1);
       }
     }
+    if (c.mat_disp[ob.material])
+      for (int a = 0; a < 3; ++a) {
+        dlo[a] = std::min(dlo[a], lo[a]);
+        dhi[a] = std::max(dhi[a], hi[a]);
+      }
     // planes are independent (each cell is written by one plane's thread)
 #pragma omp parallel for schedule(static)
     for (int i = lo[0]; i < hi[0]; ++i) {
@@ -365,9 +382,9 @@ int compile_scene(const xfb_scene& s, Compiled& c, std::string* err) {
   if (c.ade_kind != XFB_ADE_NONE) {
     int b0 = c.nx, b1 = 0, b2 = c.ny, b3 = 0, b4 = c.nz, b5 = 0;
 #pragma omp parallel for schedule(static) reduction(min : b0, b2, b4) reduction(max : b1, b3, b5)
-    for (int i = 0; i < c.nx; ++i)
-      for (int j = 0; j < c.ny; ++j)
-        for (int kk = 0; kk < c.nz; ++kk) {
+    for (int i = dlo[0]; i < dhi[0]; ++i)
+      for (int j = dlo[1]; j < dhi[1]; ++j)
+        for (int kk = dlo[2]; kk < dhi[2]; ++kk) {
           const int m = c.mat_id[(static_cast<size_t>(i) * c.ny + j) * c.nz + kk];
           if (c.ade_mat[static_cast<size_t>(m) * kAdeMat] != 0) {
             b0 = std::min(b0, i); b1 = std::max(b1, i + 1);

@@ -2,6 +2,8 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -26,6 +28,27 @@ enum Coef {
   CHXH, CHXEY, CHXEZ, CHYH, CHYEZ, CHYEX, CHZH, CHZEX, CHZEY
 };
 
+// Allocator whose resize() leaves new elements uninitialised, so that a large
+// array is first touched (its pages faulted in) by the threads that fill it.
+template <typename T>
+struct DefaultInit : std::allocator<T> {
+  template <typename U>
+  struct rebind {
+    using other = DefaultInit<U>;
+  };
+  DefaultInit() = default;
+  template <typename U>
+  DefaultInit(const DefaultInit<U>&) noexcept {}
+  template <typename U>
+  void construct(U* p) noexcept {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <typename U, typename... A>
+  void construct(U* p, A&&... a) {
+    ::new (static_cast<void*>(p)) U(static_cast<A&&>(a)...);
+  }
+};
+
 // Result of compiling an xfb_scene on the host: the data XFDTD_CORE would hand
 // to the reference's *HD wrappers, in engine form (material index + LUT
 // instead of 18 per-cell coefficient arrays).
@@ -34,7 +57,7 @@ struct Compiled {
   int nx = 0, ny = 0, nz = 0;
   double dx = 0, dy = 0, dz = 0, dt = 0;
   double origin[3] = {0, 0, 0};
-  std::vector<uint8_t> mat_id;   // [nx][ny][nz]
+  std::vector<uint8_t, DefaultInit<uint8_t>> mat_id;   // [nx][ny][nz]
   int n_mat = 0;
   std::vector<double> coeff;     // [n_mat][18]
   // Compact form of the same coefficients: [n_mat][8] = ce, cb/dx, cb/dy, cb/dz,
@@ -120,5 +143,11 @@ constexpr double kTdC0 = 299792458.0;
 // (ref - r . dir) / (c dt).
 double td_delay_steps(const Compiled& c, int face, int i, int j, int k);
 void compile_td(Compiled& c, double theta, double phi);
+
+// Read-back copies into large host result arrays, split over host threads
+// (host_copy.cpp): dst[q] = double(src[q]) for q < n, and a byte copy.
+void host_widen(const float* src, double* dst, long long n);
+void host_widen(const double* src, double* dst, long long n);
+void host_copy(const void* src, void* dst, size_t bytes);
 
 }  // namespace xfb

@@ -910,10 +910,11 @@ class Batch:
 class SimulationHD:
     """Drop-in for ``xfdtd::cuda::SimulationHD`` (simulation_hd.cuh:37-88).
 
-    init(n) compiles the host scene, uploads the device state and allocates
-    the host result arrays (the fields in ``host().emf``, the NF2FF surface
-    currents), as XFDTD_CORE's Simulation::init does; run(n) has their pages
-    faulted in on background host threads while the device steps.
+    init(n) compiles the host scene, allocates the host result arrays (the
+    fields in ``host().emf``, the NF2FF surface currents), as XFDTD_CORE's
+    Simulation::init does, and uploads the device state; background host
+    threads fault in the result arrays' pages meanwhile and while the device
+    steps.
     copyDeviceToHost() fills them, as the reference copies results back into
     the host objects (simulation_hd.cu:228-247)."""
 
@@ -950,9 +951,11 @@ class SimulationHD:
         if self.kernel_path is not None:
             self.handle.set_kernel_path(self.kernel_path)
         self.handle.set_launch_hint(self._grid, self._block)
-        self.handle.init(time_step)
-        # after the device init: large untouched host mappings made it slower
+        # the host result arrays' pages are faulted in by host threads while
+        # the device state is set up and stepped
         self._alloc_host_results()
+        self.prefaultHostResults()
+        self.handle.init(time_step)
         self.timings = {"compile": t1 - t0, "init": time.perf_counter() - t1}
         gi = self.handle.info()
         for w in self._host.sources:
@@ -962,16 +965,18 @@ class SimulationHD:
     def run(self, time_step: int):
         """Reference run(n): initialise, advance n steps, copy results back
         into the host objects.  The pages of the host result arrays are
-        faulted in on host threads while the device steps."""
+        faulted in on host threads while the device initialises and steps."""
         self.init(time_step)
-        self.prefaultHostResults()
         self.handle.step(time_step)
         self.handle.sync()
         self.copyDeviceToHost()
 
     def prefaultHostResults(self):
         """Start faulting in the host result arrays on background host threads
-        (xfb_host_prefault); the next read joins them."""
+        (xfb_host_prefault); the next read joins them.  init() starts it; a
+        second call before the next read queues nothing."""
+        if getattr(self.handle, "_prefault_keep", None):
+            return
         emf = self._host.emf
         for f in range(6):
             a = emf.field(f) if emf is not None else None
