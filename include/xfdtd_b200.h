@@ -301,7 +301,8 @@ int xfb_read_field(xfb_handle* h, int field, double* dst, size_t dst_len);
  * page faults of every destination page (about 5x slower than into resident
  * memory), so a caller that allocates its result arrays ahead of a run (as
  * XFDTD_CORE allocates the host fields in Simulation::init) lets the faults
- * run while the device initialises and steps.  The range must stay allocated
+ * run while the device initialises and steps (it may be called between
+ * xfb_create and xfb_init for that).  The range must stay allocated
  * until the handle's next read, far-field or get_state call,
  * xfb_host_prefault_wait or xfb_destroy; each of these waits for the threads
  * first. */
