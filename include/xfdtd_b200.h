@@ -609,6 +609,8 @@ typedef struct xfb_compiled_view {
   double nf2ff_td_theta, nf2ff_td_phi;
   long long nf2ff_td_bins;      /* time bins of the potentials (after init)  */
   double origin[3];             /* physical position of node (0, 0, 0)      */
+  int ade_box[6];               /* i0 i1 j0 j1 k0 k1: cell bounds of the
+                                   dispersive cells (all 0 when none)        */
 } xfb_compiled_view;
 
 int xfb_compiled_view_get(const xfb_handle* h, xfb_compiled_view* out);

@@ -214,3 +214,38 @@ def test_ade_e_coefficients_consistent():
     assert am[1, 2] == pytest.approx(-1 / (2 * D), rel=1e-14)
     assert lut(v)[1][0] == pytest.approx((EPS0 / dt - pole[1, :, 3].sum() / 2) / D, rel=1e-14)
     np.testing.assert_allclose(pole[1, :, 5], 1 + pole[1, :, 0])
+
+
+def dispersive_bounds(v, gi):
+    ids = np.ctypeslib.as_array(v.material_id, shape=(gi.nx, gi.ny, gi.nz))
+    am = np.ctypeslib.as_array(v.ade_mat, shape=(v.n_materials, 3))
+    cells = np.argwhere(am[ids, 0] != 0)
+    if len(cells) == 0:
+        return [0] * 6
+    lo, hi = cells.min(axis=0), cells.max(axis=0) + 1
+    return [int(lo[0]), int(hi[0]), int(lo[1]), int(hi[1]), int(lo[2]), int(hi[2])]
+
+
+@pytest.mark.parametrize("layout", ["sphere", "sphere_cut_by_cube", "two_spheres", "dispersive_fill", "none"])
+def test_ade_box_is_the_dispersive_cell_bounds(layout):
+    """The ADE box (storage of the recursions' state) equals the bounds of
+    the cells that hold a dispersive material, however objects overlap."""
+    mat = X.DrudeMedium("d", 1.0, [2e10], [1e9])
+    s = X.Simulation(1e-3, 1e-3, 1e-3, 0.9)
+    fill = mat if layout == "dispersive_fill" else X.Material.createAir()
+    s.addObject(X.Object("domain", X.Cube(X.Vector(-0.02, -0.02, -0.02), X.Vector(0.04, 0.04, 0.04)), fill))
+    if layout in ("sphere", "sphere_cut_by_cube", "two_spheres"):
+        s.addObject(X.Object("s1", X.Sphere(X.Vector(0.003, -0.002, 0.001), 0.009), mat))
+    if layout == "two_spheres":
+        s.addObject(X.Object("s2", X.Sphere(X.Vector(-0.012, 0.01, 0.008), 0.004), mat))
+    if layout == "sphere_cut_by_cube":  # a later object takes half of the sphere's cells
+        s.addObject(X.Object("cut", X.Cube(X.Vector(-0.02, -0.02, -0.02), X.Vector(0.04, 0.04, 0.021)),
+                             X.Material.createPec()))
+    if layout == "dispersive_fill":  # an air block in a dispersive domain
+        s.addObject(X.Object("hole", X.Cube(X.Vector(-0.01, -0.01, -0.01), X.Vector(0.02, 0.02, 0.02)),
+                             X.Material.createAir()))
+    h, v, gi = compile_sim(s)
+    want = dispersive_bounds(v, gi)
+    assert list(v.ade_box) == want
+    if layout != "none":
+        assert want[0] < want[1]

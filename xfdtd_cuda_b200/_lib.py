@@ -140,6 +140,7 @@ class CompiledView(C.Structure):
         ("nf2ff_te", _dp), ("nf2ff_th", _dp),
         ("nf2ff_td_enabled", C.c_int), ("nf2ff_td_box", C.c_int * 6), ("nf2ff_td_theta", C.c_double),
         ("nf2ff_td_phi", C.c_double), ("nf2ff_td_bins", C.c_longlong), ("origin", C.c_double * 3),
+        ("ade_box", C.c_int * 6),
     ]
 
 

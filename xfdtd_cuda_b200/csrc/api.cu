@@ -1116,6 +1116,7 @@ int xfb_compiled_view_get(const xfb_handle* h, xfb_compiled_view* v) {
   v->nf2ff_td_phi = c.td_phi;
   v->nf2ff_td_bins = c.td_bins;
   for (int a = 0; a < 3; ++a) v->origin[a] = c.origin[a];
+  for (int q = 0; q < 6; ++q) v->ade_box[q] = c.ade_box[q];
   return XFB_OK;
 }
 
