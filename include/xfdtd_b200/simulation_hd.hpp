@@ -13,6 +13,7 @@
 #include <cstddef>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -194,19 +195,23 @@ class SimulationHD {
   SimulationHD(const SimulationHD&) = delete;
   SimulationHD& operator=(const SimulationHD&) = delete;
 
-  // device buffers for n steps (reference init + copyHostToDevice)
+  // device buffers for n steps (reference init + copyHostToDevice); the host
+  // result arrays are allocated meanwhile
   void init(Index time_step) {
+    start_results();
     b200::check(xfb_init(h_, static_cast<long long>(time_step)), h_);
     total_ = time_step;
   }
   void copyHostToDevice() { init(total_); }
   // re-initialise for n steps, advance them, pull the results
   void run(Index time_step) {
+    start_results();
     b200::check(xfb_run(h_, static_cast<long long>(time_step)), h_);
     total_ = time_step;
     copyDeviceToHost();
   }
   void copyDeviceToHost() {
+    join_results();
     xfb_grid_info gi{};
     b200::check(xfb_get_grid_info(h_, &gi), h_);
     for (int f = 0; f < 6; ++f) {
@@ -215,11 +220,12 @@ class SimulationHD {
         continue;
       }
       const size_t n = field_size(gi, f);
-      fields_[f].assign(n, 0.0);
+      if (fields_[f].size() != n) fields_[f].assign(n, 0.0);
       b200::check(xfb_read_field(h_, f, fields_[f].data(), n), h_);
     }
   }
   void releaseDevice() {
+    join_results();
     if (h_) xfb_destroy(h_);
     h_ = nullptr;
   }
@@ -256,6 +262,32 @@ class SimulationHD {
     if (gi.dim == 2) s[2] = 1;
     return static_cast<size_t>(s[0] * s[1] * s[2]);
   }
+  // The result arrays of the components (zero-filled, so every page is
+  // faulted in) are allocated by one host thread each while the device
+  // initialises and steps; copyDeviceToHost joins them first.  A thread that
+  // cannot allocate leaves its array empty for copyDeviceToHost to size.
+  void start_results() {
+    join_results();
+    xfb_grid_info gi{};
+    b200::check(xfb_get_grid_info(h_, &gi), h_);
+    for (int f = 0; f < 6; ++f) {
+      if (gi.dim == 2 && !(f == XFB_EZ || f == XFB_HX || f == XFB_HY)) continue;
+      const size_t n = field_size(gi, f);
+      if (fields_[f].size() == n) continue;
+      std::vector<double>* v = &fields_[f];
+      alloc_.emplace_back([v, n] {
+        try {
+          v->assign(n, 0.0);
+        } catch (...) {
+          v->clear();
+        }
+      });
+    }
+  }
+  void join_results() {
+    for (std::thread& t : alloc_) t.join();
+    alloc_.clear();
+  }
   void hint() {
     const unsigned g[3] = {grid_.x, grid_.y, grid_.z}, b[3] = {block_.x, block_.y, block_.z};
     b200::check(xfb_set_launch_hint(h_, g, b), h_);
@@ -265,6 +297,7 @@ class SimulationHD {
   Index total_ = 0;
   Dim3 grid_, block_;
   std::array<std::vector<double>, 6> fields_;
+  std::vector<std::thread> alloc_;  // result-array allocation threads
 };
 
 }  // namespace cuda
